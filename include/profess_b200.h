@@ -1,0 +1,161 @@
+/*
+ * profess_b200 — C ABI of the B200 orbital-free DFT density-solve engine.
+ *
+ * This is the drop-in boundary for the density-solve path of PROFESS: the
+ * energy/potential evaluation (module CalPotPlus, CalculatePotentialPlus) and
+ * the sqrt-density truncated-Newton optimiser (module RhoOptN, method NTN,
+ * ProjNormRhoMinimization).  A Fortran host binds these entry points through
+ * iso_c_binding; every argument is a plain pointer or scalar, arrays are
+ * Fortran-ordered (x fastest) REAL(DP) buffers exactly as the reference holds
+ * them, and every entry point returns an int status (0 = OK; see OFDFT_E*).
+ * ofdft_last_error() gives the message of the last failure on this thread.
+ *
+ * Objects: an engine owns device memory, streams and FFT plans; a slot is one
+ * cell (grid, lattice, functional parameters, kernel tables, ion potential and
+ * solver state) inside an engine.  One engine may hold many slots, which are
+ * then evaluated/solved together (batched, one launch per pass for all slots).
+ */
+#ifndef PROFESS_B200_H
+#define PROFESS_B200_H
+
+#include <stddef.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* status codes */
+#define OFDFT_OK 0
+#define OFDFT_EINVAL 1      /* bad argument */
+#define OFDFT_ECUDA 2       /* CUDA runtime failure */
+#define OFDFT_ENOMEM 3      /* device memory exhausted */
+#define OFDFT_EBUSY 4       /* slot is running */
+#define OFDFT_ENAN 5        /* non-finite value in a reduction */
+#define OFDFT_EGRAD 6       /* dE/dtheta too large (RhoLineSearch.f90:243-245) */
+#define OFDFT_ELINESEARCH 7 /* line search error past maxIter (RhoLineSearch.f90:431-440) */
+#define OFDFT_ETIMEOUT 8    /* solve exceeded the caller's tick budget */
+
+/* kinetic functional codes (CellInfo::kinetic) */
+#define OFDFT_KEDF_WT 4
+#define OFDFT_KEDF_WGC 5
+
+/* precision of a slot */
+#define OFDFT_FP64 0
+#define OFDFT_FP32 1
+
+/* convergence tests (RhoOptimizers::conv_check) */
+#define OFDFT_CONV_ENE 0
+#define OFDFT_CONV_POT 1
+#define OFDFT_CONV_BOTH 2
+
+typedef struct ofdft_engine ofdft_engine;
+
+/* Cell description: the module state CalculatePotentialPlus reads through USE
+ * association (Source/CalPotential.f90:41-116; CellInfo, KEDF_TF, KEDF_VW,
+ * KEDF_WTkernel, KEDF_WGCkernel, Sys, Ewald). */
+typedef struct ofdft_cell_desc {
+  int n1, n2, n3;          /* real-space grid n1G, n2G, n3G */
+  double lattice[9];       /* cell%cellReal in bohr, column-major: lattice[3*i+k] = component k of vector i */
+  int kinetic;             /* OFDFT_KEDF_WT or OFDFT_KEDF_WGC (second order, WGCT = 2) */
+  double lambda, mu;       /* TF and vW coefficients (KEDF_TF::lambda, KEDF_VW::mu) */
+  double alpha, beta;      /* nonlocal exponents (KEDF_WTkernel::alpha, beta) */
+  double gamma;            /* WGC gamma (KEDF_WGCkernel::gamma); kernel construction only */
+  double rho0;             /* Sys::rho0, WT/WGC kernel reference density */
+  double rho_s;            /* Sys::rhoS, WGC Taylor expansion density */
+  double ion_ion_energy;   /* Ewald::ionIonEnergy (Ha), copied into eTable(6) */
+  int precision;           /* OFDFT_FP64 or OFDFT_FP32 */
+} ofdft_cell_desc;
+
+/* Options of the NTN solve (RhoOptimizers module state, Source/RhoOptimizers.f90:44-101). */
+typedef struct ofdft_ntn_options {
+  int max_iter;            /* maxIter, default 500 */
+  int conv_check;          /* OFDFT_CONV_*, default ENE */
+  double pot_tol;          /* pot_tol, default 1e-5 */
+  double tole;             /* tole (Ha), default 1e-6 */
+  int max_line;            /* maxLine (Source/RhoLineSearch.f90:34), default 200 */
+  int max_ticks;           /* safety bound on engine ticks for the blocking call (0 = 20000) */
+} ofdft_ntn_options;
+
+/* Outcome of a solve (rhoOutcome, numEnergyTotal, numPotentialTotal ...). */
+typedef struct ofdft_ntn_stats {
+  int outcome;             /* rhoOutcome: 0 converged, 1 max iterations / no descent */
+  int iterations;          /* outer NTN iterations */
+  int num_evals;           /* potential evaluations (CalculatePotentialPlus calls) */
+  int num_cg;              /* inner CG steps in total */
+  int num_line;            /* line-search evaluations in total */
+  int history_len;         /* entries available from ofdft_slot_history */
+  double pot_norm;         /* final potential norm (StepInformation) */
+  int error;               /* internal error code (0 none) */
+  int ticks;               /* engine ticks the solve took */
+} ofdft_ntn_stats;
+
+const char* ofdft_last_error(void);
+int ofdft_version(void);
+
+/* ---------------------------------------------------------------- engine */
+int ofdft_engine_create(ofdft_engine** out);
+int ofdft_engine_destroy(ofdft_engine* e);
+
+/* ---------------------------------------------------------------- slots */
+/* Allocate a slot for one cell.  Replaces the module set-up that precedes the
+ * first CalculatePotentialPlus call (Source/Initializer.f90, SetupKEDF.f90). */
+int ofdft_slot_create(ofdft_engine* e, const ofdft_cell_desc* desc, int* slot);
+int ofdft_slot_destroy(ofdft_engine* e, int slot);
+/* KEDF_WTkernel::keKernel(k1G,k2G,k3G,nplanes), k1G = n1/2+1 (Source/KEDF_WTkernel.f90:81-208,
+ * Source/KEDF_WGCkernel.f90:109-277); nplanes = 1 for WT, 4 for WGC. */
+int ofdft_slot_set_kernel(ofdft_engine* e, int slot, const double* kernel, int nplanes);
+/* IonElectronSpline::ionPotReal(n1G,n2G,n3G) (Source/RefreshIons.f90:215-221). */
+int ofdft_slot_set_ion_potential(ofdft_engine* e, int slot, const double* ion_pot);
+/* The WT kernel built on the device from LindG (replaces FillWT, KEDF_WTkernel.f90:81-208). */
+int ofdft_slot_build_wt_kernel(ofdft_engine* e, int slot);
+/* The WGC kernel planes from radial tables of w, eta*w', eta^2*w'' on the eta
+ * grid (Source/KEDF_WGCkernel.f90:166-230); splines are evaluated on the device. */
+int ofdft_slot_build_wgc_kernel(ofdft_engine* e, int slot, int ntab, const double* eta,
+                                const double* w, const double* w1, const double* w2);
+/* The ion-electron potential built on the device by the cardinal B-spline
+ * method (IonElectronPotRecipSpline, Source/IonElectronSpline.f90:83-216):
+ * frac[3*nion] fractional coordinates, species[nion] 0-based species index;
+ * per species s: npts[s] points of the recpot table on [0, max_g[s]] (bohr^-1)
+ * with values pot_values (Ha*bohr^3), spline knots vqs and second derivatives
+ * pot_dd, packed one species after the other; charge[s] the ionic charge. */
+int ofdft_slot_build_ion_potential(ofdft_engine* e, int slot, int nion, const double* frac,
+                                   const int* species, int nspecies, const int* npts,
+                                   const double* max_g, const double* charge,
+                                   const double* pot_values, const double* vqs, const double* pot_dd);
+
+/* ---------------------------------------------------------------- drop-in calls */
+/* CalculatePotentialPlus(rho, optSqrt, potential, eTable) (Source/CalPotential.f90:41-647),
+ * numSpin = 1.  rho and potential are (n1,n2,n3) x-fastest; eTable (9 doubles,
+ * Report.f90:270-308 order) may be NULL, which skips the energy terms. */
+int ofdft_calculate_potential_plus(ofdft_engine* e, int slot, const double* rho, int opt_sqrt,
+                                   double* potential, double* etable);
+/* ProjNormRhoMinimization(energy, dir_type = 1) (Source/RhoOptN.f90:60-545):
+ * rho (n1,n2,n3) is Sys::rhoR on entry and the optimised density on return;
+ * energy receives the 9-entry table; opts may be NULL for the defaults. */
+int ofdft_proj_norm_rho_minimization(ofdft_engine* e, int slot, double* rho, double* energy,
+                                     const ofdft_ntn_options* opts, ofdft_ntn_stats* stats);
+
+/* ---------------------------------------------------------------- batched / asynchronous */
+int ofdft_slot_start_solve(ofdft_engine* e, int slot, const double* rho, const ofdft_ntn_options* opts);
+/* Start a solve from the density already resident in another slot of the same
+ * engine (e.g. an FP32 slot's result refined in an FP64 slot); no host copy. */
+int ofdft_slot_start_solve_from_slot(ofdft_engine* e, int slot, int src_slot, const ofdft_ntn_options* opts);
+int ofdft_slot_start_eval(ofdft_engine* e, int slot, const double* rho, int opt_sqrt, int want_energy);
+/* Run up to `ticks` engine ticks over every running slot; *running receives the
+ * number of slots still running afterwards. */
+int ofdft_engine_run(ofdft_engine* e, int ticks, int* running);
+/* 1 if the slot has finished (done or error), 0 if it is running. */
+int ofdft_slot_poll(ofdft_engine* e, int slot, int* finished);
+/* Results of a finished solve: rho (may be NULL) = phi^2, energy (9, may be NULL), stats. */
+int ofdft_slot_result(ofdft_engine* e, int slot, double* rho, double* energy, ofdft_ntn_stats* stats);
+/* Per-iteration trajectory (MinimizerReportSteps rows): energy (Ha), potential
+ * norm, theta, #CG, #line; up to max entries. */
+int ofdft_slot_history(ofdft_engine* e, int slot, int max, double* energy, double* pot_norm,
+                       double* theta, int* ncg, int* nline, int* n);
+/* Device-resident arrays of a slot: which = 0 phi, 1 dE/dphi, 2 ion potential. */
+int ofdft_slot_download(ofdft_engine* e, int slot, int which, double* out);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* PROFESS_B200_H */

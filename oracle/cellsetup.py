@@ -80,17 +80,13 @@ class Cell:
 def parse_recpot_text(text: str, name: str = "X") -> Species:
     """Read a CASTEP .recpot table the way ReadPseudo does (ReadIonFile.f90:821-976).
 
-    Values are eV*A^3 on a uniform q grid up to maxG (A^-1); they are converted to
-    Ha*bohr^3 and bohr^-1, the ionic charge is inferred from the first two points,
-    and a cubic spline of V(q) + 4 pi Z / q^2 is set up over the point index with
-    zero end slopes (ReadIonFile.f90:955-976)."""
+    The number of points is 3 * (records after the maxG line) - 3; the record
+    count includes the closing "1000" line (ReadIonFile.f90:856-863)."""
     lines = text.splitlines()
     k = next(i for i, ln in enumerate(lines) if "END COMMENT" in ln)
     # line k+1 is the "3 5" version line; line k+2 is maxG; then the data
-    max_g = float(lines[k + 2].split()[0]) * BOHR
-    data_lines = lines[k + 3:]
-    # number of points = 3 * (records after maxG) - 3 (ReadIonFile.f90:856-863)
-    records = [ln for ln in data_lines if ln.strip() != ""]
+    max_g_ang = float(lines[k + 2].split()[0])
+    records = [ln for ln in lines[k + 3:] if ln.strip() != ""]
     if not records or records[-1].split()[0] != "1000":
         raise ValueError("Pseudopotential lacks the proper terminator")
     num_points = 3 * len(records) - 3
@@ -100,9 +96,21 @@ def parse_recpot_text(text: str, name: str = "X") -> Species:
     vals = np.array([float(t) for t in toks[:num_points]], dtype=float)
     if len(vals) < num_points:
         raise ValueError("recpot data shorter than declared")
+    return species_from_table(max_g_ang, vals, name)
+
+
+def species_from_table(max_g_ang: float, values_ev_a3: np.ndarray, name: str = "X") -> Species:
+    """Species from a recpot table: maxG in A^-1 and V(q) in eV*A^3.
+
+    Converts to Ha*bohr^3 and bohr^-1, infers the ionic charge from the first
+    two points and sets up the cubic spline of V(q) + 4 pi Z / q^2 over the
+    point index with zero end slopes (ReadIonFile.f90:914-976)."""
+    vals = np.array(values_ev_a3, dtype=float)
     if vals[-1] == 1000.0:  # ReadIonFile.f90:914-917
         vals[-1] = 0.0
     vals = vals / (BOHR ** 3 * HARTREE_TO_EV)
+    max_g = max_g_ang * BOHR
+    num_points = len(vals)
     dq = max_g / float(num_points - 1)
     charge = int(np.rint(-(vals[1] - vals[0]) * dq ** 2 / (4.0 * PI)))
     t = np.arange(1, num_points + 1, dtype=float)
@@ -196,7 +204,7 @@ def parse_ion_file(text: str, recpots: dict) -> Cell:
     """Minimal reader for the reference's .ion blocks (ReadIonFile.f90).
 
     Supports LATTICE_CART (Angstrom, one lattice vector per line),
-    POSITIONS_FRAC and SPECIES_POT; ``recpots`` maps species name to recpot text."""
+    POSITIONS_FRAC and SPECIES_POT; ``recpots`` maps species name to recpot text or a Species."""
     def block(name):
         m = re.search(r"%BLOCK\s+" + name + r"(.*?)%END\s*BLOCK\s+" + name, text, re.S | re.I)
         if not m:
@@ -209,7 +217,8 @@ def parse_ion_file(text: str, recpots: dict) -> Cell:
     pos = block("POSITIONS_FRAC")
     sp_rows = block("SPECIES_POT")
     names = [r[0] for r in sp_rows]
-    species = [parse_recpot_text(recpots[nm], nm) for nm in names]
+    species = [recpots[nm] if isinstance(recpots[nm], Species) else parse_recpot_text(recpots[nm], nm)
+               for nm in names]
     idx = np.array([names.index(r[0]) for r in pos], dtype=np.int64)
     frac = np.array([[float(x) for x in r[1:4]] for r in pos])
     return Cell(lattice=lattice, frac=frac, species_of_ion=idx, species=species)

@@ -123,6 +123,29 @@ int ofdft_slot_build_ion_potential(ofdft_engine* e, int slot, int nion, const do
                                    const double* max_g, const double* charge,
                                    const double* pot_values, const double* vqs, const double* pot_dd);
 
+/* Ion forces (Ha/bohr, nion x 3, row i = ion i) on the slot's current density
+ * (rho = NULL: the density of the last solve, phi^2) or on the given rho:
+ * ion-electron forces by the B-spline method (IonElectronForcesSpline /
+ * CalculateSplineForces, Source/IonElectronSpline.f90:219-355,642-753) plus,
+ * when include_ewald, the ion-ion Ewald forces (ForcesII_IE,
+ * Source/CalForce.f90:134-239).  Needs ofdft_slot_build_ion_potential first. */
+int ofdft_slot_forces(ofdft_engine* e, int slot, const double* rho, int include_ewald, double* forces);
+
+/* ---------------------------------------------------------------- host set-up helpers */
+/* Ewald ion-ion energy (Ha) and forces (may be NULL) of point charges
+ * (EwaldEnergy / EwaldForces, Source/Ewald.f90:465-1193,1196+).  lattice as in
+ * ofdft_cell_desc; frac[3*nion]; charges[nion]. */
+int ofdft_ewald(const double* lattice, int nion, const double* frac, const double* charges, double* energy,
+                double* forces);
+/* FFT grid from the kinetic-energy cutoff (Ha): SizeSystem / PadFFTdims
+ * (Source/SetupFFT.f90:193-382) with dimType 1 (7-smooth sizes). */
+int ofdft_grid_size(double ecut_ha, const double* lattice, int* n);
+/* Radial WGC kernel tables (eta, w, eta w', eta^2 w'') on the reference's eta
+ * grid from the kernel ODE (makeKernel2, Source/KEDF_KernelODE.f90:254-537).
+ * Call with max = 0 to get the table length in *n. */
+int ofdft_wgc_radial_tables(double alpha, double beta, double gamma, int max, double* eta, double* w, double* w1,
+                            double* w2, int* n);
+
 /* ---------------------------------------------------------------- drop-in calls */
 /* CalculatePotentialPlus(rho, optSqrt, potential, eTable) (Source/CalPotential.f90:41-647),
  * numSpin = 1.  rho and potential are (n1,n2,n3) x-fastest; eTable (9 doubles,

@@ -31,6 +31,7 @@ NVCC_FLAGS = [
     "-gencode", "arch=compute_100a,code=sm_100a",
     "-Xcompiler", "-fPIC", "-shared",
     "--expt-relaxed-constexpr",
+    "-Xcompiler", "-fopenmp", "-lgomp",
 ]
 
 
@@ -64,7 +65,7 @@ def build_emu(force: bool = False) -> str:
     if not force and not _stale(EMU_PATH):
         return EMU_PATH
     os.makedirs(EMU_DIR, exist_ok=True)
-    cmd = ["g++", "-O2", "-std=c++17", "-fPIC", "-shared", "-DOFDFT_EMU", "-x", "c++",
+    cmd = ["g++", "-O2", "-std=c++17", "-fPIC", "-shared", "-fopenmp", "-DOFDFT_EMU", "-x", "c++",
            "-I", INCLUDE, "-I", CSRC, os.path.join(CSRC, "engine.cu"), "-o", EMU_PATH]
     subprocess.run(cmd, check=True)
     return EMU_PATH

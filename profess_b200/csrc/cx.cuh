@@ -54,5 +54,16 @@ HD double m_pow(double a, double b) { return pow(a, b); }
 HD float m_pow(float a, float b) { return powf(a, b); }
 HD double m_log(double v) { return log(v); }
 HD float m_log(float v) { return logf(v); }
+#if defined(__CUDA_ARCH__)
+HD double m_rcbrt(double v) { return rcbrt(v); }
+HD float m_rcbrt(float v) { return rcbrtf(v); }
+HD double m_rsqrt(double v) { return rsqrt(v); }
+HD float m_rsqrt(float v) { return rsqrtf(v); }
+#else
+HD double m_rcbrt(double v) { return 1.0 / cbrt(v); }
+HD float m_rcbrt(float v) { return 1.0f / cbrtf(v); }
+HD double m_rsqrt(double v) { return 1.0 / sqrt(v); }
+HD float m_rsqrt(float v) { return 1.0f / sqrtf(v); }
+#endif
 
 }  // namespace ofdft

@@ -20,7 +20,7 @@
 #include <string>
 #include <vector>
 
-#include "passes.cuh"
+#include "setup.cuh"
 #include "profess_b200.h"
 
 #if !defined(OFDFT_EMU)
@@ -118,6 +118,7 @@ struct PlanTable {
             re.push_back(cosl(ang));
             im.push_back(sinl(ang));
           }
+        p.ns_magic[s] = (unsigned)(((1u << 20) + (unsigned)ns - 1) / (unsigned)ns);
         off += ns * (R - 1);
         ns *= R;
       }
@@ -146,30 +147,59 @@ struct PlanTable {
 };
 
 // ------------------------------------------------------------ kernels
-enum Pass : int { P_VEC = 0, P_X1 = 1, P_Y2 = 2, P_Z3 = 3, P_Y4 = 4, P_X5 = 5, NPASS = 6 };
-constexpr int VEC_PER_TICK = 3;
+enum Pass : int { P_VEC = 0, P_X1 = 1, P_Y2 = 2, P_Z3 = 3, P_Y4 = 4, P_X5 = 5, P_CTL = 6, NPASS = 7 };
+constexpr int VEC_PER_TICK = 2;
 constexpr int VCHUNK = 4096;
 
 #if !defined(OFDFT_EMU)
-template <typename T> __global__ void k_vec(Args<T> a) {
+template <typename T> __global__ void __launch_bounds__(256) k_vec(Args<T> a) {
   extern __shared__ __align__(16) char sm[];
   vec_block<T>(a, blockIdx.x, threadIdx.x, blockDim.x, sm);
 }
-template <typename T> __global__ void k_xfwd(Args<T> a) {
+template <typename T> __global__ void __launch_bounds__(256) k_xfwd(Args<T> a) {
   extern __shared__ __align__(16) char sm[];
   xfwd_block<T>(a, blockIdx.x, threadIdx.x, blockDim.x, sm);
 }
-template <typename T> __global__ void k_ypass(Args<T> a, int dir) {
+template <typename T> __global__ void __launch_bounds__(256) k_ypass(Args<T> a, int dir) {
   extern __shared__ __align__(16) char sm[];
   ypass_block<T>(a, blockIdx.x, threadIdx.x, blockDim.x, sm, dir);
 }
-template <typename T> __global__ void k_zpass(Args<T> a) {
+template <typename T> __global__ void __launch_bounds__(256) k_zpass(Args<T> a) {
   extern __shared__ __align__(16) char sm[];
   zpass_block<T>(a, blockIdx.x, threadIdx.x, blockDim.x, sm);
 }
-template <typename T> __global__ void k_xinv(Args<T> a) {
+template <typename T> __global__ void __launch_bounds__(256, 3) k_xinv(Args<T> a) {
   extern __shared__ __align__(16) char sm[];
   xinv_block<T>(a, blockIdx.x, threadIdx.x, blockDim.x, sm);
+}
+template <typename T> __global__ void __launch_bounds__(256) k_fill_kernel(const SlotDev* sd, KernArgs ka, int kind) {
+  const SlotDev& s = *sd;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < (int)s.Nc; i += gridDim.x * blockDim.x)
+    fill_kernel_point<T>(s, ka, kind, i);
+}
+template <typename T> __global__ void __launch_bounds__(256) k_spread(const SlotDev* sd, const IonStencil* st) {
+  for (int w = threadIdx.x; w < SPLINE_ORDER * SPLINE_ORDER * SPLINE_ORDER; w += blockDim.x)
+    spread_ion<T>(*sd, st[blockIdx.x], w);
+}
+template <typename T> __global__ void __launch_bounds__(256) k_force_gather(const SlotDev* sd, const IonStencil* st,
+                                                                           double* out) {
+  __shared__ double red[3][256];
+  double f3[3] = {0, 0, 0};
+  for (int w = threadIdx.x; w < SPLINE_ORDER * SPLINE_ORDER * SPLINE_ORDER; w += blockDim.x)
+    force_term<T>(*sd, st[blockIdx.x], w, f3);
+  for (int k = 0; k < 3; ++k) red[k][threadIdx.x] = f3[k];
+  __syncthreads();
+  for (int stride = blockDim.x / 2; stride > 0; stride >>= 1) {
+    if ((int)threadIdx.x < stride)
+      for (int k = 0; k < 3; ++k) red[k][threadIdx.x] += red[k][threadIdx.x + stride];
+    __syncthreads();
+  }
+  if (threadIdx.x == 0)
+    for (int k = 0; k < 3; ++k) out[3 * blockIdx.x + k] = red[k][0];
+}
+template <typename T> __global__ void __launch_bounds__(64) k_ctl(Args<T> a, int kid) {
+  __shared__ double sm[NCH * 33 + 2];
+  ctl_block(a.slots, a.ctl, a.tasks, kid, blockIdx.x, threadIdx.x, blockDim.x, (char*)sm);
 }
 #endif
 
@@ -187,8 +217,15 @@ struct HostSlot {
   int prec = 0;
   SlotDev sd;
   std::vector<void*> allocs;
-  int nrowpairs = 0, rp = 1, tx = 8;
+  int nrowpairs = 0, rp1 = 1;
   int nplanes = 0;
+  int nion = 0;                 // ions of the last ion-potential build
+  IonStencil* d_stencil = nullptr;
+  std::vector<IonStencil> stencils;
+  double cell_inv_t[9];         // TRANSPOSE(Inverse(cellReal)), row-major
+  double lattice[9];
+  double rho0 = 0, gamma = 2.7;
+  std::vector<double> frac, zion;
 };
 
 static size_t elem_size(int prec) { return prec == OFDFT_FP32 ? 4 : 8; }
@@ -202,10 +239,26 @@ struct Engine {
   LaunchList lists[2][NPASS];
   bool dirty = true;
   std::vector<char> emu_smem;
+#if defined(OFDFT_EMU)
+  int d2h_stream(void* h, const void* d, size_t n) { return d2h(h, d, n); }
+#else
+  cudaStream_t stream = nullptr;
+  cudaGraphExec_t graph_exec = nullptr;
+  int graph_ticks = 0;
+  int d2h_stream(void* h, const void* d, size_t n) {
+    int rc = cuda_check(cudaMemcpyAsync(h, d, n, cudaMemcpyDeviceToHost, stream), "D2H async");
+    if (rc) return rc;
+    return cuda_check(cudaStreamSynchronize(stream), "stream synchronize");
+  }
+#endif
 
   int init(int capacity) {
     cap = capacity;
     slots.resize(cap);
+#if !defined(OFDFT_EMU)
+    int rs = cuda_check(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking), "stream create");
+    if (rs) return rs;
+#endif
     int rc = dmalloc((void**)&d_slots, sizeof(SlotDev) * cap);
     if (rc) return rc;
     rc = dmalloc((void**)&d_ctl, sizeof(Ctl) * cap);
@@ -214,18 +267,30 @@ struct Engine {
   }
 
   void release() {
+#if !defined(OFDFT_EMU)
+    if (graph_exec) cudaGraphExecDestroy(graph_exec);
+    graph_exec = nullptr;
+    if (stream) cudaStreamSynchronize(stream);
+#endif
     for (int i = 0; i < cap; ++i) free_slot(i);
     for (auto& pl : lists)
       for (auto& l : pl) dfree(l.d);
     dfree(d_slots);
     dfree(d_ctl);
     plans.release();
+#if !defined(OFDFT_EMU)
+    if (stream) cudaStreamDestroy(stream);
+    stream = nullptr;
+#endif
   }
 
   void free_slot(int i) {
     HostSlot& h = slots[i];
     for (void* p : h.allocs) dfree(p);
     h.allocs.clear();
+    if (h.d_stencil) dfree(h.d_stencil);
+    h.d_stencil = nullptr;
+    h.nion = 0;
     h.used = false;
     h.running = false;
     dirty = true;
@@ -287,6 +352,11 @@ struct Engine {
       for (int r = 0; r < 3; ++r) s.recip[3 * c + r] = inv[c][r] * twopi;
     s.vol = std::fabs(det);
     s.dv = s.vol / (double)s.N;
+    for (int k = 0; k < 9; ++k) h.lattice[k] = L[k];
+    for (int r = 0; r < 3; ++r)
+      for (int c2 = 0; c2 < 3; ++c2) h.cell_inv_t[3 * r + c2] = inv[c2][r];
+    h.rho0 = d->rho0;
+    h.gamma = d->gamma;
     s.inv_n = 1.0 / (double)s.N;
     s.kinetic = d->kinetic;
     s.lambda = d->lambda;
@@ -296,6 +366,7 @@ struct Engine {
     s.rho_s = d->rho_s;
     s.ion_ion = d->ion_ion_energy;
     s.alpha_eq_beta = (d->alpha == d->beta) ? 1 : 0;
+    s.pow56 = (s.alpha_eq_beta && std::fabs(d->alpha - 5.0 / 6.0) < 1e-15) ? 1 : 0;
     if (s.kinetic == KIN_WT) {
       s.nf = s.alpha_eq_beta ? 3 : 4;
       s.ngroups = s.nf;
@@ -314,10 +385,17 @@ struct Engine {
     // launch geometry
     const long long nrows = (long long)s.n2 * s.n3;
     h.nrowpairs = (int)((nrows + 1) / 2);
-    h.rp = std::max(1, std::min(16, 512 / s.n1));
-    h.tx = h.prec == OFDFT_FP32 ? 16 : 8;
+    const size_t csz = 2 * elem_size(h.prec);
+    // tile sizes: about 1-2 K complex points per block, at most ~100 KB of shared memory
+    h.rp1 = std::max(1, std::min(32, 2048 / s.n1));
+    while (h.rp1 > 1 && 2 * (size_t)h.rp1 * s.n1 * csz > 100 * 1024) h.rp1--;
+    s.rp = std::max(1, std::min(32, 1024 / s.n1));
+    while (s.rp > 1 && 2 * (size_t)s.nf * s.rp * s.n1 * csz > 72 * 1024) s.rp--;
+    const int gmax = s.kinetic == KIN_WGC ? 3 : 1;
+    s.tx = 16;
+    while (s.tx > 2 && 2 * (size_t)gmax * s.tx * std::max(s.n2, s.n3) * csz > 100 * 1024) s.tx /= 2;
     s.ntask[K_VEC] = (int)((s.N + VCHUNK - 1) / VCHUNK);
-    s.ntask[K_X5] = (h.nrowpairs + h.rp - 1) / h.rp;
+    s.ntask[K_X5] = (h.nrowpairs + s.rp - 1) / s.rp;
     // buffers
     const size_t es = elem_size(h.prec);
     int rc;
@@ -328,7 +406,6 @@ struct Engine {
     if ((rc = alloc(h, &s.spec, 2 * es * s.Nc * s.nf))) { free_slot(idx); return rc; }
     const int ntmax = std::max(s.ntask[K_VEC], s.ntask[K_X5]);
     if ((rc = alloc(h, (void**)&s.partials, sizeof(double) * NCH * ntmax))) { free_slot(idx); return rc; }
-    if ((rc = alloc(h, (void**)&s.done, sizeof(int) * NKID))) { free_slot(idx); return rc; }
     if ((rc = alloc(h, (void**)&s.hist, sizeof(HistEntry) * HIST_MAX))) { free_slot(idx); return rc; }
     if ((rc = upload_slot(idx))) { free_slot(idx); return rc; }
     Ctl c;
@@ -337,6 +414,239 @@ struct Engine {
     if ((rc = h2d(d_ctl + idx, &c, sizeof(Ctl)))) { free_slot(idx); return rc; }
     dirty = true;
     *out = idx;
+    return OFDFT_OK;
+  }
+
+  // ---------------------------------------------------------- set-up on the device
+  int sync_stream() {
+#if defined(OFDFT_EMU)
+    return OFDFT_OK;
+#else
+    return cuda_check(cudaStreamSynchronize(stream), "stream synchronize");
+#endif
+  }
+
+  int launch_fill(int i, const KernArgs& ka, int kind) {
+    HostSlot& h = slots[i];
+#if defined(OFDFT_EMU)
+    for (int idx = 0; idx < (int)h.sd.Nc; ++idx) {
+      if (h.prec == OFDFT_FP32) fill_kernel_point<float>(h.sd, ka, kind, idx);
+      else fill_kernel_point<double>(h.sd, ka, kind, idx);
+    }
+    return OFDFT_OK;
+#else
+    const int blocks = (int)std::min<long long>(4096, (h.sd.Nc + 255) / 256);
+    if (h.prec == OFDFT_FP32) k_fill_kernel<float><<<blocks, 256, 0, stream>>>(d_slots + i, ka, kind);
+    else k_fill_kernel<double><<<blocks, 256, 0, stream>>>(d_slots + i, ka, kind);
+    int rc = cuda_check(cudaGetLastError(), "fill kernel launch");
+    return rc ? rc : sync_stream();
+#endif
+  }
+
+  int build_wt_kernel(int i) {
+    int rc = check_slot(i);
+    if (rc) return rc;
+    HostSlot& h = slots[i];
+    const SlotDev& s = h.sd;
+    if (s.kinetic != KIN_WT) return fail(OFDFT_EINVAL, "the slot's functional is not WT");
+    if (!(h.rho0 > 0)) return fail(OFDFT_EINVAL, "rho0 must be positive to build the WT kernel");
+    KernArgs ka;
+    memset(&ka, 0, sizeof(ka));
+    lind_series(ka.ser);
+    ka.lam = s.lambda;
+    ka.mu = s.mu;
+    ka.coef = 5.0 / (9.0 * s.alpha * s.beta * std::pow(h.rho0, s.alpha + s.beta - 5.0 / 3.0));
+    ka.tkf = 2.0 * std::pow(3.0 * h.rho0 * PI_D * PI_D, 1.0 / 3.0);
+    return launch_fill(i, ka, KIN_WT);
+  }
+
+  int build_wgc_kernel(int i, int ntab, const double* eta, const double* w, const double* w1, const double* w2) {
+    int rc = check_slot(i);
+    if (rc) return rc;
+    HostSlot& h = slots[i];
+    const SlotDev& s = h.sd;
+    if (s.kinetic != KIN_WGC) return fail(OFDFT_EINVAL, "the slot's functional is not WGC");
+    if (!(s.rho_s > 0)) return fail(OFDFT_EINVAL, "rho_s must be positive to build the WGC kernel");
+    std::vector<double> te, tw, tw1, tw2;
+    if (ntab > 1 && eta && w && w1 && w2) {
+      te.assign(eta, eta + ntab);
+      tw.assign(w, w + ntab);
+      tw1.assign(w1, w1 + ntab);
+      tw2.assign(w2, w2 + ntab);
+    } else if (wgc_radial_tables(s.alpha, s.beta, h.gamma, te, tw, tw1, tw2)) {
+      return fail(OFDFT_EINVAL, "WGC kernel ODE did not converge");
+    }
+    const int n = (int)te.size();
+    std::vector<double> tab(7 * (size_t)n);
+    std::vector<double> pp = spline_cubic_set(te, tw, 0, 0.0, 0, 0.0);
+    std::vector<double> pp1 = spline_cubic_set(te, tw1, 0, 0.0, 0, 0.0);
+    std::vector<double> pp2 = spline_cubic_set(te, tw2, 0, 0.0, 0, 0.0);
+    for (int k = 0; k < n; ++k) {
+      tab[k] = te[k]; tab[n + k] = tw[k]; tab[2 * n + k] = tw1[k]; tab[3 * n + k] = tw2[k];
+      tab[4 * n + k] = pp[k]; tab[5 * n + k] = pp1[k]; tab[6 * n + k] = pp2[k];
+    }
+    double* dtab = nullptr;
+    if ((rc = dmalloc((void**)&dtab, sizeof(double) * tab.size()))) return rc;
+    if ((rc = h2d(dtab, tab.data(), sizeof(double) * tab.size()))) { dfree(dtab); return rc; }
+    KernArgs ka;
+    memset(&ka, 0, sizeof(ka));
+    ka.rho_s = s.rho_s;
+    ka.gamma = h.gamma;
+    ka.tkf = 2.0 * std::pow(3.0 * PI_D * PI_D * s.rho_s, 1.0 / 3.0);
+    ka.ntab = n;
+    ka.tab = dtab;
+    rc = launch_fill(i, ka, KIN_WGC);
+    dfree(dtab);
+    return rc;
+  }
+
+  int build_ion_potential(int i, int nion, const double* frac, const int* species, int nspec, const int* npts,
+                          const double* max_g, const double* charge, const double* pot_values, const double* vqs,
+                          const double* pot_dd) {
+    int rc = check_slot(i);
+    if (rc) return rc;
+    HostSlot& h = slots[i];
+    SlotDev& s = h.sd;
+    if (nion < 1 || nspec < 1 || nspec > MAX_SPECIES || nspec > s.nf)
+      return fail(OFDFT_EINVAL, "bad ion or species count for this slot");
+    std::vector<double> tab;
+    IonAux ax;
+    memset(&ax, 0, sizeof(ax));
+    ax.nspec = nspec;
+    int off_in = 0;
+    for (int sp = 0; sp < nspec; ++sp) {
+      if (npts[sp] < 4) return fail(OFDFT_EINVAL, "pseudopotential table too short");
+      PspDev& p = ax.psp[sp];
+      p.npts = npts[sp];
+      p.off = (int)tab.size();
+      p.max_g = max_g[sp];
+      p.charge = charge[sp];
+      p.v0 = pot_values[off_in];
+      p.dq = max_g[sp] / (double)(npts[sp] - 1);
+      tab.insert(tab.end(), vqs + off_in, vqs + off_in + npts[sp]);
+      tab.insert(tab.end(), pot_dd + off_in, pot_dd + off_in + npts[sp]);
+      off_in += npts[sp];
+    }
+    for (int k = 0; k < nion; ++k)
+      if (species[k] < 0 || species[k] >= nspec) return fail(OFDFT_EINVAL, "ion species index out of range");
+    const std::vector<cx<double>> b1 = bspline_b(s.k1, s.n1), b2 = bspline_b(s.n2, s.n2), b3 = bspline_b(s.n3, s.n3);
+    const size_t bytes = sizeof(double) * tab.size() + sizeof(cx<double>) * (b1.size() + b2.size() + b3.size());
+    void* aux = nullptr;
+    if ((rc = alloc(h, &aux, bytes))) return rc;
+    char* cur = (char*)aux;
+    if ((rc = h2d(cur, tab.data(), sizeof(double) * tab.size()))) return rc;
+    ax.tab = (const double*)cur;
+    cur += sizeof(double) * tab.size();
+    if ((rc = h2d(cur, b1.data(), sizeof(cx<double>) * b1.size()))) return rc;
+    ax.b1 = (const cx<double>*)cur;
+    cur += sizeof(cx<double>) * b1.size();
+    if ((rc = h2d(cur, b2.data(), sizeof(cx<double>) * b2.size()))) return rc;
+    ax.b2 = (const cx<double>*)cur;
+    cur += sizeof(cx<double>) * b2.size();
+    if ((rc = h2d(cur, b3.data(), sizeof(cx<double>) * b3.size()))) return rc;
+    ax.b3 = (const cx<double>*)cur;
+    s.ion = ax;
+    if ((rc = upload_slot(i))) return rc;
+    // ion stencils (kept for the forces)
+    const int nn[3] = {s.n1, s.n2, s.n3};
+    h.stencils.clear();
+    h.frac.assign(frac, frac + 3 * nion);
+    h.zion.resize(nion);
+    for (int k = 0; k < nion; ++k) {
+      h.stencils.push_back(ion_stencil(frac + 3 * k, species[k], nn));
+      h.zion[k] = charge[species[k]];
+    }
+    if (h.nion != nion) {
+      if (h.d_stencil) dfree(h.d_stencil);
+      h.d_stencil = nullptr;
+      if ((rc = dmalloc((void**)&h.d_stencil, sizeof(IonStencil) * nion))) return rc;
+      h.nion = nion;
+    }
+    if ((rc = h2d(h.d_stencil, h.stencils.data(), sizeof(IonStencil) * nion))) return rc;
+    const size_t es = elem_size(h.prec);
+    for (int sp = 0; sp < nspec; ++sp)
+      if ((rc = dzero(s.buf[B_PHI + sp], es * s.N))) return rc;
+#if defined(OFDFT_EMU)
+    for (int k = 0; k < nion; ++k)
+      for (int w = 0; w < SPLINE_ORDER * SPLINE_ORDER * SPLINE_ORDER; ++w) {
+        if (h.prec == OFDFT_FP32) spread_ion<float>(s, h.stencils[k], w);
+        else spread_ion<double>(s, h.stencils[k], w);
+      }
+#else
+    if (h.prec == OFDFT_FP32) k_spread<float><<<nion, 256, 0, stream>>>(d_slots + i, h.d_stencil);
+    else k_spread<double><<<nion, 256, 0, stream>>>(d_slots + i, h.d_stencil);
+    if ((rc = cuda_check(cudaGetLastError(), "spread launch"))) return rc;
+    if ((rc = sync_stream())) return rc;
+#endif
+    Ctl c;
+    base_ctl(c, h.prec);
+    c.ev = EV_ION;
+    if ((rc = put_ctl(i, c))) return rc;
+    return run_one(i);
+  }
+
+  // Run a slot that needs a single evaluation tick.
+  int run_one(int i) {
+    slots[i].running = true;
+    dirty = true;
+    int running = 0;
+    int rc = run(4, &running, 1);
+    if (rc) return rc;
+    if (slots[i].running) return fail(OFDFT_ETIMEOUT, "set-up pass did not finish");
+    Ctl c;
+    if ((rc = get_ctl(i, c))) return rc;
+    return c.status == ST_DONE ? OFDFT_OK : fail(OFDFT_ENAN, "set-up pass failed");
+  }
+
+  int forces(int i, const double* rho, int include_ewald, double* out) {
+    int rc = check_slot(i);
+    if (rc) return rc;
+    HostSlot& h = slots[i];
+    SlotDev& s = h.sd;
+    if (h.nion < 1 || s.ion.nspec < 1) return fail(OFDFT_EINVAL, "build the ion potential before the forces");
+    Ctl c;
+    if ((rc = get_ctl(i, c))) return rc;
+    const int iphi = c.status == ST_IDLE ? B_PHI : c.iphi;
+    base_ctl(c, h.prec);
+    c.iphi = iphi;
+    c.ev = EV_FORCE;
+    c.ca = 1.0;
+    c.cb = 0.0;
+    if (rho) {
+      if ((rc = upload_real(h.prec, s.buf[B_PHI], rho, s.N))) return rc;
+      c.iphi = B_PHI;
+      c.force_rho = 1;
+    }
+    if ((rc = put_ctl(i, c))) return rc;
+    if ((rc = run_one(i))) return rc;
+    std::vector<double> q(3 * (size_t)h.nion, 0.0);
+#if defined(OFDFT_EMU)
+    for (int k = 0; k < h.nion; ++k)
+      for (int w = 0; w < SPLINE_ORDER * SPLINE_ORDER * SPLINE_ORDER; ++w) {
+        if (h.prec == OFDFT_FP32) force_term<float>(s, h.stencils[k], w, &q[3 * k]);
+        else force_term<double>(s, h.stencils[k], w, &q[3 * k]);
+      }
+#else
+    double* dq = nullptr;
+    if ((rc = dmalloc((void**)&dq, sizeof(double) * q.size()))) return rc;
+    if (h.prec == OFDFT_FP32) k_force_gather<float><<<h.nion, 256, 0, stream>>>(d_slots + i, h.d_stencil, dq);
+    else k_force_gather<double><<<h.nion, 256, 0, stream>>>(d_slots + i, h.d_stencil, dq);
+    rc = cuda_check(cudaGetLastError(), "force gather launch");
+    if (!rc) rc = sync_stream();
+    if (!rc) rc = d2h(q.data(), dq, sizeof(double) * q.size());
+    dfree(dq);
+    if (rc) return rc;
+#endif
+    // F_ie = -cellInv * sum(qIonDeriv * Factor) (CalculateSplineForces)
+    for (int k = 0; k < h.nion; ++k)
+      for (int r = 0; r < 3; ++r)
+        out[3 * k + r] = -(h.cell_inv_t[3 * r] * q[3 * k] + h.cell_inv_t[3 * r + 1] * q[3 * k + 1] +
+                           h.cell_inv_t[3 * r + 2] * q[3 * k + 2]);
+    if (include_ewald) {
+      std::vector<double> fii(3 * (size_t)h.nion);
+      ewald(h.lattice, h.nion, h.frac.data(), h.zion.data(), fii.data());
+      for (size_t k = 0; k < fii.size(); ++k) out[k] += fii[k];
+    }
     return OFDFT_OK;
   }
 
@@ -431,28 +741,32 @@ struct Engine {
       const size_t cs = 2 * elem_size(h.prec);
       for (int t = 0; t < s.ntask[K_VEC]; ++t) L[P_VEC].h.push_back({i, t, 0, 0});
       L[P_VEC].nthr = 256;
-      L[P_VEC].smem = std::max(L[P_VEC].smem, (size_t)(NCH * 256 * sizeof(double) + 16));
+      L[P_VEC].smem = std::max(L[P_VEC].smem, (size_t)(NCH * 33 * sizeof(double) + 16));
       for (int f = 0; f < s.nf; ++f)
-        for (int r = 0; r < h.nrowpairs; r += h.rp)
-          L[P_X1].h.push_back({i, f, r, std::min(h.rp, h.nrowpairs - r)});
-      L[P_X1].nthr = 128;
-      L[P_X1].smem = std::max(L[P_X1].smem, 2 * (size_t)h.rp * s.n1 * cs);
+        for (int r = 0; r < h.nrowpairs; r += h.rp1)
+          L[P_X1].h.push_back({i, f, r, std::min(h.rp1, h.nrowpairs - r)});
+      L[P_X1].nthr = 256;
+      L[P_X1].smem = std::max(L[P_X1].smem, 2 * (size_t)h.rp1 * s.n1 * cs);
       for (int pass : {P_Y2, P_Y4}) {
         for (int f = 0; f < s.nf; ++f)
           for (int z = 0; z < s.n3; ++z)
-            for (int kx = 0; kx < s.k1; kx += h.tx) L[pass].h.push_back({i, f, z, kx});
-        L[pass].nthr = 128;
-        L[pass].smem = std::max(L[pass].smem, 2 * (size_t)h.tx * s.n2 * cs);
+            for (int kx = 0; kx < s.k1; kx += s.tx) L[pass].h.push_back({i, f, z, kx});
+        L[pass].nthr = 256;
+        L[pass].smem = std::max(L[pass].smem, 2 * (size_t)s.tx * s.n2 * cs);
       }
+      const int gmax = s.kinetic == KIN_WGC ? 3 : 1;
       for (int g = 0; g < s.ngroups; ++g)
         for (int ky = 0; ky < s.n2; ++ky)
-          for (int kx = 0; kx < s.k1; kx += h.tx) L[P_Z3].h.push_back({i, g, ky, kx});
-      L[P_Z3].nthr = 128;
-      L[P_Z3].smem = std::max(L[P_Z3].smem, 4 * (size_t)h.tx * s.n3 * cs);
+          for (int kx = 0; kx < s.k1; kx += s.tx) L[P_Z3].h.push_back({i, g, ky, kx});
+      L[P_Z3].nthr = 256;
+      L[P_Z3].smem = std::max(L[P_Z3].smem, 2 * (size_t)std::max(gmax, s.ion.nspec) * s.tx * s.n3 * cs);
       int ord = 0;
-      for (int r = 0; r < h.nrowpairs; r += h.rp) L[P_X5].h.push_back({i, r, std::min(h.rp, h.nrowpairs - r), ord++});
-      L[P_X5].nthr = 128;
-      L[P_X5].smem = std::max(L[P_X5].smem, (size_t)(s.nf + 1) * h.rp * s.n1 * cs + NCH * 128 * sizeof(double) + 16);
+      for (int r = 0; r < h.nrowpairs; r += s.rp) L[P_X5].h.push_back({i, r, std::min(s.rp, h.nrowpairs - r), ord++});
+      L[P_CTL].h.push_back({i, 0, 0, 0});
+      L[P_CTL].nthr = 64;
+      L[P_CTL].smem = 0;
+      L[P_X5].nthr = 256;
+      L[P_X5].smem = std::max(L[P_X5].smem, 2 * (size_t)s.nf * s.rp * s.n1 * cs + NCH * 33 * sizeof(double) + 16);
     }
 #if defined(OFDFT_EMU)
     for (int p = 0; p < 2; ++p)
@@ -485,7 +799,6 @@ struct Engine {
     a.ctl = d_ctl;
     a.tasks = lists[prec][pass].d;
     a.tw = (const cx<T>*)(prec == OFDFT_FP32 ? plans.d_tw32 : plans.d_tw64);
-    a.tx = prec == OFDFT_FP32 ? 16 : 8;
     a.vchunk = VCHUNK;
     return a;
   }
@@ -500,13 +813,17 @@ struct Engine {
       Args<T> a = args<T>(prec, pass);
       for (int b = 0; b < (int)l.h.size(); ++b) fn(a, b, emu_smem.data());
     };
-    for (int v = 0; v < VEC_PER_TICK; ++v)
+    static double ctl_sm[NCH * 33 + 2];
+    for (int v = 0; v < VEC_PER_TICK; ++v) {
       run(P_VEC, [](Args<T>& a, int b, char* sm) { vec_block<T>(a, b, 0, 1, sm); });
+      run(P_CTL, [](Args<T>& a, int b, char*) { ctl_block(a.slots, a.ctl, a.tasks, K_VEC, b, 0, 1, (char*)ctl_sm); });
+    }
     run(P_X1, [](Args<T>& a, int b, char* sm) { xfwd_block<T>(a, b, 0, 1, sm); });
     run(P_Y2, [](Args<T>& a, int b, char* sm) { ypass_block<T>(a, b, 0, 1, sm, -1); });
     run(P_Z3, [](Args<T>& a, int b, char* sm) { zpass_block<T>(a, b, 0, 1, sm); });
     run(P_Y4, [](Args<T>& a, int b, char* sm) { ypass_block<T>(a, b, 0, 1, sm, 1); });
     run(P_X5, [](Args<T>& a, int b, char* sm) { xinv_block<T>(a, b, 0, 1, sm); });
+    run(P_CTL, [](Args<T>& a, int b, char*) { ctl_block(a.slots, a.ctl, a.tasks, K_X5, b, 0, 1, (char*)ctl_sm); });
     return OFDFT_OK;
   }
 #else
@@ -514,53 +831,107 @@ struct Engine {
   int launch_one(int prec, int pass, K kern, X... extra) {
     LaunchList& l = lists[prec][pass];
     if (l.h.empty()) return OFDFT_OK;
-    if (l.smem > 48 * 1024) {
-      int rc = cuda_check(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)l.smem),
-                          "cudaFuncSetAttribute");
-      if (rc) return rc;
-    }
-    kern<<<(unsigned)l.h.size(), l.nthr, l.smem>>>(args<T>(prec, pass), extra...);
+    kern<<<(unsigned)l.h.size(), l.nthr, l.smem, stream>>>(args<T>(prec, pass), extra...);
     return cuda_check(cudaGetLastError(), "kernel launch");
   }
   template <typename T>
   int launch_prec(int prec) {
     int rc;
-    for (int v = 0; v < VEC_PER_TICK; ++v)
+    for (int v = 0; v < VEC_PER_TICK; ++v) {
       if ((rc = launch_one<T>(prec, P_VEC, k_vec<T>))) return rc;
+      if ((rc = launch_one<T>(prec, P_CTL, k_ctl<T>, (int)K_VEC))) return rc;
+    }
     if ((rc = launch_one<T>(prec, P_X1, k_xfwd<T>))) return rc;
     if ((rc = launch_one<T>(prec, P_Y2, k_ypass<T>, -1))) return rc;
     if ((rc = launch_one<T>(prec, P_Z3, k_zpass<T>))) return rc;
     if ((rc = launch_one<T>(prec, P_Y4, k_ypass<T>, 1))) return rc;
-    return launch_one<T>(prec, P_X5, k_xinv<T>);
+    if ((rc = launch_one<T>(prec, P_X5, k_xinv<T>))) return rc;
+    return launch_one<T>(prec, P_CTL, k_ctl<T>, (int)K_X5);
   }
 #endif
 
   int tick() {
     int rc;
-    if (dirty && (rc = build_lists())) return rc;
     if ((rc = launch_prec<double>(OFDFT_FP64))) return rc;
     return launch_prec<float>(OFDFT_FP32);
+  }
+
+#if !defined(OFDFT_EMU)
+  // Kernels whose dynamic shared memory exceeds the default 48 KB need the
+  // opt-in attribute; it must be set outside stream capture.
+  template <typename T>
+  int set_smem_attrs(int prec) {
+    int rc;
+    auto attr = [&](auto kern, int pass) -> int {
+      const size_t sm = lists[prec][pass].smem;
+      if (sm <= 48 * 1024) return OFDFT_OK;
+      return cuda_check(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm),
+                        "cudaFuncSetAttribute");
+    };
+    if ((rc = attr(k_vec<T>, P_VEC))) return rc;
+    if ((rc = attr(k_xfwd<T>, P_X1))) return rc;
+    if ((rc = attr(k_ypass<T>, P_Y2))) return rc;
+    if ((rc = attr(k_ypass<T>, P_Y4))) return rc;
+    if ((rc = attr(k_zpass<T>, P_Z3))) return rc;
+    return attr(k_xinv<T>, P_X5);
+  }
+
+  // Capture `nticks` ticks into one CUDA graph (re-captured when the set of
+  // running slots changes).
+  int capture(int nticks) {
+    if (graph_exec) {
+      cudaGraphExecDestroy(graph_exec);
+      graph_exec = nullptr;
+    }
+    int rc = set_smem_attrs<double>(OFDFT_FP64);
+    if (!rc) rc = set_smem_attrs<float>(OFDFT_FP32);
+    if (rc) return rc;
+    if ((rc = cuda_check(cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal), "begin capture")))
+      return rc;
+    for (int k = 0; k < nticks && rc == OFDFT_OK; ++k) rc = tick();
+    cudaGraph_t g = nullptr;
+    const int rc2 = cuda_check(cudaStreamEndCapture(stream, &g), "end capture");
+    if (rc) { if (g) cudaGraphDestroy(g); return rc; }
+    if (rc2) return rc2;
+    rc = cuda_check(cudaGraphInstantiate(&graph_exec, g, 0), "graph instantiate");
+    cudaGraphDestroy(g);
+    graph_ticks = nticks;
+    return rc;
+  }
+#endif
+
+  // Launch `n` ticks (through the captured graph when it covers n).
+  int launch_ticks(int n) {
+    int rc;
+    if (dirty) {
+      if ((rc = build_lists())) return rc;
+#if !defined(OFDFT_EMU)
+      if ((rc = capture(n))) return rc;
+#endif
+    }
+#if !defined(OFDFT_EMU)
+    if (graph_exec && graph_ticks == n) return cuda_check(cudaGraphLaunch(graph_exec, stream), "graph launch");
+#endif
+    for (int k = 0; k < n; ++k)
+      if ((rc = tick())) return rc;
+    return OFDFT_OK;
   }
 
   // Run ticks; after every `check` ticks read the slots' status and retire
   // finished slots from the task lists.
   int run(int ticks, int* running_out, int check = 8) {
     int running = 0;
+    std::vector<Ctl> cs(cap);
     for (int t = 0; t < ticks;) {
       int n = std::min(check, ticks - t);
-      for (int k = 0; k < n; ++k) {
-        int rc = tick();
-        if (rc) return rc;
-      }
-      t += n;
-      int rc = dsync();
+      int rc = launch_ticks(n);
       if (rc) return rc;
+      t += n;
+      if ((rc = d2h_stream(cs.data(), d_ctl, sizeof(Ctl) * cap))) return rc;
       running = 0;
       for (int i = 0; i < cap; ++i) {
         if (!slots[i].used || !slots[i].running) continue;
-        Ctl c;
-        if ((rc = get_ctl(i, c))) return rc;
-        if (c.status == ST_RUNNING) {
+        if (cs[i].status == ST_RUNNING) {
           ++running;
         } else {
           slots[i].running = false;
@@ -767,14 +1138,84 @@ int ofdft_proj_norm_rho_minimization(ofdft_engine* e, int slot, double* rho, dou
 int ofdft_slot_start_solve_from_slot(ofdft_engine*, int, int, const ofdft_ntn_options*) {
   return fail(OFDFT_EINVAL, "not available yet");
 }
-int ofdft_slot_build_wt_kernel(ofdft_engine*, int) { return fail(OFDFT_EINVAL, "not available yet"); }
-int ofdft_slot_build_wgc_kernel(ofdft_engine*, int, int, const double*, const double*, const double*,
-                                const double*) {
-  return fail(OFDFT_EINVAL, "not available yet");
+int ofdft_slot_build_wt_kernel(ofdft_engine* e, int slot) {
+  if (!e) return fail(OFDFT_EINVAL, "null engine");
+  return e->eng.build_wt_kernel(slot);
 }
-int ofdft_slot_build_ion_potential(ofdft_engine*, int, int, const double*, const int*, int, const int*,
-                                   const double*, const double*, const double*, const double*, const double*) {
-  return fail(OFDFT_EINVAL, "not available yet");
+
+int ofdft_slot_build_wgc_kernel(ofdft_engine* e, int slot, int ntab, const double* eta, const double* w,
+                                const double* w1, const double* w2) {
+  if (!e) return fail(OFDFT_EINVAL, "null engine");
+  return e->eng.build_wgc_kernel(slot, ntab, eta, w, w1, w2);
+}
+
+int ofdft_slot_build_ion_potential(ofdft_engine* e, int slot, int nion, const double* frac, const int* species,
+                                   int nspecies, const int* npts, const double* max_g, const double* charge,
+                                   const double* pot_values, const double* vqs, const double* pot_dd) {
+  if (!e || !frac || !species || !npts || !max_g || !charge || !pot_values || !vqs || !pot_dd)
+    return fail(OFDFT_EINVAL, "null argument");
+  return e->eng.build_ion_potential(slot, nion, frac, species, nspecies, npts, max_g, charge, pot_values, vqs,
+                                    pot_dd);
+}
+
+int ofdft_slot_forces(ofdft_engine* e, int slot, const double* rho, int include_ewald, double* forces) {
+  if (!e || !forces) return fail(OFDFT_EINVAL, "null argument");
+  return e->eng.forces(slot, rho, include_ewald, forces);
+}
+
+int ofdft_ewald(const double* lattice, int nion, const double* frac, const double* charges, double* energy,
+                double* forces) {
+  if (!lattice || !frac || !charges || !energy || nion < 1) return fail(OFDFT_EINVAL, "bad argument");
+  *energy = ewald(lattice, nion, frac, charges, forces);
+  return OFDFT_OK;
+}
+
+int ofdft_grid_size(double ecut_ha, const double* lattice, int* n) {
+  if (!lattice || !n || !(ecut_ha > 0)) return fail(OFDFT_EINVAL, "bad argument");
+  // SizeSystem / PadFFTdims (SetupFFT.f90:193-382), dimType 1
+  const double qmax = std::sqrt(ecut_ha * 2.0);
+  for (int a = 0; a < 3; ++a) {
+    const double len = std::sqrt(lattice[3 * a] * lattice[3 * a] + lattice[3 * a + 1] * lattice[3 * a + 1] +
+                                 lattice[3 * a + 2] * lattice[3 * a + 2]);
+    const double r = qmax * len / PI_D;
+    const double eps = 1.0e-14, lr = std::log(r);
+    const int p2 = (int)(lr / std::log(2.0) - eps + 1), p3 = (int)(lr / std::log(3.0) - eps + 1);
+    const int p5 = (int)(lr / std::log(5.0) - eps + 1), p7 = (int)(lr / std::log(7.0) - eps + 1);
+    long long best = 1;
+    for (int k = 0; k < p7; ++k) best *= 7;
+    for (int i7 = 0; i7 <= p7; ++i7)
+      for (int i5 = 0; i5 <= p5; ++i5)
+        for (int i3 = 0; i3 <= p3; ++i3)
+          for (int i2 = 0; i2 <= p2; ++i2) {
+            long long t = 1;
+            for (int k = 0; k < i7; ++k) t *= 7;
+            for (int k = 0; k < i5; ++k) t *= 5;
+            for (int k = 0; k < i3; ++k) t *= 3;
+            for (int k = 0; k < i2; ++k) t *= 2;
+            if ((double)t >= r) {
+              if (t < best) best = t;
+              break;
+            }
+          }
+    n[a] = (int)best;
+  }
+  return OFDFT_OK;
+}
+
+int ofdft_wgc_radial_tables(double alpha, double beta, double gamma, int max, double* eta, double* w, double* w1,
+                            double* w2, int* n) {
+  if (!n) return fail(OFDFT_EINVAL, "null argument");
+  std::vector<double> te, tw, tw1, tw2;
+  if (wgc_radial_tables(alpha, beta, gamma, te, tw, tw1, tw2)) return fail(OFDFT_EINVAL, "ODE did not converge");
+  *n = (int)te.size();
+  if (max < (int)te.size()) return OFDFT_OK;  // size query
+  for (size_t k = 0; k < te.size(); ++k) {
+    if (eta) eta[k] = te[k];
+    if (w) w[k] = tw[k];
+    if (w1) w1[k] = tw1[k];
+    if (w2) w2[k] = tw2[k];
+  }
+  return OFDFT_OK;
 }
 
 }  // extern "C"

@@ -4,11 +4,12 @@
 // one Stockham stage per radix.  Each stage reads R points at stride n/R,
 // multiplies by the stage twiddles, does a radix-R butterfly in registers and
 // writes the R outputs in self-sorting order, ping-ponging between two shared
-// buffers; a final copy brings the result back when the stage count is odd.
-// Many independent transforms of the same length are done together: element i
-// of transform b lives at buf[b*sb + i*si].  Work items (b, butterfly) are
-// spread over the block's threads with b fastest, so with sb == 1 consecutive
-// threads touch consecutive shared-memory words.
+// buffers; the caller reads the result from whichever buffer fft_batch
+// returns.  Many independent transforms of the same length are done together:
+// element i of transform b lives at buf[b + i*si].  Work items (b, butterfly)
+// are spread over the block's threads with b fastest, so consecutive threads
+// touch consecutive shared-memory words; the index arithmetic uses
+// multiply-high divisions by constants prepared on the host.
 //
 // Twiddles are precomputed on the host in long double and stored per plan:
 // stage s with span Ns (product of the earlier radices) and radix R uses
@@ -28,8 +29,26 @@ struct FftPlan {
   int R[FFT_MAX_STAGES];
   int Ns[FFT_MAX_STAGES];
   int tw[FFT_MAX_STAGES];  // offset of the stage's twiddles in the plan table
+  unsigned ns_magic[FFT_MAX_STAGES];  // ceil(2^20 / Ns): j / Ns == (j * magic) >> 20 for j < 2048
   int tw_base;             // offset of this plan in the global twiddle table
 };
+
+// Exact quotient j / d for 0 <= j < 2048 and 1 <= d <= 512 from magic = ceil(2^20 / d).
+HD int magic_div(int j, unsigned magic) { return (int)(((unsigned)j * magic) >> 20); }
+
+// Exact quotient w / d for 0 <= w < 2^24 and 1 <= d <= 4096 from m32 = ceil(2^32 / d)
+// (d = 1 is encoded as m32 = 0).
+HD int magic_div32(int w, unsigned m32) {
+  if (m32 == 0u) return w;
+#if defined(__CUDA_ARCH__)
+  return (int)__umulhi((unsigned)w, m32);
+#else
+  return (int)(((unsigned long long)(unsigned)w * m32) >> 32);
+#endif
+}
+HD unsigned magic32(int d) {
+  return d <= 1 ? 0u : (unsigned)((0x100000000ULL + (unsigned long long)d - 1) / (unsigned long long)d);
+}
 
 // cos/sin of 2*pi*k/R for the odd radices (mathematical constants).
 #define OFDFT_S3 0.8660254037844386467637232
@@ -141,18 +160,20 @@ template <typename T> struct Dft<T, 5> { static HD void run(cx<T>* v, int d) { d
 template <typename T> struct Dft<T, 7> { static HD void run(cx<T>* v, int d) { dft7(v, d); } };
 template <typename T> struct Dft<T, 8> { static HD void run(cx<T>* v, int d) { dft8(v, d); } };
 
-// One Stockham stage of radix R over nb transforms: src -> dst.
+// One Stockham stage of radix R over nb transforms: src -> dst.  Element i of
+// transform b is at [b + i*si] (si >= nb); mnb = magic32(nb).
 template <typename T, int R>
-HD void fft_stage_r(const cx<T>* src, cx<T>* dst, int nb, int sb, int si, int n, int Ns,
-                    const cx<T>* tw, int dir, int tid, int nthr) {
+HD void fft_stage_r(const cx<T>* __restrict__ src, cx<T>* __restrict__ dst, int nb, unsigned mnb, int si, int n,
+                    int Ns, unsigned magic, const cx<T>* __restrict__ tw, int dir, int tid, int nthr) {
   const int nbf = n / R;  // butterflies per transform
-  const int total = nb * nbf;
+  const int total = nbf * nb;
   for (int w = tid; w < total; w += nthr) {
-    const int b = w % nb;
-    const int j = w / nb;
-    const int kmod = j % Ns;
+    const int j = magic_div32(w, mnb);
+    const int b = w - j * nb;
+    const int jq = magic_div(j, magic);
+    const int kmod = j - jq * Ns;
     cx<T> v[R];
-    const cx<T>* s = src + b * sb;
+    const cx<T>* s = src + b;
 #pragma unroll
     for (int m = 0; m < R; ++m) v[m] = s[(j + m * nbf) * si];
     if (Ns > 1) {
@@ -165,50 +186,46 @@ HD void fft_stage_r(const cx<T>* src, cx<T>* dst, int nb, int sb, int si, int n,
       }
     }
     Dft<T, R>::run(v, dir);
-    cx<T>* d = dst + b * sb;
-    const int base = (j / Ns) * Ns * R + kmod;
+    cx<T>* d = dst + b;
+    const int base = jq * Ns * R + kmod;
 #pragma unroll
     for (int m = 0; m < R; ++m) d[(base + m * Ns) * si] = v[m];
   }
 }
 
 template <typename T>
-HD void fft_stage(const cx<T>* src, cx<T>* dst, int nb, int sb, int si, int n, int R, int Ns,
+HD void fft_stage(const cx<T>* src, cx<T>* dst, int nb, unsigned mnb, int si, int n, int R, int Ns, unsigned magic,
                   const cx<T>* tw, int dir, int tid, int nthr) {
   switch (R) {
-    case 2: fft_stage_r<T, 2>(src, dst, nb, sb, si, n, Ns, tw, dir, tid, nthr); break;
-    case 3: fft_stage_r<T, 3>(src, dst, nb, sb, si, n, Ns, tw, dir, tid, nthr); break;
-    case 4: fft_stage_r<T, 4>(src, dst, nb, sb, si, n, Ns, tw, dir, tid, nthr); break;
-    case 5: fft_stage_r<T, 5>(src, dst, nb, sb, si, n, Ns, tw, dir, tid, nthr); break;
-    case 7: fft_stage_r<T, 7>(src, dst, nb, sb, si, n, Ns, tw, dir, tid, nthr); break;
-    case 8: fft_stage_r<T, 8>(src, dst, nb, sb, si, n, Ns, tw, dir, tid, nthr); break;
+    case 2: fft_stage_r<T, 2>(src, dst, nb, mnb, si, n, Ns, magic, tw, dir, tid, nthr); break;
+    case 3: fft_stage_r<T, 3>(src, dst, nb, mnb, si, n, Ns, magic, tw, dir, tid, nthr); break;
+    case 4: fft_stage_r<T, 4>(src, dst, nb, mnb, si, n, Ns, magic, tw, dir, tid, nthr); break;
+    case 5: fft_stage_r<T, 5>(src, dst, nb, mnb, si, n, Ns, magic, tw, dir, tid, nthr); break;
+    case 7: fft_stage_r<T, 7>(src, dst, nb, mnb, si, n, Ns, magic, tw, dir, tid, nthr); break;
+    case 8: fft_stage_r<T, 8>(src, dst, nb, mnb, si, n, Ns, magic, tw, dir, tid, nthr); break;
     default: break;
   }
 }
 
 // Full transform of nb sequences held in buf (tmp is scratch of the same
-// layout).  dir = -1 forward, +1 inverse.  The result is left in buf.
-// Must be called by every thread of the block (it synchronises).
+// layout), element i of sequence b at [b + i*si].  dir = -1 forward, +1
+// inverse.  Returns the buffer (buf or tmp) holding the result.  Must be
+// called by every thread of the block.
 template <typename T>
-HD void fft_batch(cx<T>* buf, cx<T>* tmp, int nb, int sb, int si, const FftPlan& p,
-                  const cx<T>* twtab, int dir, int tid, int nthr) {
+HD cx<T>* fft_batch(cx<T>* buf, cx<T>* tmp, int nb, int si, const FftPlan& p,
+                    const cx<T>* twtab, int dir, int tid, int nthr) {
   cx<T>* a = buf;
   cx<T>* b = tmp;
+  const unsigned mnb = magic32(nb);
   for (int s = 0; s < p.nst; ++s) {
-    fft_stage(a, b, nb, sb, si, p.n, p.R[s], p.Ns[s], twtab + p.tw_base + p.tw[s], dir, tid, nthr);
+    fft_stage(a, b, nb, mnb, si, p.n, p.R[s], p.Ns[s], p.ns_magic[s], twtab + p.tw_base + p.tw[s], dir, tid,
+              nthr);
     BLOCK_SYNC();
     cx<T>* t = a;
     a = b;
     b = t;
   }
-  if (a != buf) {
-    const int total = nb * p.n;
-    for (int w = tid; w < total; w += nthr) {
-      const int bb = w % nb, i = w / nb;
-      buf[bb * sb + i * si] = a[bb * sb + i * si];
-    }
-    BLOCK_SYNC();
-  }
+  return a;
 }
 
 }  // namespace ofdft

@@ -122,6 +122,11 @@ HDNI inline void ntn_after(Ctl& c, const SlotDev& s, const double* red, int kid,
         ctl_energy(c, s, red);
         ctl_finish(c, ST_DONE, ERR_NONE);
         return;
+      case EV_ION:
+      case EV_FORCE:
+        c.num_evals--;
+        ctl_finish(c, ST_DONE, ERR_NONE);
+        return;
       case EV_PHI:  // first evaluation of ProjNormRhoMinimization (RhoOptN.f90:357-362)
         ctl_energy(c, s, red);
         c.mu = s.dv * red[CH_M0] / (2.0 * c.tot_ele);

@@ -12,22 +12,14 @@
 //                       real-space epilogue (potential, chain rule, energies and
 //                       the optimiser's fused sums)
 //
-// Every block processes one task.  Blocks that finish a slot's work in the
-// vector kernel or in pass 5 add their per-channel partial sums to the slot's
-// partials; the last of them reduces the partials in a fixed order (the result
+// Every block processes one task.  Blocks of the vector kernel and of pass 5
+// store their per-channel sums in the slot's partials; a controller kernel
+// that follows (one block per slot) reduces them in a fixed order (the result
 // does not depend on block scheduling) and runs the NTN controller.
 #pragma once
 #include "ntn_ctl.cuh"
 
 namespace ofdft {
-
-#if defined(__CUDA_ARCH__)
-HD int atomic_inc(int* p) { return atomicAdd(p, 1); }
-HD void fence() { __threadfence(); }
-#else
-HD int atomic_inc(int* p) { int v = *p; *p = v + 1; return v; }
-HD void fence() {}
-#endif
 
 constexpr double PI_D = 3.141592653589793238462643;
 constexpr double C_TF = 2.87123400018819;  // Source/KEDF_TF.f90:42
@@ -38,52 +30,101 @@ struct Args {
   Ctl* ctl;
   const Task* tasks;
   const cx<T>* tw;
-  int tx;      // kx tile width of the Y/Z passes
   int vchunk;  // points per task of the vector kernel
 };
 
+// V_loc(|q|) by the index-knot cubic spline (PspRecipCubicSpline, LocalPseudoPot.f90:92-202).
+HD double psp_value(const IonAux& x, int sp, double q) {
+  const PspDev& p = x.psp[sp];
+  if (q == 0.0) return p.v0;
+  if (q >= p.max_g) return 0.0;
+  const double pos = q / p.dq + 1.0;
+  const int left = (int)floor(pos);
+  const double dt = pos - (double)left;
+  const double* vqs = x.tab + p.off;
+  const double* pdd = x.tab + p.off + p.npts;
+  const double yl = vqs[left - 1], yr = vqs[left];
+  const double pl = pdd[left - 1], pr = pdd[left];
+  const double yval = yl + dt * (yr - yl - (pr / 6.0 + pl / 3.0) + dt * (0.5 * pl + dt * ((pr - pl) / 6.0)));
+  return yval - 4.0 * PI_D * p.charge / (q * q);
+}
+
 // ------------------------------------------------------------ reductions
-// Reduce acc[NCH] over the block into sred[0*nthr], sred[1*nthr], ...
+// Reduce acc[NCH] over the block; the block totals end up in sred[0..NCH-1].
+// On the device: warp shuffles, then one warp over the per-warp sums (sred
+// needs NCH * 33 doubles).  In the host emulation the block has one thread.
 HDNI inline void block_reduce(double* sred, const double* acc, int tid, int nthr) {
-  for (int ch = 0; ch < NCH; ++ch) sred[ch * nthr + tid] = acc[ch];
-  BLOCK_SYNC();
-  for (int stride = nthr / 2; stride > 0; stride >>= 1) {
-    for (int w = tid; w < NCH * stride; w += nthr) {
-      const int ch = w / stride, i = w % stride;
-      sred[ch * nthr + i] += sred[ch * nthr + i + stride];
+#if defined(__CUDA_ARCH__)
+  const int lane = tid & 31, warp = tid >> 5, nw = (nthr + 31) >> 5;
+  double v[NCH];
+#pragma unroll
+  for (int ch = 0; ch < NCH; ++ch) {
+    double x = acc[ch];
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) x += __shfl_down_sync(0xffffffffu, x, o);
+    v[ch] = x;
+  }
+  if (lane == 0) {
+#pragma unroll
+    for (int ch = 0; ch < NCH; ++ch) sred[NCH + ch * 32 + warp] = v[ch];
+  }
+  __syncthreads();
+  if (warp == 0) {
+#pragma unroll
+    for (int ch = 0; ch < NCH; ++ch) {
+      double x = lane < nw ? sred[NCH + ch * 32 + lane] : 0.0;
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) x += __shfl_down_sync(0xffffffffu, x, o);
+      if (lane == 0) sred[ch] = x;
     }
-    BLOCK_SYNC();
+  }
+  __syncthreads();
+#else
+  (void)tid;
+  (void)nthr;
+  for (int ch = 0; ch < NCH; ++ch) sred[ch] = acc[ch];
+#endif
+}
+
+// Store this task's per-channel sums in the slot's partials.
+HDNI inline void store_partials(SlotDev& s, int task_idx, const double* acc, double* sred, int tid, int nthr) {
+  block_reduce(sred, acc, tid, nthr);
+  if (tid == 0) {
+#pragma unroll
+    for (int ch = 0; ch < NCH; ++ch) s.partials[(size_t)task_idx * NCH + ch] = sred[ch];
   }
 }
 
-// Store this task's partials; the last task of the slot reduces them and runs
-// the controller.  kid selects the done counter; what is the op / eval mode.
-HDNI inline void slot_finish(SlotDev& s, Ctl& c, int kid, int what, int task_idx, const double* acc,
-                             double* sred, int* sflag, int tid, int nthr) {
-  block_reduce(sred, acc, tid, nthr);
-  for (int ch = tid; ch < NCH; ch += nthr) s.partials[(long long)task_idx * NCH + ch] = sred[ch * nthr];
-  BLOCK_SYNC();
-  if (tid == 0) {
-    fence();
-    const int prev = atomic_inc(&s.done[kid]);
-    *sflag = (prev == s.ntask[kid] - 1) ? 1 : 0;
-  }
-  BLOCK_SYNC();
-  if (*sflag == 0) return;
-  fence();
+// Controller kernel body, one block per running slot: reduce the partials
+// of the work kernel that just ran (in a fixed order, independent of block
+// scheduling) and advance the slot's NTN state machine.  kid = K_VEC after the
+// vector kernel, K_X5 after pass 5.
+HDNI inline void ctl_block(SlotDev* slots, Ctl* ctls, const Task* tasks, int kid, int bid, int tid, int nthr,
+                           char* smem) {
+  const int si = tasks[bid].slot;
+  SlotDev& s = slots[si];
+  Ctl& c = ctls[si];
+  if (c.status != ST_RUNNING) return;
+  const int what = kid == K_VEC ? c.op : c.ev;
+  if (what == 0) return;
+  double* sred = (double*)smem;
   const int nt = s.ntask[kid];
   double part[NCH];
+#pragma unroll
   for (int ch = 0; ch < NCH; ++ch) part[ch] = 0.0;
-  for (int t = tid; t < nt; t += nthr)
-    for (int ch = 0; ch < NCH; ++ch) part[ch] += s.partials[(long long)t * NCH + ch];
+  for (int t = tid; t < nt; t += nthr) {
+#pragma unroll
+    for (int ch = 0; ch < NCH; ++ch) part[ch] += s.partials[(size_t)t * NCH + ch];
+  }
   block_reduce(sred, part, tid, nthr);
   if (tid == 0) {
     double red[NCH];
-    for (int ch = 0; ch < NCH; ++ch) red[ch] = sred[ch * nthr];
-    s.done[kid] = 0;
-    ntn_after(c, s, red, kid, what);
+#pragma unroll
+    for (int ch = 0; ch < NCH; ++ch) red[ch] = sred[ch];
+    Ctl local = c;
+    ntn_after(local, s, red, kid, what);
+    c = local;
   }
-  BLOCK_SYNC();
 }
 
 // ------------------------------------------------------------ vector ops
@@ -94,37 +135,40 @@ HDNI void vec_block(const Args<T>& a, int bid, int tid, int nthr, char* smem) {
   Ctl& c = a.ctl[t.slot];
   const int op = c.op;
   if (c.status != ST_RUNNING || op == OP_NONE) return;
-  T* phi = (T*)s.buf[c.iphi];
-  T* w0 = (T*)s.buf[c.iw0];
-  T* w1 = (T*)s.buf[c.iw1];
-  T* bb = (T*)s.buf[B_B];
-  T* r = (T*)s.buf[B_R];
-  T* p = (T*)s.buf[B_P];
-  T* d = (T*)s.buf[B_D];
+  T* __restrict__ phi = (T*)s.buf[c.iphi];
+  const T* __restrict__ w0 = (const T*)s.buf[c.iw0];
+  const T* __restrict__ w1 = (const T*)s.buf[c.iw1];
+  T* __restrict__ bb = (T*)s.buf[B_B];
+  T* __restrict__ r = (T*)s.buf[B_R];
+  T* __restrict__ p = (T*)s.buf[B_P];
+  T* __restrict__ d = (T*)s.buf[B_D];
   const T k = (T)c.opc;
-  const long long i0 = (long long)t.a * a.vchunk;
-  long long i1 = i0 + a.vchunk;
-  if (i1 > s.N) i1 = s.N;
+  const int i0 = t.a * a.vchunk;
+  const int n = (int)s.N;
+  const int i1 = i0 + a.vchunk < n ? i0 + a.vchunk : n;
   double acc[NCH];
+#pragma unroll
   for (int ch = 0; ch < NCH; ++ch) acc[ch] = 0.0;
-  for (long long i = i0 + tid; i < i1; i += nthr) {
-    switch (op) {
-      case OP_SQRT_INIT: {
+  switch (op) {
+    case OP_SQRT_INIT:
+      for (int i = i0 + tid; i < i1; i += nthr) {
         const T rho = phi[i];
         acc[0] += (double)rho;
         phi[i] = m_sqrt(rho < T(0) ? -rho : rho);
-        break;
       }
-      case OP_DLDPHI: {
+      break;
+    case OP_DLDPHI:
+      for (int i = i0 + tid; i < i1; i += nthr) {
         const T v = w0[i] - k * T(2) * phi[i];
         bb[i] = v;
         r[i] = -v;
         p[i] = -v;
         d[i] = T(0);
         acc[0] += (double)v * (double)v;
-        break;
       }
-      case OP_CGSTEP: {
+      break;
+    case OP_CGSTEP:
+      for (int i = i0 + tid; i < i1; i += nthr) {
         const T dn = d[i] + k * p[i];
         const T rn = r[i] - k * w1[i];
         d[i] = dn;
@@ -134,17 +178,19 @@ HDNI void vec_block(const Args<T>& a, int bid, int tid, int nthr, char* smem) {
         acc[0] += (double)rn * (double)rn;
         acc[1] += (double)pd * (double)pd;
         acc[2] += (double)f * (double)dn;
-        break;
       }
-      case OP_PUPD: {
+      break;
+    case OP_PUPD:
+      for (int i = i0 + tid; i < i1; i += nthr) {
         const T pn = r[i] + k * p[i];
         p[i] = pn;
         acc[0] += (double)pn * (double)pn;
-        break;
       }
-      case OP_DIRNEG:
-      case OP_NG1:
-      case OP_SD: {
+      break;
+    case OP_DIRNEG:
+    case OP_NG1:
+    case OP_SD:
+      for (int i = i0 + tid; i < i1; i += nthr) {
         T dn;
         if (op == OP_DIRNEG) dn = -(d[i] - k * p[i]);
         else if (op == OP_SD) dn = -bb[i];
@@ -154,60 +200,98 @@ HDNI void vec_block(const Args<T>& a, int bid, int tid, int nthr, char* smem) {
         const T pd = f + dn;
         acc[1] += (double)pd * (double)pd;
         acc[2] += (double)f * (double)dn;
-        break;
       }
-      case OP_NG2: {
+      break;
+    case OP_NG2:
+      for (int i = i0 + tid; i < i1; i += nthr) {
         const T dn = d[i] - phi[i] * k;
         d[i] = dn;
         acc[0] += (double)dn * (double)dn;
         acc[1] += (double)w0[i] * (double)dn;
-        break;
       }
-      default:
-        break;
+      break;
+    default:
+      break;
+  }
+  store_partials(s, t.a, acc, (double*)smem, tid, nthr);
+}
+
+// ------------------------------------------------------------ evaluation inputs
+// phi_in = ca * A + cb * B of the current evaluation (or rho itself for the
+// drop-in evaluation), held in registers for a whole block.
+template <typename T>
+struct EvalIn {
+  const T* __restrict__ A;
+  const T* __restrict__ B;
+  T ca, cb;
+  int rho_mode;
+  HD void at(int i, T& phin, T& rho, T& sq) const {
+    if (rho_mode) {
+      rho = A[i];
+      sq = m_sqrt(rho);
+      phin = sq;
+    } else {
+      phin = ca * A[i] + cb * B[i];
+      rho = phin * phin;
+      sq = phin < T(0) ? -phin : phin;  // sqrt(rho) = |phi_in|
     }
   }
-  double* sred = (double*)smem;
-  int* sflag = (int*)(sred + NCH * nthr);
-  slot_finish(s, c, K_VEC, op, t.a, acc, sred, sflag, tid, nthr);
+};
+
+template <typename T>
+HD EvalIn<T> eval_in(const SlotDev& s, const Ctl& c) {
+  EvalIn<T> e;
+  e.A = (const T*)s.buf[c.iphi];
+  e.B = (const T*)s.buf[c.evb];
+  e.ca = (T)c.ca;
+  e.cb = (T)c.cb;
+  e.rho_mode = (c.ev == EV_RHO || (c.ev == EV_FORCE && c.force_rho)) ? 1 : 0;
+  return e;
 }
 
-// ------------------------------------------------------------ fields
-// phi_in of the current evaluation at point i, and rho = phi_in^2.
+// Functional parameters of the real-space stages, in registers.
 template <typename T>
-HD void phi_in_at(const SlotDev& s, const Ctl& c, long long i, T& phin, T& rho) {
-  const T* A = (const T*)s.buf[c.iphi];
-  if (c.ev == EV_RHO) {
-    rho = A[i];
-    phin = m_sqrt(rho);
-    return;
-  }
-  const T* B = (const T*)s.buf[c.evb];
-  phin = (T)c.ca * A[i] + (T)c.cb * B[i];
-  rho = phin * phin;
+struct FieldPar {
+  int wt, pow56, aeqb, sum53;
+  T alpha, beta, rho_s;
+};
+
+template <typename T>
+HD FieldPar<T> field_par(const SlotDev& s) {
+  FieldPar<T> f;
+  f.wt = s.kinetic == KIN_WT;
+  f.pow56 = s.pow56;
+  f.aeqb = s.alpha_eq_beta;
+  f.sum53 = (s.alpha + s.beta - 5.0 / 3.0) < 1e-14 && (s.alpha + s.beta - 5.0 / 3.0) > -1e-14;
+  f.alpha = (T)s.alpha;
+  f.beta = (T)s.beta;
+  f.rho_s = (T)s.rho_s;
+  return f;
 }
 
-// Value of forward field f (see the field tables in the header comment of
-// SlotDev setup) at density rho.
+// Value of forward field f at density rho (sq = sqrt(rho)).  WT fields:
+// rho, rho^beta, sqrt(rho), rho^alpha.  WGC fields: rho, sqrt(rho), then for
+// x = alpha (f = 2..4) and x = beta (f = 5..7): rho^x, theta rho^x,
+// theta^2 rho^x / 2 with theta = rho - rho* (KEDF_WGC.f90:219-270).
 template <typename T>
-HD T field_value(const SlotDev& s, int f, T rho) {
-  if (s.kinetic == KIN_WT) {
+HD T field_value(const FieldPar<T>& fp, int f, T rho, T sq) {
+  if (fp.wt) {
     switch (f) {
       case 0: return rho;
-      case 1: return m_pow(rho, (T)s.beta);
-      case 2: return m_sqrt(rho);
-      default: return m_pow(rho, (T)s.alpha);
+      case 1: return fp.pow56 ? sq * m_cbrt(rho) : m_pow(rho, fp.beta);
+      case 2: return sq;
+      default: return m_pow(rho, fp.alpha);
     }
   }
   switch (f) {
     case 0: return rho;
-    case 1: return m_sqrt(rho);
+    case 1: return sq;
     default: break;
   }
-  const T ex = f < 5 ? (T)s.alpha : (T)s.beta;
+  const T ex = f < 5 ? fp.alpha : fp.beta;
   const int k = (f - 2) % 3;
   const T rx = m_pow(rho, ex);
-  const T th = rho - (T)s.rho_s;
+  const T th = rho - fp.rho_s;
   if (k == 0) return rx;
   if (k == 1) return th * rx;
   return th * th * rx / T(2);
@@ -217,35 +301,49 @@ HD T field_value(const SlotDev& s, int f, T rho) {
 template <typename T>
 HDNI void xfwd_block(const Args<T>& a, int bid, int tid, int nthr, char* smem) {
   const Task t = a.tasks[bid];
-  SlotDev& s = a.slots[t.slot];
+  const SlotDev& s = a.slots[t.slot];
   const Ctl& c = a.ctl[t.slot];
   if (c.status != ST_RUNNING || c.ev == EV_NONE) return;
   const int f = t.a, rp0 = t.b, nb = t.c;
+  const int ev = c.ev;
+  if (ev == EV_ION && f >= s.ion.nspec) return;
+  if (ev == EV_FORCE && f != 0) return;
   const int n1 = s.n1, k1 = s.k1;
-  const long long nrows = (long long)s.n2 * s.n3;
+  const int nrows = s.n2 * s.n3;
+  const EvalIn<T> in = eval_in<T>(s, c);
+  const T* __restrict__ qion = (const T*)s.buf[B_PHI + (f < NBUF ? f : 0)];
+  const FieldPar<T> fp = field_par<T>(s);
+  const FftPlan& px = s.px;
+  cx<T>* __restrict__ out = (cx<T>*)s.spec + (size_t)f * (size_t)s.Nc;
   cx<T>* buf = (cx<T>*)smem;
-  cx<T>* tmp = buf + (size_t)nb * n1;
+  cx<T>* tmp = buf + nb * n1;
+  const unsigned mn1 = magic32(n1);
   for (int w = tid; w < nb * n1; w += nthr) {
-    const int b = w / n1, i = w % n1;
-    const long long j0 = 2LL * (rp0 + b), j1 = j0 + 1;
-    T phin, rho;
-    phi_in_at(s, c, j0 * n1 + i, phin, rho);
-    const T v0 = field_value(s, f, rho);
-    T v1 = T(0);
-    if (j1 < nrows) {
-      phi_in_at(s, c, j1 * n1 + i, phin, rho);
-      v1 = field_value(s, f, rho);
+    const int b = magic_div32(w, mn1), i = w - b * n1;
+    const int j0 = 2 * (rp0 + b), j1 = j0 + 1;
+    T v0, v1 = T(0);
+    if (ev == EV_ION) {  // B-spline charge of species f (FillQIonTable)
+      v0 = qion[j0 * n1 + i];
+      if (j1 < nrows) v1 = qion[j1 * n1 + i];
+    } else {
+      T phin, rho, sq;
+      in.at(j0 * n1 + i, phin, rho, sq);
+      v0 = ev == EV_FORCE ? rho : field_value(fp, f, rho, sq);
+      if (j1 < nrows) {
+        in.at(j1 * n1 + i, phin, rho, sq);
+        v1 = ev == EV_FORCE ? rho : field_value(fp, f, rho, sq);
+      }
     }
     buf[b + i * nb] = mk<T>(v0, v1);
   }
   BLOCK_SYNC();
-  fft_batch(buf, tmp, nb, 1, nb, s.px, a.tw, -1, tid, nthr);
-  cx<T>* out = (cx<T>*)s.spec + (long long)f * s.Nc;
+  const cx<T>* res = fft_batch(buf, tmp, nb, nb, px, a.tw, -1, tid, nthr);
+  const unsigned mk1 = magic32(k1);
   for (int w = tid; w < nb * k1; w += nthr) {
-    const int b = w / k1, k = w % k1;
-    const long long j0 = 2LL * (rp0 + b), j1 = j0 + 1;
-    const cx<T> z = buf[b + k * nb];
-    const cx<T> zc = conj(buf[b + ((n1 - k) % n1) * nb]);
+    const int b = magic_div32(w, mk1), k = w - b * k1;
+    const int j0 = 2 * (rp0 + b), j1 = j0 + 1;
+    const cx<T> z = res[b + k * nb];
+    const cx<T> zc = conj(res[b + (k == 0 ? 0 : n1 - k) * nb]);
     const cx<T> sum = z + zc, dif = z - zc;
     out[j0 * k1 + k] = mk<T>(sum.x * T(0.5), sum.y * T(0.5));
     if (j1 < nrows) out[j1 * k1 + k] = mk<T>(dif.y * T(0.5), -dif.x * T(0.5));
@@ -256,103 +354,146 @@ HDNI void xfwd_block(const Args<T>& a, int bid, int tid, int nthr, char* smem) {
 template <typename T>
 HDNI void ypass_block(const Args<T>& a, int bid, int tid, int nthr, char* smem, int dir) {
   const Task t = a.tasks[bid];
-  SlotDev& s = a.slots[t.slot];
+  const SlotDev& s = a.slots[t.slot];
   const Ctl& c = a.ctl[t.slot];
   if (c.status != ST_RUNNING || c.ev == EV_NONE) return;
   const int f = t.a, z = t.b, kx0 = t.c;
-  const int n2 = s.n2, k1 = s.k1, TX = a.tx;
+  if (c.ev == EV_ION && f >= (dir < 0 ? s.ion.nspec : 1)) return;
+  if (c.ev == EV_FORCE && f >= (dir < 0 ? 1 : s.ion.nspec)) return;
+  const int n2 = s.n2, k1 = s.k1, TX = s.tx;
   const int nb = (k1 - kx0) < TX ? (k1 - kx0) : TX;
   cx<T>* buf = (cx<T>*)smem;
-  cx<T>* tmp = buf + (size_t)TX * n2;
-  cx<T>* sp = (cx<T>*)s.spec + (long long)f * s.Nc + (long long)z * n2 * k1 + kx0;
+  cx<T>* tmp = buf + nb * n2;
+  cx<T>* __restrict__ sp = (cx<T>*)s.spec + (size_t)f * (size_t)s.Nc + (size_t)z * n2 * k1 + kx0;
+  const unsigned mnb = magic32(nb);
   for (int w = tid; w < nb * n2; w += nthr) {
-    const int i = w / nb, b = w % nb;
-    buf[b + i * TX] = sp[(long long)i * k1 + b];
+    const int i = magic_div32(w, mnb), b = w - i * nb;
+    buf[w] = sp[i * k1 + b];
   }
   BLOCK_SYNC();
-  fft_batch(buf, tmp, nb, 1, TX, s.py, a.tw, dir, tid, nthr);
+  const cx<T>* res = fft_batch(buf, tmp, nb, nb, s.py, a.tw, dir, tid, nthr);
   for (int w = tid; w < nb * n2; w += nthr) {
-    const int i = w / nb, b = w % nb;
-    sp[(long long)i * k1 + b] = buf[b + i * TX];
+    const int i = magic_div32(w, mnb), b = w - i * nb;
+    sp[i * k1 + b] = res[w];
   }
 }
 
 // ------------------------------------------------------------ pass 3
+// All gn fields of a group are transformed as one batch of gn*nb sequences
+// laid out [kz][q*nb + b].
 template <typename T>
 HDNI void zpass_block(const Args<T>& a, int bid, int tid, int nthr, char* smem) {
   const Task t = a.tasks[bid];
-  SlotDev& s = a.slots[t.slot];
+  const SlotDev& s = a.slots[t.slot];
   const Ctl& c = a.ctl[t.slot];
   if (c.status != ST_RUNNING || c.ev == EV_NONE) return;
   const int g = t.a, ky = t.b, kx0 = t.c;
-  const int n2 = s.n2, n3 = s.n3, k1 = s.k1, TX = a.tx;
+  const int ev = c.ev;
+  const bool setup_mode = ev == EV_ION || ev == EV_FORCE;
+  if (setup_mode && g != 0) return;
+  const int n2 = s.n2, n3 = s.n3, k1 = s.k1, TX = s.tx;
   const int nb = (k1 - kx0) < TX ? (k1 - kx0) : TX;
-  const int kind = s.group_kind[g], f0 = s.group_f0[g], gn = s.group_nf[g];
-  const long long plane = (long long)n2 * k1;
-  cx<T>* fb[3];
-  for (int q = 0; q < 3; ++q) fb[q] = (cx<T>*)smem + (size_t)q * TX * n3;
-  cx<T>* tmp = (cx<T>*)smem + (size_t)3 * TX * n3;
-  for (int w = tid; w < gn * nb * n3; w += nthr) {
-    const int q = w / (nb * n3), rem = w % (nb * n3);
-    const int i = rem / nb, b = rem % nb;
-    const cx<T>* sp = (const cx<T>*)s.spec + (long long)(f0 + q) * s.Nc;
-    fb[q][b + i * TX] = sp[(long long)i * plane + (long long)ky * k1 + kx0 + b];
+  const int kind = ev == EV_ION ? G_ION : ev == EV_FORCE ? G_FORCE : s.group_kind[g];
+  const int gn = setup_mode ? s.ion.nspec : s.group_nf[g];
+  const int gin = ev == EV_FORCE ? 1 : gn;  // fields loaded
+  const int gout = ev == EV_ION ? 1 : gn;   // fields stored
+  const int NB = gn * nb;
+  const int plane = n2 * k1;
+  const int Nc = (int)s.Nc;
+  cx<T>* __restrict__ spec =
+      (cx<T>*)s.spec + (size_t)(setup_mode ? 0 : s.group_f0[g]) * (size_t)Nc + ky * k1 + kx0;
+  cx<T>* buf = (cx<T>*)smem;
+  cx<T>* tmp = buf + NB * n3;
+  const unsigned mNB = magic32(NB), mnb = magic32(nb);
+  for (int w = tid; w < NB * n3; w += nthr) {
+    const int i = magic_div32(w, mNB), qb = w - i * NB;
+    const int q = magic_div32(qb, mnb), b = qb - q * nb;
+    buf[w] = q < gin ? spec[(size_t)q * Nc + i * plane + b] : mk<T>(T(0), T(0));
   }
   BLOCK_SYNC();
-  for (int q = 0; q < gn; ++q) fft_batch(fb[q], tmp, nb, 1, TX, s.pz, a.tw, -1, tid, nthr);
+  cx<T>* res = fft_batch(buf, tmp, NB, NB, s.pz, a.tw, -1, tid, nthr);
+  cx<T>* oth = res == buf ? tmp : buf;
   const int m2 = ky > n2 / 2 ? ky - n2 : ky;
-  const T* kern = (const T*)s.kern;
+  const T* __restrict__ kern = (const T*)s.kern + ky * k1 + kx0;
+  const T sc = (T)s.inv_n;
+  double rc[9];
+#pragma unroll
+  for (int q = 0; q < 9; ++q) rc[q] = s.recip[q];
+  const double gy0 = rc[3] * m2, gy1 = rc[4] * m2, gy2 = rc[5] * m2;
   for (int w = tid; w < nb * n3; w += nthr) {
-    const int i = w / nb, b = w % nb;
+    const int i = magic_div32(w, mnb), b = w - i * nb;
     const int m1 = kx0 + b;
     const int m3 = i > n3 / 2 ? i - n3 : i;
-    const double gx = s.recip[0] * m1 + s.recip[3] * m2 + s.recip[6] * m3;
-    const double gy = s.recip[1] * m1 + s.recip[4] * m2 + s.recip[7] * m3;
-    const double gz = s.recip[2] * m1 + s.recip[5] * m2 + s.recip[8] * m3;
+    const double gx = rc[0] * m1 + gy0 + rc[6] * m3;
+    const double gy = rc[1] * m1 + gy1 + rc[7] * m3;
+    const double gz = rc[2] * m1 + gy2 + rc[8] * m3;
     const double q = sqrt(gx * gx + gy * gy + gz * gz);
     const double q2 = q * q;
-    const long long idx = (long long)i * plane + (long long)ky * k1 + m1;
-    const int e = b + i * TX;
-    const T sc = (T)s.inv_n;
+    const int kidx = i * plane + b;
+    cx<T>* e = res + i * NB + b;
     switch (kind) {
       case G_HARTREE: {
         const T m = (m1 == 0 && ky == 0 && i == 0) ? T(0) : (T)(4.0 * PI_D / q2) * sc;
-        fb[0][e] = fb[0][e] * m;
+        e[0] = e[0] * m;
         break;
       }
       case G_VW:
-        fb[0][e] = fb[0][e] * ((T)q2 * sc);
+        e[0] = e[0] * ((T)q2 * sc);
         break;
       case G_KMUL:
-        fb[0][e] = fb[0][e] * (kern[idx] * sc);
+        e[0] = e[0] * (kern[kidx] * sc);
         break;
-      default: {  // second-order WGC triple (KEDF_WGC.f90:219-236)
-        const T K1 = kern[idx], K2 = kern[s.Nc + idx], K3 = kern[2 * s.Nc + idx], K4 = kern[3 * s.Nc + idx];
-        const cx<T> F0 = fb[0][e], F1 = fb[1][e], F2 = fb[2][e];
-        fb[0][e] = (F0 * K1 + F1 * K2 + F2 * K3) * sc;
-        fb[1][e] = (F0 * K2 + F1 * K4) * sc;
-        fb[2][e] = F0 * (K3 * sc);
+      case G_WGC3: {  // second-order WGC triple (KEDF_WGC.f90:219-236)
+        const T K1 = kern[kidx], K2 = kern[Nc + kidx], K3 = kern[2 * Nc + kidx], K4 = kern[3 * Nc + kidx];
+        const cx<T> F0 = e[0], F1 = e[nb], F2 = e[2 * nb];
+        e[0] = (F0 * K1 + F1 * K2 + F2 * K3) * sc;
+        e[nb] = (F0 * K2 + F1 * K4) * sc;
+        e[2 * nb] = F0 * (K3 * sc);
+        break;
+      }
+      case G_ION: {  // conj(sum_s V_s(|G|) b1 b2 b3 S_s) N / vol, times the 1/N forward scale
+        // (IonElectronPotRecipSpline, IonElectronSpline.f90:180-203)
+        const cx<double> bb = cmul(cmul(s.ion.b1[m1], s.ion.b2[ky]), s.ion.b3[i]);
+        double yr = 0.0, yi = 0.0;
+        for (int sp = 0; sp < gn; ++sp) {
+          const double v = psp_value(s.ion, sp, q);
+          const cx<T> F = e[sp * nb];
+          yr += v * (double)F.x;
+          yi += v * (double)F.y;
+        }
+        const double pr = yr * bb.x - yi * bb.y, pim = yr * bb.y + yi * bb.x;
+        e[0] = mk<T>((T)(pr / s.vol), (T)(-pim / s.vol));
+        break;
+      }
+      default: {  // G_FORCE: rho(G) V_s(|G|) b1 b2 b3 per species, G = 0 excluded
+        // (IonElectronForcesSpline, IonElectronSpline.f90:300-330)
+        const cx<double> bb = cmul(cmul(s.ion.b1[m1], s.ion.b2[ky]), s.ion.b3[i]);
+        const cx<T> F = e[0];
+        const bool g0 = m1 == 0 && ky == 0 && i == 0;
+        for (int sp = gn - 1; sp >= 0; --sp) {
+          const double v = g0 ? 0.0 : psp_value(s.ion, sp, q) * s.inv_n;
+          const double fr = (double)F.x * v, fi = (double)F.y * v;
+          e[sp * nb] = mk<T>((T)(fr * bb.x - fi * bb.y), (T)(fr * bb.y + fi * bb.x));
+        }
         break;
       }
     }
   }
   BLOCK_SYNC();
-  for (int q = 0; q < gn; ++q) fft_batch(fb[q], tmp, nb, 1, TX, s.pz, a.tw, 1, tid, nthr);
-  for (int w = tid; w < gn * nb * n3; w += nthr) {
-    const int q = w / (nb * n3), rem = w % (nb * n3);
-    const int i = rem / nb, b = rem % nb;
-    cx<T>* sp = (cx<T>*)s.spec + (long long)(f0 + q) * s.Nc;
-    sp[(long long)i * plane + (long long)ky * k1 + kx0 + b] = fb[q][b + i * TX];
+  const cx<T>* out = fft_batch(res, oth, NB, NB, s.pz, a.tw, 1, tid, nthr);
+  for (int w = tid; w < NB * n3; w += nthr) {
+    const int i = magic_div32(w, mNB), qb = w - i * NB;
+    const int q = magic_div32(qb, mnb), b = qb - q * nb;
+    if (q < gout) spec[(size_t)q * Nc + i * plane + b] = out[w];
   }
 }
 
 // ------------------------------------------------------------ pass 5
-// Perdew-Zunger LDA potential and energy density (XC_LDA.f90:51-310), with
-// r13 = rho^(1/3).
+// Perdew-Zunger LDA potential and energy density (XC_LDA.f90:51-310) from
+// rho, r13 = rho^(1/3) and rs = cC / r13.
 template <typename T>
-HD void lda_point(T rho, T r13, T& vxc, T& exc) {
-  const T cXp = T(-0.98474502184269641), cXe = T(-0.73855876638202234), cC = T(0.62035049089940009);
-  const T rs = cC / r13;
+HD void lda_point(T rho, T r13, T rs, T& vxc, T& exc) {
+  const T cXp = T(-0.98474502184269641), cXe = T(-0.73855876638202234);
   if (rs < T(1)) {
     const T lr = m_log(rs);
     vxc = cXp * r13 + lr * (T(3.11e-2) + T(1.33333333333333333e-3) * rs) + T(-5.83666666666666666e-2) +
@@ -361,11 +502,16 @@ HD void lda_point(T rho, T r13, T& vxc, T& exc) {
   } else {
     const T sr = m_sqrt(rs);
     const T den = T(1) + T(1.0529) * sr + T(3.334e-1) * rs;
-    vxc = cXp * r13 + (T(-1.423e-1) + T(-0.174798948333333333) * sr + T(-6.325709333333333333e-2) * rs) / (den * den);
-    exc = cXe * rho * r13 + rho * (T(-1.423e-1) / den);
+    const T iden = T(1) / den;
+    vxc = cXp * r13 + (T(-1.423e-1) + T(-0.174798948333333333) * sr + T(-6.325709333333333333e-2) * rs) *
+                          (iden * iden);
+    exc = cXe * rho * r13 + rho * (T(-1.423e-1) * iden);
   }
 }
 
+// All nf fields of a row-pair range are transformed as one batch of nf*nb
+// sequences laid out [i][f*nb + b]; then every point of the rows gets the
+// real-space epilogue.
 template <typename T>
 HDNI void xinv_block(const Args<T>& a, int bid, int tid, int nthr, char* smem) {
   const Task t = a.tasks[bid];
@@ -374,134 +520,205 @@ HDNI void xinv_block(const Args<T>& a, int bid, int tid, int nthr, char* smem) {
   const int ev = c.ev;
   if (c.status != ST_RUNNING || ev == EV_NONE) return;
   const int rp0 = t.a, nb = t.b, ordinal = t.c;
-  const int n1 = s.n1, k1 = s.k1, nf = s.nf;
-  const long long nrows = (long long)s.n2 * s.n3;
-  cx<T>* fb = (cx<T>*)smem;  // nf buffers of nb*n1
-  cx<T>* tmp = fb + (size_t)nf * nb * n1;
+  const bool setup_mode = ev == EV_ION || ev == EV_FORCE;
+  const int n1 = s.n1, k1 = s.k1;
+  const int nf = ev == EV_ION ? 1 : ev == EV_FORCE ? s.ion.nspec : s.nf;
+  const int NB = nf * nb;
+  const int nrows = s.n2 * s.n3;
+  const int Nc = (int)s.Nc;
+  const cx<T>* __restrict__ spec = (const cx<T>*)s.spec;
+  cx<T>* buf = (cx<T>*)smem;
+  cx<T>* tmp = buf + NB * n1;
   const bool even = (n1 % 2) == 0;
-  for (int f = 0; f < nf; ++f) {
-    const cx<T>* sp = (const cx<T>*)s.spec + (long long)f * s.Nc;
-    cx<T>* bf = fb + (size_t)f * nb * n1;
-    for (int w = tid; w < nb * n1; w += nthr) {
-      const int b = w / n1, k = w % n1;
-      const long long j0 = 2LL * (rp0 + b), j1 = j0 + 1;
-      cx<T> A, B;
-      if (k < k1) {
-        A = sp[j0 * k1 + k];
-        B = j1 < nrows ? sp[j1 * k1 + k] : mk<T>(T(0), T(0));
-        if (k == 0 || (even && k == n1 / 2)) {  // c2r ignores these imaginary parts
-          A.y = T(0);
-          B.y = T(0);
-        }
-      } else {
-        const int kk = n1 - k;
-        A = conj(sp[j0 * k1 + kk]);
-        B = j1 < nrows ? conj(sp[j1 * k1 + kk]) : mk<T>(T(0), T(0));
-      }
-      bf[b + k * nb] = mk<T>(A.x - B.y, A.y + B.x);
+  const int nyq = even ? n1 / 2 : -1;
+  // gather: consecutive threads read consecutive k of one half-spectrum row
+  const unsigned mn1 = magic32(n1), mnb = magic32(nb);
+  for (int w = tid; w < NB * n1; w += nthr) {
+    const int fb = magic_div32(w, mn1), k = w - fb * n1;
+    const int f = magic_div32(fb, mnb), b = fb - f * nb;
+    const cx<T>* sp = spec + (size_t)f * Nc;
+    const int j0 = 2 * (rp0 + b), j1 = j0 + 1;
+    const bool has1 = j1 < nrows;
+    const bool lo = k < k1;
+    const int kk = lo ? k : n1 - k;
+    cx<T> A = sp[j0 * k1 + kk];
+    cx<T> B = has1 ? sp[j1 * k1 + kk] : mk<T>(T(0), T(0));
+    if (!lo) {
+      A.y = -A.y;
+      B.y = -B.y;
+    } else if (k == 0 || k == nyq) {  // c2r ignores these imaginary parts
+      A.y = T(0);
+      B.y = T(0);
     }
+    buf[k * NB + fb] = mk<T>(A.x - B.y, A.y + B.x);
   }
   BLOCK_SYNC();
-  for (int f = 0; f < nf; ++f) fft_batch(fb + (size_t)f * nb * n1, tmp, nb, 1, nb, s.px, a.tw, 1, tid, nthr);
+  const cx<T>* res = fft_batch(buf, tmp, NB, NB, s.px, a.tw, 1, tid, nthr);
+  if (setup_mode) {
+    // EV_ION: ionPotReal; EV_FORCE: the per-species Factor arrays in buf[B_B + s]
+    const unsigned m2n1s = magic32(2 * n1);
+    for (int w = tid; w < nb * 2 * n1; w += nthr) {
+      const int b = magic_div32(w, m2n1s), rem = w - b * 2 * n1;
+      const int half = rem >= n1 ? 1 : 0, i = rem - half * n1;
+      const int j = 2 * (rp0 + b) + half;
+      if (j >= nrows) continue;
+      for (int f = 0; f < nf; ++f) {
+        const cx<T> z = res[i * NB + f * nb + b];
+        T* dst = ev == EV_ION ? (T*)s.vion : (T*)s.buf[B_B + f];
+        dst[j * n1 + i] = half == 0 ? z.x : z.y;
+      }
+    }
+    double zero[NCH];
+#pragma unroll
+    for (int ch = 0; ch < NCH; ++ch) zero[ch] = 0.0;
+    store_partials(s, ordinal, zero, (double*)(tmp + NB * n1), tid, nthr);
+    return;
+  }
 
-  const T* vion = (const T*)s.vion;
-  T* phi = (T*)s.buf[c.iphi];
-  T* w0 = (T*)s.buf[c.iw0];
-  T* w1 = (T*)s.buf[c.iw1];
-  T* trial = (T*)s.buf[c.itrial];
-  const T* bb = (const T*)s.buf[B_B];
-  const T* p = (const T*)s.buf[B_P];
-  const T* d = (const T*)s.buf[B_D];
+  const EvalIn<T> in = eval_in<T>(s, c);
+  const FieldPar<T> fp = field_par<T>(s);
+  const T* __restrict__ vion = (const T*)s.vion;
+  const T* __restrict__ phi = (const T*)s.buf[c.iphi];
+  T* __restrict__ w0 = (T*)s.buf[c.iw0];
+  T* __restrict__ w1 = (T*)s.buf[c.iw1];
+  T* __restrict__ trial = (T*)s.buf[c.itrial];
+  const T* __restrict__ bb = (const T*)s.buf[B_B];
+  const T* __restrict__ p = (const T*)s.buf[B_P];
+  const T* __restrict__ d = (const T*)s.buf[B_D];
   const bool energy = (ev != EV_CG) && (ev != EV_RHO || c.want_energy);
-  const T lam = (T)s.lambda, muv = (T)s.mu, al = (T)s.alpha, be = (T)s.beta, cTF = (T)C_TF;
-  const T mu0 = (T)c.mu, eps = (T)c.eps, st = (T)c.st, ctd = (T)(c.ct * c.dscale);
+  const bool opt_sqrt = c.opt_sqrt != 0 || ev != EV_RHO;
+  const T lam = (T)s.lambda, muv = (T)s.mu, al = fp.alpha, be = fp.beta, cTF = (T)C_TF;
+  const T mu0 = (T)c.mu, ieps = (T)(ev == EV_CG ? 1.0 / c.eps : 0.0), st = (T)c.st, ctd = (T)(c.ct * c.dscale);
+  const T ctf53 = T(5) / T(3) * cTF * lam;
+  const T cC = T(0.62035049089940009);
   double acc[NCH];
+#pragma unroll
   for (int ch = 0; ch < NCH; ++ch) acc[ch] = 0.0;
-  for (int w = tid; w < nb * 2 * n1; w += nthr) {
-    const int b = w / (2 * n1), rem = w % (2 * n1);
-    const int half = rem / n1, i = rem % n1;
-    const long long j = 2LL * (rp0 + b) + half;
-    if (j >= nrows) continue;
-    const long long idx = j * n1 + i;
-    T o[MAX_FIELDS];
-    for (int f = 0; f < nf; ++f) {
-      const cx<T> z = fb[(size_t)f * nb * n1 + b + i * nb];
-      o[f] = half == 0 ? z.x : z.y;
-    }
-    T phin, rho;
-    phi_in_at(s, c, idx, phin, rho);
-    const T sq = m_sqrt(rho);
-    const T r13 = m_cbrt(rho);
-    const T r23 = r13 * r13;
-    T vxc, exc;
-    lda_point(rho, r13, vxc, exc);
-    T vnl, enl, lap;
-    if (s.kinetic == KIN_WT) {
-      const T rb = m_pow(rho, be);
-      const T ra = s.alpha_eq_beta ? rb : m_pow(rho, al);
-      const T pa = nf > 3 ? o[3] : o[1];
-      vnl = cTF * (al * (ra / rho) * o[1] + be * (rb / rho) * pa);
-      enl = cTF * ra * o[1];
-      lap = o[2];
-    } else {
-      const T th = rho - (T)s.rho_s;
-      const T ra = m_pow(rho, al), rb = m_pow(rho, be);
-      vnl = cTF * ((rb / rho) * (be * o[2] + (rho + be * th) * o[3] + th * (rho + be * th / T(2)) * o[4]) +
-                   (ra / rho) * (al * o[5] + (rho + al * th) * o[6] + th * (rho + al * th / T(2)) * o[7]));
-      enl = cTF * rb * (o[2] + th * o[3] + th * th / T(2) * o[4]);
-      lap = o[1];
-    }
-    const T vi = vion[idx];
-    const T potr = vi + o[0] + vxc + (T(5) / T(3) * cTF * lam) * r23 + vnl;
-    T pot;
-    if (ev == EV_RHO && !c.opt_sqrt)
-      pot = potr + muv * lap / (T(2) * sq);
-    else
-      pot = T(2) * sq * potr + muv * lap;
-    if (energy) {
-      acc[CH_EIE] += (double)rho * (double)vi;
-      acc[CH_EH] += 0.5 * (double)o[0] * (double)rho;
-      acc[CH_EXC] += (double)exc;
-      acc[CH_ETF] += (double)(lam * cTF) * (double)(rho * r23);
-      acc[CH_EVW] += 0.5 * (double)muv * (double)sq * (double)lap;
-      acc[CH_ENL] += (double)enl;
-    }
-    const T sg = phin < T(0) ? T(-1) : T(1);
-    switch (ev) {
-      case EV_RHO:
-        w0[idx] = pot;
-        break;
-      case EV_PHI: {
-        const T gg = pot * sg;
-        w0[idx] = gg;
-        acc[CH_M0] += (double)gg * (double)phin;
-        acc[CH_M1] += (double)phin * (double)phin;
-        break;
+  const unsigned m2n1 = magic32(2 * n1);
+  const int total = nb * 2 * n1;
+  for (int w0i = tid; w0i < total; w0i += 2 * nthr) {
+    // two points per iteration: all global loads of both are issued first
+    int idxs[2];
+    bool ok[2];
+    T vi[2], aa[2], bx[2], ex[2], ey[2];
+    int rb[2];
+#pragma unroll
+    for (int u = 0; u < 2; ++u) {
+      const int w = w0i + u * nthr;
+      const int b = magic_div32(w, m2n1), rem = w - b * 2 * n1;
+      const int half = rem >= n1 ? 1 : 0, i = rem - half * n1;
+      const int j = 2 * (rp0 + b) + half;
+      ok[u] = w < total && j < nrows;
+      const int idx = ok[u] ? j * n1 + i : 0;
+      idxs[u] = idx;
+      rb[u] = i * NB + b + (half << 30);
+      vi[u] = vion[idx];
+      aa[u] = in.A[idx];
+      bx[u] = in.rho_mode ? T(0) : in.B[idx];
+      ex[u] = T(0);
+      ey[u] = T(0);
+      if (ev == EV_CG) {
+        ex[u] = bb[idx];
+        ey[u] = p[idx];
+      } else if (ev == EV_LS) {
+        ex[u] = phi[idx];
+        ey[u] = d[idx];
       }
-      case EV_CG: {
-        const T gg = pot * sg;
-        const T ap = ((gg - mu0 * T(2) * phin) - bb[idx]) / eps;
-        w1[idx] = ap;
-        acc[CH_M0] += (double)p[idx] * (double)ap;
-        break;
+    }
+#pragma unroll
+    for (int u = 0; u < 2; ++u) {
+      if (!ok[u]) continue;
+      const int idx = idxs[u];
+      const int half = rb[u] >> 30;
+      const cx<T>* rv = res + (rb[u] & ((1 << 30) - 1));
+      T o[MAX_FIELDS];
+#pragma unroll
+      for (int f = 0; f < MAX_FIELDS; ++f) {
+        if (f < nf) {
+          const cx<T> z = rv[f * nb];
+          o[f] = half == 0 ? z.x : z.y;
+        } else {
+          o[f] = T(0);
+        }
       }
-      default: {  // EV_LS
-        const T gg = pot * sg;
-        w1[idx] = gg;
-        trial[idx] = phin;
-        const T dir = -phi[idx] * st + d[idx] * ctd;
-        const T dl = gg - T(2) * phin * mu0;
-        acc[CH_M0] += (double)gg * (double)dir;
-        acc[CH_M1] += (double)dl * (double)dl;
-        acc[CH_M2] += (double)gg * (double)phin;
-        acc[CH_M3] += (double)phin * (double)phin;
-        break;
+      T phin, rho, sq;
+      if (in.rho_mode) {
+        rho = aa[u];
+        sq = m_sqrt(rho);
+        phin = sq;
+      } else {
+        phin = in.ca * aa[u] + in.cb * bx[u];
+        rho = phin * phin;
+        sq = phin < T(0) ? -phin : phin;
+      }
+      const T x = m_rcbrt(rho);        // rho^(-1/3)
+      const T r13 = rho * x * x;       // rho^(1/3)
+      const T r23 = r13 * r13;
+      const T rinv = x * x * x;        // 1/rho
+      T vxc, exc;
+      lda_point(rho, r13, cC * x, vxc, exc);
+      T vnl, enl, lap;
+      if (fp.wt) {
+        const T rbeta = fp.pow56 ? sq * r13 : m_pow(rho, be);
+        const T ralpha = fp.aeqb ? rbeta : m_pow(rho, al);
+        const T pa = nf > 3 ? o[3] : o[1];
+        vnl = cTF * (al * (ralpha * rinv) * o[1] + be * (rbeta * rinv) * pa);
+        enl = cTF * ralpha * o[1];
+        lap = o[2];
+      } else {
+        const T th = rho - fp.rho_s;
+        const T ralpha = m_pow(rho, al);
+        const T rbeta = fp.sum53 ? rho * r23 / ralpha : m_pow(rho, be);
+        vnl = cTF * ((rbeta * rinv) * (be * o[2] + (rho + be * th) * o[3] + th * (rho + be * th * T(0.5)) * o[4]) +
+                     (ralpha * rinv) * (al * o[5] + (rho + al * th) * o[6] + th * (rho + al * th * T(0.5)) * o[7]));
+        enl = cTF * rbeta * (o[2] + th * o[3] + th * th * T(0.5) * o[4]);
+        lap = o[1];
+      }
+      const T potr = vi[u] + o[0] + vxc + ctf53 * r23 + vnl;
+      const T pot = opt_sqrt ? T(2) * sq * potr + muv * lap : potr + muv * lap * (T(0.5) * sq * rinv);
+      if (energy) {
+        acc[CH_EIE] += (double)rho * (double)vi[u];
+        acc[CH_EH] += 0.5 * (double)o[0] * (double)rho;
+        acc[CH_EXC] += (double)exc;
+        acc[CH_ETF] += (double)(lam * cTF) * (double)(rho * r23);
+        acc[CH_EVW] += 0.5 * (double)muv * (double)sq * (double)lap;
+        acc[CH_ENL] += (double)enl;
+      }
+      const T sg = phin < T(0) ? T(-1) : T(1);
+      switch (ev) {
+        case EV_RHO:
+          w0[idx] = pot;
+          break;
+        case EV_PHI: {
+          const T gg = pot * sg;
+          w0[idx] = gg;
+          acc[CH_M0] += (double)gg * (double)phin;
+          acc[CH_M1] += (double)phin * (double)phin;
+          break;
+        }
+        case EV_CG: {
+          const T gg = pot * sg;
+          const T ap = ((gg - mu0 * T(2) * phin) - ex[u]) * ieps;
+          w1[idx] = ap;
+          acc[CH_M0] += (double)ey[u] * (double)ap;
+          break;
+        }
+        default: {  // EV_LS
+          const T gg = pot * sg;
+          w1[idx] = gg;
+          trial[idx] = phin;
+          const T dir = -ex[u] * st + ey[u] * ctd;
+          const T dl = gg - T(2) * phin * mu0;
+          acc[CH_M0] += (double)gg * (double)dir;
+          acc[CH_M1] += (double)dl * (double)dl;
+          acc[CH_M2] += (double)gg * (double)phin;
+          acc[CH_M3] += (double)phin * (double)phin;
+          break;
+        }
       }
     }
   }
-  double* sred = (double*)(tmp + (size_t)nb * n1);
-  int* sflag = (int*)(sred + NCH * nthr);
-  slot_finish(s, c, K_X5, ev, ordinal, acc, sred, sflag, tid, nthr);
+  store_partials(s, ordinal, acc, (double*)(tmp + NB * n1), tid, nthr);
 }
 
 }  // namespace ofdft

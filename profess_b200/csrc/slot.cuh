@@ -30,12 +30,12 @@ enum BufId : int {
 enum Kinetic : int { KIN_WT = 4, KIN_WGC = 5 };
 
 // Z-pass field groups (which k-space operator applies to which spectra)
-enum GroupKind : int { G_HARTREE = 0, G_VW = 1, G_KMUL = 2, G_WGC3 = 3 };
+enum GroupKind : int { G_HARTREE = 0, G_VW = 1, G_KMUL = 2, G_WGC3 = 3, G_ION = 4, G_FORCE = 5 };
 constexpr int MAX_FIELDS = 8;
 constexpr int MAX_GROUPS = 4;
 
 // ---------------------------------------------------------------- modes
-enum EvalMode : int { EV_NONE = 0, EV_RHO = 1, EV_PHI = 2, EV_CG = 3, EV_LS = 4 };
+enum EvalMode : int { EV_NONE = 0, EV_RHO = 1, EV_PHI = 2, EV_CG = 3, EV_LS = 4, EV_ION = 5, EV_FORCE = 6 };
 enum VecOp : int {
   OP_NONE = 0,
   OP_SQRT_INIT = 1,  // phi = sqrt|rho|; sum rho
@@ -64,6 +64,25 @@ struct HistEntry {
   int ncg, nline;
 };
 
+// Local pseudopotential spline of one species (ReadIonFile.f90:914-976).
+struct PspDev {
+  int npts;
+  int off;  // offset of this species' vqs / pot_dd in the packed table
+  double max_g, charge, v0, dq;
+};
+
+constexpr int MAX_SPECIES = 4;
+
+// Tables of the ion-electron set-up and forces (EV_ION / EV_FORCE modes).
+struct IonAux {
+  int nspec;
+  PspDev psp[MAX_SPECIES];
+  const double* tab;      // packed vqs then pot_dd for every species
+  const cx<double>* b1;   // exponential-spline factors, k1 entries
+  const cx<double>* b2;   // n2 entries
+  const cx<double>* b3;   // n3 entries
+};
+
 struct SlotDev {
   int n1, n2, n3, k1;
   long long N, Nc;
@@ -71,6 +90,9 @@ struct SlotDev {
   double recip[9];  // cellRecip, column-major: recip[3*c + r] = b_c component r
   double dv, inv_n, vol;
   int kinetic, nf, ngroups, alpha_eq_beta;
+  int pow56;       // alpha == beta == 5/6: rho^(5/6) = sqrt(rho) * cbrt(rho)
+  int tx;          // kx tile width of the Y/Z passes
+  int rp;          // row pairs per X-pass task
   int group_kind[MAX_GROUPS];
   int group_f0[MAX_GROUPS];
   int group_nf[MAX_GROUPS];
@@ -79,8 +101,8 @@ struct SlotDev {
   void* vion;   // ionPotReal (N)
   void* kern;   // keKernel planes (nplanes * Nc), real
   void* spec;   // nf half spectra (nf * Nc complex)
+  IonAux ion;
   double* partials;  // ntask_max * NCH
-  int* done;         // NKID counters
   int ntask[NKID];
   HistEntry* hist;
 };
@@ -89,6 +111,7 @@ struct Ctl {
   int status, error, state, op, ev;
   int iphi, itrial, iw0, iw1, evb;
   int opt_sqrt, want_energy;
+  int force_rho;  // EV_FORCE input: 1 = rho in buf[B_PHI], 0 = phi in buf[iphi]
   // prologue coefficients: phi_in = ca * buf[iphi] + cb * buf[evb]
   double ca, cb;
   double opc;  // op coefficient

@@ -87,9 +87,48 @@ SIGNATURES = {
     "ofdft_slot_result": [_vp, ctypes.c_int, _dp, _dp, ctypes.POINTER(NtnStats)],
     "ofdft_slot_history": [_vp, ctypes.c_int, ctypes.c_int, _dp, _dp, _dp, _ip, _ip, _ip],
     "ofdft_slot_download": [_vp, ctypes.c_int, ctypes.c_int, _dp],
+    "ofdft_slot_forces": [_vp, ctypes.c_int, _dp, ctypes.c_int, _dp],
+    "ofdft_ewald": [_dp, ctypes.c_int, _dp, _dp, _dp, _dp],
+    "ofdft_grid_size": [ctypes.c_double, _dp, _ip],
+    "ofdft_wgc_radial_tables": [ctypes.c_double, ctypes.c_double, ctypes.c_double, ctypes.c_int, _dp, _dp, _dp,
+                                _dp, _ip],
 }
 
 _LIBS = {}
+
+
+def ewald(lib, lattice, frac, charges, want_forces=False):
+    """Ewald ion-ion energy (Ha) and forces of point charges (host)."""
+    lat = np.ascontiguousarray(np.asarray(lattice, float).ravel(order="F"))
+    fr = np.ascontiguousarray(frac, dtype=np.float64).reshape(-1, 3)
+    z = np.ascontiguousarray(charges, dtype=np.float64)
+    e = np.zeros(1)
+    f = np.zeros_like(fr) if want_forces else None
+    rc = lib.ofdft_ewald(_ptr(lat), fr.shape[0], _ptr(fr), _ptr(z), _ptr(e), _ptr(f) if want_forces else None)
+    if rc:
+        raise OfdftError(rc, lib.ofdft_last_error().decode())
+    return float(e[0]), f
+
+
+def grid_size(lib, ecut_ha, lattice):
+    """SizeSystem: 7-smooth grid for the cutoff (Ha)."""
+    lat = np.ascontiguousarray(np.asarray(lattice, float).ravel(order="F"))
+    n = np.zeros(3, dtype=np.int32)
+    rc = lib.ofdft_grid_size(float(ecut_ha), _ptr(lat), n.ctypes.data_as(_ip))
+    if rc:
+        raise OfdftError(rc, lib.ofdft_last_error().decode())
+    return tuple(int(x) for x in n)
+
+
+def wgc_radial_tables(lib, alpha, beta, gamma):
+    """(eta, w, eta w', eta^2 w'') of the WGC kernel ODE, integrated by the library."""
+    n = ctypes.c_int()
+    lib.ofdft_wgc_radial_tables(alpha, beta, gamma, 0, None, None, None, None, ctypes.byref(n))
+    arrs = [np.zeros(n.value) for _ in range(4)]
+    rc = lib.ofdft_wgc_radial_tables(alpha, beta, gamma, n.value, *[_ptr(a) for a in arrs], ctypes.byref(n))
+    if rc:
+        raise OfdftError(rc, lib.ofdft_last_error().decode())
+    return tuple(arrs)
 
 
 def load_library(path: str | None = None) -> ctypes.CDLL:
@@ -174,6 +213,45 @@ class Engine:
             k = k[None]
         flat = np.concatenate([np.asfortranarray(p).ravel(order="F") for p in k])
         self._check(self.lib.ofdft_slot_set_kernel(self.h, slot, _ptr(flat), k.shape[0]))
+
+    def build_wt_kernel(self, slot):
+        """FillWT on the device (needs rho0 in the slot description)."""
+        self._check(self.lib.ofdft_slot_build_wt_kernel(self.h, slot))
+
+    def build_wgc_kernel(self, slot, tables=None):
+        """WGC kernel planes on the device; tables = (eta, w, eta w', eta^2 w'')
+        or None for the library's own ODE integration."""
+        if tables is None:
+            self._check(self.lib.ofdft_slot_build_wgc_kernel(self.h, slot, 0, None, None, None, None))
+            return
+        t = [np.ascontiguousarray(x, dtype=np.float64) for x in tables]
+        self._check(self.lib.ofdft_slot_build_wgc_kernel(self.h, slot, len(t[0]), _ptr(t[0]), _ptr(t[1]),
+                                                         _ptr(t[2]), _ptr(t[3])))
+
+    def build_ion_potential(self, slot, frac, species_of_ion, species):
+        """Ion-electron potential by the B-spline method on the device.
+
+        ``species``: sequence of objects with charge, max_g (bohr^-1),
+        pot_values (Ha bohr^3), vqs and pot_dd arrays (ReadPseudo's tables)."""
+        fr = np.ascontiguousarray(frac, dtype=np.float64).reshape(-1, 3)
+        sp = np.ascontiguousarray(species_of_ion, dtype=np.int32)
+        npts = np.array([len(x.pot_values) for x in species], dtype=np.int32)
+        maxg = np.array([x.max_g for x in species], dtype=np.float64)
+        chg = np.array([float(x.charge) for x in species], dtype=np.float64)
+        pv = np.ascontiguousarray(np.concatenate([x.pot_values for x in species]), dtype=np.float64)
+        vq = np.ascontiguousarray(np.concatenate([x.vqs for x in species]), dtype=np.float64)
+        pd = np.ascontiguousarray(np.concatenate([x.pot_dd for x in species]), dtype=np.float64)
+        self._check(self.lib.ofdft_slot_build_ion_potential(
+            self.h, slot, fr.shape[0], _ptr(fr), sp.ctypes.data_as(_ip), len(species), npts.ctypes.data_as(_ip),
+            _ptr(maxg), _ptr(chg), _ptr(pv), _ptr(vq), _ptr(pd)))
+
+    def forces(self, slot, nion, rho=None, include_ewald=True):
+        """Ion forces (nion, 3) in Ha/bohr on rho (or the slot's solved density)."""
+        out = np.zeros((nion, 3))
+        r = _fortran(rho, self.shapes[slot]) if rho is not None else None
+        self._check(self.lib.ofdft_slot_forces(self.h, slot, _ptr(r) if r is not None else None,
+                                               int(bool(include_ewald)), _ptr(out)))
+        return out
 
     def set_ion_potential(self, slot, vion):
         v = _fortran(vion, self.shapes[slot])

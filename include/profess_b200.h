@@ -74,11 +74,14 @@ typedef struct ofdft_ntn_options {
   double tole;             /* tole (Ha), default 1e-6 */
   int max_line;            /* maxLine (Source/RhoLineSearch.f90:34), default 200 */
   int max_ticks;           /* safety bound on engine ticks for the blocking call (0 = 20000) */
+  int stall_line;          /* > 0: stop with outcome 2, keeping the last accepted density, when one
+                              line search needs more than this many trials (the FP32 precision
+                              floor of a mixed-precision solve); 0 = reference behaviour */
 } ofdft_ntn_options;
 
 /* Outcome of a solve (rhoOutcome, numEnergyTotal, numPotentialTotal ...). */
 typedef struct ofdft_ntn_stats {
-  int outcome;             /* rhoOutcome: 0 converged, 1 max iterations / no descent */
+  int outcome;             /* rhoOutcome: 0 converged, 1 max iterations / no descent, 2 stalled */
   int iterations;          /* outer NTN iterations */
   int num_evals;           /* potential evaluations (CalculatePotentialPlus calls) */
   int num_cg;              /* inner CG steps in total */
@@ -159,6 +162,9 @@ int ofdft_proj_norm_rho_minimization(ofdft_engine* e, int slot, double* rho, dou
                                      const ofdft_ntn_options* opts, ofdft_ntn_stats* stats);
 
 /* ---------------------------------------------------------------- batched / asynchronous */
+/* Keep an input density resident on the device; start calls with rho = NULL use it. */
+int ofdft_slot_set_input(ofdft_engine* e, int slot, const double* rho);
+/* Start a solve from rho (host) or, with rho = NULL, from the resident input. */
 int ofdft_slot_start_solve(ofdft_engine* e, int slot, const double* rho, const ofdft_ntn_options* opts);
 /* Start a solve from the density already resident in another slot of the same
  * engine (e.g. an FP32 slot's result refined in an FP64 slot); no host copy. */
@@ -177,6 +183,15 @@ int ofdft_slot_history(ofdft_engine* e, int slot, int max, double* energy, doubl
                        double* theta, int* ncg, int* nline, int* n);
 /* Device-resident arrays of a slot: which = 0 phi, 1 dE/dphi, 2 ion potential. */
 int ofdft_slot_download(ofdft_engine* e, int slot, int which, double* out);
+
+/* ---------------------------------------------------------------- instrumentation */
+/* The CUDA stream (cudaStream_t) the engine launches on. */
+int ofdft_engine_stream(ofdft_engine* e, void** stream);
+/* Kernel launches and ticks issued so far by this engine. */
+int ofdft_engine_counters(ofdft_engine* e, long long* kernel_launches, long long* ticks);
+/* Mean device time (ms) of one batched potential evaluation over every idle
+ * slot with a resident input density, timed with events on the engine stream. */
+int ofdft_engine_time_eval(ofdft_engine* e, int iters, double* ms);
 
 #ifdef __cplusplus
 }

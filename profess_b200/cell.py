@@ -1,0 +1,37 @@
+"""Put a cell on an engine slot with every table built by the library.
+
+This is the set-up the reference does before its first density solve
+(Source/Initializer.f90; KEDFRefresh, Source/SetupKEDF.f90:629-683;
+RefreshIonTerms, Source/RefreshIons.f90:125-238): the kinetic kernel is
+filled on the device (WT from LindG, WGC from the kernel ODE's radial tables),
+the ion-electron potential is built on the device by the B-spline method and
+the Ewald energy is summed on the host.
+"""
+from __future__ import annotations
+
+from . import native
+from .workloads import Cell
+
+
+def ion_ion_energy(lib, cell: Cell) -> float:
+    e, _ = native.ewald(lib, cell.lattice, cell.frac, cell.charges())
+    return e
+
+
+def setup_slot(eng: native.Engine, cell: Cell, precision=native.FP64, ion_ion=None) -> int:
+    """Create a slot for ``cell`` and build its kernel and ion potential on the device."""
+    rho_avg = cell.num_electrons / cell.vol
+    if ion_ion is None:
+        ion_ion = ion_ion_energy(eng.lib, cell)
+    s = eng.slot_create(cell.grid, cell.lattice, kinetic=cell.kinetic, alpha=cell.alpha, beta=cell.beta,
+                        gamma=cell.gamma, rho0=rho_avg, rho_s=rho_avg, ion_ion=ion_ion, precision=precision)
+    try:
+        if cell.kinetic == native.KEDF_WT:
+            eng.build_wt_kernel(s)
+        else:
+            eng.build_wgc_kernel(s)
+        eng.build_ion_potential(s, cell.frac, cell.species_of_ion, cell.species)
+    except Exception:
+        eng.slot_destroy(s)
+        raise
+    return s

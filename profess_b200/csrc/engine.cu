@@ -197,6 +197,12 @@ template <typename T> __global__ void __launch_bounds__(256) k_force_gather(cons
   if (threadIdx.x == 0)
     for (int k = 0; k < 3; ++k) out[3 * blockIdx.x + k] = red[k][0];
 }
+template <typename S, typename D> __global__ void __launch_bounds__(256) k_square_copy(const S* src, D* dst, long long n) {
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+    const double v = (double)src[i];
+    dst[i] = (D)(v * v);
+  }
+}
 template <typename T> __global__ void __launch_bounds__(64) k_ctl(Args<T> a, int kid) {
   __shared__ double sm[NCH * 33 + 2];
   ctl_block(a.slots, a.ctl, a.tasks, kid, blockIdx.x, threadIdx.x, blockDim.x, (char*)sm);
@@ -226,6 +232,7 @@ struct HostSlot {
   double lattice[9];
   double rho0 = 0, gamma = 2.7;
   std::vector<double> frac, zion;
+  void* input = nullptr;        // device-resident input density (ofdft_slot_set_input)
 };
 
 static size_t elem_size(int prec) { return prec == OFDFT_FP32 ? 4 : 8; }
@@ -239,6 +246,14 @@ struct Engine {
   LaunchList lists[2][NPASS];
   bool dirty = true;
   std::vector<char> emu_smem;
+  long long n_launches = 0, n_ticks = 0;
+  long long launches_per_tick() const {
+    long long n = 0;
+    for (int p = 0; p < 2; ++p)
+      for (int k = 0; k < NPASS; ++k)
+        if (!lists[p][k].h.empty()) n += (k == P_VEC ? VEC_PER_TICK : k == P_CTL ? VEC_PER_TICK + 1 : 1);
+    return n;
+  }
 #if defined(OFDFT_EMU)
   int d2h_stream(void* h, const void* d, size_t n) { return d2h(h, d, n); }
 #else
@@ -279,6 +294,8 @@ struct Engine {
     dfree(d_ctl);
     plans.release();
 #if !defined(OFDFT_EMU)
+    if (pinned) cudaFreeHost(pinned);
+    pinned = nullptr;
     if (stream) cudaStreamDestroy(stream);
     stream = nullptr;
 #endif
@@ -291,6 +308,8 @@ struct Engine {
     if (h.d_stencil) dfree(h.d_stencil);
     h.d_stencil = nullptr;
     h.nion = 0;
+    if (h.input) dfree(h.input);
+    h.input = nullptr;
     h.used = false;
     h.running = false;
     dirty = true;
@@ -656,19 +675,72 @@ struct Engine {
     return OFDFT_OK;
   }
 
-  // Upload a host FP64 array into a device array of the slot's precision.
+  // Host <-> device copies of FP64 host arrays into/out of device arrays of
+  // the slot's precision, staged through a pinned host buffer on the engine
+  // stream.
+  std::vector<char> emu_stage;
+  void* pinned = nullptr;
+  size_t pinned_bytes = 0;
+  int stage(size_t bytes, void** p) {
+#if defined(OFDFT_EMU)
+    if (emu_stage.size() < bytes) emu_stage.resize(bytes);
+    *p = emu_stage.data();
+    return OFDFT_OK;
+#else
+    if (pinned_bytes < bytes) {
+      if (pinned) cudaFreeHost(pinned);
+      pinned = nullptr;
+      pinned_bytes = 0;
+      int rc = cuda_check(cudaMallocHost(&pinned, bytes), "cudaMallocHost");
+      if (rc) return rc;
+      pinned_bytes = bytes;
+    }
+    *p = pinned;
+    return OFDFT_OK;
+#endif
+  }
+  int copy_in(void* dst, const void* src, size_t n) {
+#if defined(OFDFT_EMU)
+    return h2d(dst, src, n);
+#else
+    int rc = cuda_check(cudaMemcpyAsync(dst, src, n, cudaMemcpyHostToDevice, stream), "H2D async");
+    return rc ? rc : cuda_check(cudaStreamSynchronize(stream), "stream synchronize");
+#endif
+  }
+  int copy_out(void* dst, const void* src, size_t n) {
+#if defined(OFDFT_EMU)
+    return d2h(dst, src, n);
+#else
+    int rc = cuda_check(cudaMemcpyAsync(dst, src, n, cudaMemcpyDeviceToHost, stream), "D2H async");
+    return rc ? rc : cuda_check(cudaStreamSynchronize(stream), "stream synchronize");
+#endif
+  }
   int upload_real(int prec, void* dst, const double* src, long long n) {
-    if (prec == OFDFT_FP64) return h2d(dst, src, sizeof(double) * n);
-    std::vector<float> t(n);
-    for (long long i = 0; i < n; ++i) t[i] = (float)src[i];
-    return h2d(dst, t.data(), sizeof(float) * n);
+    void* st = nullptr;
+    const size_t bytes = elem_size(prec) * (size_t)n;
+    int rc = stage(bytes, &st);
+    if (rc) return rc;
+    if (prec == OFDFT_FP64) {
+      memcpy(st, src, bytes);
+    } else {
+      float* f = (float*)st;
+      for (long long i = 0; i < n; ++i) f[i] = (float)src[i];
+    }
+    return copy_in(dst, st, bytes);
   }
   int download_real(int prec, double* dst, const void* src, long long n) {
-    if (prec == OFDFT_FP64) return d2h(dst, src, sizeof(double) * n);
-    std::vector<float> t(n);
-    int rc = d2h(t.data(), src, sizeof(float) * n);
-    for (long long i = 0; i < n; ++i) dst[i] = (double)t[i];
-    return rc;
+    void* st = nullptr;
+    const size_t bytes = elem_size(prec) * (size_t)n;
+    int rc = stage(bytes, &st);
+    if (rc) return rc;
+    if ((rc = copy_out(st, src, bytes))) return rc;
+    if (prec == OFDFT_FP64) {
+      memcpy(dst, st, bytes);
+    } else {
+      const float* f = (const float*)st;
+      for (long long i = 0; i < n; ++i) dst[i] = (double)f[i];
+    }
+    return OFDFT_OK;
   }
 
   int get_ctl(int i, Ctl& c) { return d2h(&c, d_ctl + i, sizeof(Ctl)); }
@@ -686,11 +758,27 @@ struct Engine {
     c.macheps = prec == OFDFT_FP32 ? 1.1920928955078125e-07 : 2.220446049250313e-16;
   }
 
+  // rho on the host, or NULL for the slot's device-resident input density.
+  int load_density(int i, const double* rho) {
+    HostSlot& h = slots[i];
+    if (rho) return upload_real(h.prec, h.sd.buf[B_PHI], rho, h.sd.N);
+    if (!h.input) return fail(OFDFT_EINVAL, "no device-resident input density (ofdft_slot_set_input)");
+    return d2d(h.sd.buf[B_PHI], h.input, elem_size(h.prec) * h.sd.N);
+  }
+
+  int set_input(int i, const double* rho) {
+    int rc = check_slot(i);
+    if (rc) return rc;
+    HostSlot& h = slots[i];
+    if (!h.input && (rc = dmalloc(&h.input, elem_size(h.prec) * h.sd.N))) return rc;
+    return upload_real(h.prec, h.input, rho, h.sd.N);
+  }
+
   int start_eval(int i, const double* rho, int opt_sqrt, int want_energy) {
     int rc = check_slot(i);
     if (rc) return rc;
     HostSlot& h = slots[i];
-    if ((rc = upload_real(h.prec, h.sd.buf[B_PHI], rho, h.sd.N))) return rc;
+    if ((rc = load_density(i, rho))) return rc;
     Ctl c;
     base_ctl(c, h.prec);
     c.ev = EV_RHO;
@@ -710,6 +798,7 @@ struct Engine {
     c.pot_tol = (o && o->pot_tol > 0) ? o->pot_tol : 1.0e-5;
     c.tole = (o && o->tole > 0) ? o->tole : 1.0e-6;
     c.max_line = (o && o->max_line > 0) ? o->max_line : 200;
+    c.stall_line = (o && o->stall_line > 0) ? o->stall_line : 0;
     c.outcome = -1;
   }
 
@@ -717,13 +806,106 @@ struct Engine {
     int rc = check_slot(i);
     if (rc) return rc;
     HostSlot& h = slots[i];
-    if ((rc = upload_real(h.prec, h.sd.buf[B_PHI], rho, h.sd.N))) return rc;
+    if ((rc = load_density(i, rho))) return rc;
     Ctl c;
     solve_ctl(c, h.prec, o);
     if ((rc = put_ctl(i, c))) return rc;
     h.running = true;
     dirty = true;
     return OFDFT_OK;
+  }
+
+  // Start a solve in slot i from the density phi^2 held by slot src (same grid).
+  int start_solve_from(int i, int src, const ofdft_ntn_options* o) {
+    int rc = check_slot(i);
+    if (rc) return rc;
+    if ((rc = check_slot(src))) return rc;
+    HostSlot& h = slots[i];
+    HostSlot& g = slots[src];
+    if (h.sd.N != g.sd.N || h.sd.n1 != g.sd.n1 || h.sd.n2 != g.sd.n2)
+      return fail(OFDFT_EINVAL, "source slot has a different grid");
+    Ctl cs;
+    if ((rc = get_ctl(src, cs))) return rc;
+    const void* sp = g.sd.buf[cs.iphi];
+    void* dp = h.sd.buf[B_PHI];
+    const long long n = h.sd.N;
+#if defined(OFDFT_EMU)
+    for (long long k = 0; k < n; ++k) {
+      const double v = g.prec == OFDFT_FP32 ? (double)((const float*)sp)[k] : ((const double*)sp)[k];
+      if (h.prec == OFDFT_FP32) ((float*)dp)[k] = (float)(v * v);
+      else ((double*)dp)[k] = v * v;
+    }
+#else
+    const int blocks = (int)std::min<long long>(2048, (n + 255) / 256);
+    if (g.prec == OFDFT_FP32 && h.prec == OFDFT_FP64)
+      k_square_copy<float, double><<<blocks, 256, 0, stream>>>((const float*)sp, (double*)dp, n);
+    else if (g.prec == OFDFT_FP64 && h.prec == OFDFT_FP64)
+      k_square_copy<double, double><<<blocks, 256, 0, stream>>>((const double*)sp, (double*)dp, n);
+    else if (g.prec == OFDFT_FP32 && h.prec == OFDFT_FP32)
+      k_square_copy<float, float><<<blocks, 256, 0, stream>>>((const float*)sp, (float*)dp, n);
+    else
+      k_square_copy<double, float><<<blocks, 256, 0, stream>>>((const double*)sp, (float*)dp, n);
+    if ((rc = cuda_check(cudaGetLastError(), "square copy launch"))) return rc;
+    if ((rc = sync_stream())) return rc;
+#endif
+    Ctl c;
+    solve_ctl(c, h.prec, o);
+    if ((rc = put_ctl(i, c))) return rc;
+    h.running = true;
+    dirty = true;
+    return OFDFT_OK;
+  }
+
+  // Back-to-back potential evaluations of every slot that has a resident
+  // input density; returns the mean device time of one batched evaluation
+  // (passes 1-5 and the controller kernel), timed with events on the engine stream.
+  int time_eval(int iters, double* ms_out) {
+    int rc;
+    std::vector<int> ids;
+    for (int i = 0; i < cap; ++i)
+      if (slots[i].used && !slots[i].running && slots[i].input) ids.push_back(i);
+    if (ids.empty()) return fail(OFDFT_EINVAL, "no slot with a resident input density");
+    auto start_all = [&]() -> int {
+      for (int i : ids) {
+        int r = start_eval(i, nullptr, 1, 1);
+        if (r) return r;
+      }
+      return OFDFT_OK;
+    };
+    if ((rc = start_all())) return rc;
+    int running = 0;
+    if ((rc = run(2, &running, 1))) return rc;  // warm-up and graph capture for one tick
+#if defined(OFDFT_EMU)
+    *ms_out = 0.0;
+    (void)iters;
+    return OFDFT_OK;
+#else
+    cudaEvent_t e0, e1;
+    cudaEventCreate(&e0);
+    cudaEventCreate(&e1);
+    float total = 0.0f;
+    for (int it = 0; it < iters; ++it) {
+      if ((rc = start_all())) break;
+      if (dirty && (rc = build_lists())) break;
+      if ((rc = capture(1))) break;
+      cudaEventRecord(e0, stream);
+      if ((rc = cuda_check(cudaGraphLaunch(graph_exec, stream), "graph launch"))) break;
+      cudaEventRecord(e1, stream);
+      if ((rc = sync_stream())) break;
+      float ms = 0.0f;
+      cudaEventElapsedTime(&ms, e0, e1);
+      total += ms;
+      n_ticks += 1;
+      n_launches += launches_per_tick();
+      for (int i : ids) slots[i].running = false;
+      dirty = true;
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    if (rc) return rc;
+    *ms_out = total / (double)iters;
+    return OFDFT_OK;
+#endif
   }
 
   // ---------------------------------------------------------- task lists
@@ -909,6 +1091,8 @@ struct Engine {
       if ((rc = capture(n))) return rc;
 #endif
     }
+    n_ticks += n;
+    n_launches += (long long)n * launches_per_tick();
 #if !defined(OFDFT_EMU)
     if (graph_exec && graph_ticks == n) return cuda_check(cudaGraphLaunch(graph_exec, stream), "graph launch");
 #endif
@@ -1020,13 +1204,40 @@ int ofdft_slot_set_ion_potential(ofdft_engine* e, int slot, const double* v) {
 }
 
 int ofdft_slot_start_eval(ofdft_engine* e, int slot, const double* rho, int opt_sqrt, int want_energy) {
-  if (!e || !rho) return fail(OFDFT_EINVAL, "null argument");
+  if (!e) return fail(OFDFT_EINVAL, "null argument");
   return e->eng.start_eval(slot, rho, opt_sqrt, want_energy);
 }
 
 int ofdft_slot_start_solve(ofdft_engine* e, int slot, const double* rho, const ofdft_ntn_options* o) {
-  if (!e || !rho) return fail(OFDFT_EINVAL, "null argument");
+  if (!e) return fail(OFDFT_EINVAL, "null argument");
   return e->eng.start_solve(slot, rho, o);
+}
+
+int ofdft_slot_set_input(ofdft_engine* e, int slot, const double* rho) {
+  if (!e || !rho) return fail(OFDFT_EINVAL, "null argument");
+  return e->eng.set_input(slot, rho);
+}
+
+int ofdft_engine_stream(ofdft_engine* e, void** stream) {
+  if (!e || !stream) return fail(OFDFT_EINVAL, "null argument");
+#if defined(OFDFT_EMU)
+  *stream = nullptr;
+#else
+  *stream = (void*)e->eng.stream;
+#endif
+  return OFDFT_OK;
+}
+
+int ofdft_engine_counters(ofdft_engine* e, long long* kernel_launches, long long* ticks) {
+  if (!e) return fail(OFDFT_EINVAL, "null engine");
+  if (kernel_launches) *kernel_launches = e->eng.n_launches;
+  if (ticks) *ticks = e->eng.n_ticks;
+  return OFDFT_OK;
+}
+
+int ofdft_engine_time_eval(ofdft_engine* e, int iters, double* ms) {
+  if (!e || !ms || iters < 1) return fail(OFDFT_EINVAL, "bad argument");
+  return e->eng.time_eval(iters, ms);
 }
 
 int ofdft_engine_run(ofdft_engine* e, int ticks, int* running) {
@@ -1135,8 +1346,9 @@ int ofdft_proj_norm_rho_minimization(ofdft_engine* e, int slot, double* rho, dou
   return ofdft_slot_result(e, slot, rho, energy, st);
 }
 
-int ofdft_slot_start_solve_from_slot(ofdft_engine*, int, int, const ofdft_ntn_options*) {
-  return fail(OFDFT_EINVAL, "not available yet");
+int ofdft_slot_start_solve_from_slot(ofdft_engine* e, int slot, int src_slot, const ofdft_ntn_options* o) {
+  if (!e) return fail(OFDFT_EINVAL, "null engine");
+  return e->eng.start_solve_from(slot, src_slot, o);
 }
 int ofdft_slot_build_wt_kernel(ofdft_engine* e, int slot) {
   if (!e) return fail(OFDFT_EINVAL, "null engine");

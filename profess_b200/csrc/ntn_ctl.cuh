@@ -101,6 +101,7 @@ HDNI inline void ctl_accept(Ctl& c, const SlotDev& s, const double* red) {
   t = c.iw0; c.iw0 = c.iw1; c.iw1 = t;
   c.mu = s.dv * red[CH_M2] / (2.0 * c.tot_ele);
   c.phi2 = red[CH_M3];
+  for (int k = 0; k < 9; ++k) c.energy_acc[k] = c.energy[k];
   if (exit_flag) {
     ctl_finish(c, ST_DONE, ERR_NONE);
     return;
@@ -129,6 +130,7 @@ HDNI inline void ntn_after(Ctl& c, const SlotDev& s, const double* red, int kid,
         return;
       case EV_PHI:  // first evaluation of ProjNormRhoMinimization (RhoOptN.f90:357-362)
         ctl_energy(c, s, red);
+        for (int k = 0; k < 9; ++k) c.energy_acc[k] = c.energy[k];
         c.mu = s.dv * red[CH_M0] / (2.0 * c.tot_ele);
         c.phi2 = red[CH_M1];
         c.iter = 0;
@@ -152,6 +154,13 @@ HDNI inline void ntn_after(Ctl& c, const SlotDev& s, const double* red, int kid,
         c.gradth = s.dv * red[CH_M0];
         c.nline++;
         c.num_ls++;
+        if (c.stall_line > 0 && c.nline > c.stall_line) {
+          // precision floor: keep the last accepted density and stop (outcome 2)
+          for (int k = 0; k < 9; ++k) c.energy[k] = c.energy_acc[k];
+          c.outcome = 2;
+          ctl_finish(c, ST_DONE, ERR_NONE);
+          return;
+        }
         if (c.nline > c.max_line) { ctl_accept(c, s, red); return; }
         double stp = c.theta;
         c.ls_task = ls_step(c.ls, stp, c.energy[0], c.gradth, c.ls_task);

@@ -118,9 +118,11 @@ struct Ctl {
   // optimiser scalars
   double tot_ele, mu, phi2, theta, st, ct, dscale, gradth, eps, macheps;
   double energy[9];
+  double energy_acc[9];  // energy table of the last accepted density
   double e3[3];
   double pot_norm;
   int iter, max_iter, conv_check, max_line, switch_stp, outcome, nline;
+  int stall_line;  // > 0: stop when one line search needs more trials (precision floor)
   double pot_tol, tole;
   // CG
   int cg_iter, cg_flag;

@@ -47,7 +47,7 @@ class CellDesc(ctypes.Structure):
 class NtnOptions(ctypes.Structure):
     _fields_ = [("max_iter", ctypes.c_int), ("conv_check", ctypes.c_int),
                 ("pot_tol", ctypes.c_double), ("tole", ctypes.c_double),
-                ("max_line", ctypes.c_int), ("max_ticks", ctypes.c_int)]
+                ("max_line", ctypes.c_int), ("max_ticks", ctypes.c_int), ("stall_line", ctypes.c_int)]
 
 
 class NtnStats(ctypes.Structure):
@@ -88,6 +88,10 @@ SIGNATURES = {
     "ofdft_slot_history": [_vp, ctypes.c_int, ctypes.c_int, _dp, _dp, _dp, _ip, _ip, _ip],
     "ofdft_slot_download": [_vp, ctypes.c_int, ctypes.c_int, _dp],
     "ofdft_slot_forces": [_vp, ctypes.c_int, _dp, ctypes.c_int, _dp],
+    "ofdft_slot_set_input": [_vp, ctypes.c_int, _dp],
+    "ofdft_engine_stream": [_vp, ctypes.POINTER(_vp)],
+    "ofdft_engine_counters": [_vp, ctypes.POINTER(ctypes.c_longlong), ctypes.POINTER(ctypes.c_longlong)],
+    "ofdft_engine_time_eval": [_vp, ctypes.c_int, _dp],
     "ofdft_ewald": [_dp, ctypes.c_int, _dp, _dp, _dp, _dp],
     "ofdft_grid_size": [ctypes.c_double, _dp, _ip],
     "ofdft_wgc_radial_tables": [ctypes.c_double, ctypes.c_double, ctypes.c_double, ctypes.c_int, _dp, _dp, _dp,
@@ -160,9 +164,11 @@ def _fortran(a, shape=None) -> np.ndarray:
     return np.asfortranarray(a)
 
 
-def ntn_options(max_iter=500, conv_check=CONV_ENE, pot_tol=1.0e-5, tole=1.0e-6, max_line=200, max_ticks=0):
-    """RhoOptimizers defaults (Source/RhoOptimizers.f90:44-101)."""
-    return NtnOptions(max_iter, conv_check, pot_tol, tole, max_line, max_ticks)
+def ntn_options(max_iter=500, conv_check=CONV_ENE, pot_tol=1.0e-5, tole=1.0e-6, max_line=200, max_ticks=0,
+                stall_line=0):
+    """RhoOptimizers defaults (Source/RhoOptimizers.f90:44-101); stall_line > 0
+    stops at the line-search precision floor (mixed-precision FP32 phase)."""
+    return NtnOptions(max_iter, conv_check, pot_tol, tole, max_line, max_ticks, stall_line)
 
 
 class Engine:
@@ -280,10 +286,33 @@ class Engine:
         return r, e, st.as_dict()
 
     # -------------------------------------------------------------- async
-    def start_solve(self, slot, rho, opts: NtnOptions | None = None):
-        r = _fortran(rho, self.shapes[slot])
+    def start_solve(self, slot, rho=None, opts: NtnOptions | None = None):
+        """Start a solve from host rho, or from the resident input when rho is None."""
         o = opts or ntn_options()
+        if rho is None:
+            self._check(self.lib.ofdft_slot_start_solve(self.h, slot, None, ctypes.byref(o)))
+            return
+        r = _fortran(rho, self.shapes[slot])
         self._check(self.lib.ofdft_slot_start_solve(self.h, slot, _ptr(r), ctypes.byref(o)))
+
+    def set_input(self, slot, rho):
+        r = _fortran(rho, self.shapes[slot])
+        self._check(self.lib.ofdft_slot_set_input(self.h, slot, _ptr(r)))
+
+    def stream(self) -> int:
+        p = _vp()
+        self._check(self.lib.ofdft_engine_stream(self.h, ctypes.byref(p)))
+        return p.value or 0
+
+    def counters(self):
+        a, b = ctypes.c_longlong(), ctypes.c_longlong()
+        self._check(self.lib.ofdft_engine_counters(self.h, ctypes.byref(a), ctypes.byref(b)))
+        return a.value, b.value
+
+    def time_eval(self, iters=10) -> float:
+        ms = np.zeros(1)
+        self._check(self.lib.ofdft_engine_time_eval(self.h, int(iters), _ptr(ms)))
+        return float(ms[0])
 
     def start_solve_from_slot(self, slot, src, opts: NtnOptions | None = None):
         o = opts or ntn_options()

@@ -161,6 +161,23 @@ int ofdft_calculate_potential_plus(ofdft_engine* e, int slot, const double* rho,
 int ofdft_proj_norm_rho_minimization(ofdft_engine* e, int slot, double* rho, double* energy,
                                      const ofdft_ntn_options* opts, ofdft_ntn_stats* stats);
 
+/* Allocation-free CalculatePotentialPlus (no counterpart in the reference).
+ * For callers that cannot allocate device memory themselves or through this
+ * library (a host code running inside a device-memory pool it does not own,
+ * or under a memory budget fixed before the solve): all scratch comes from a
+ * 12 MiB array compiled into the library, which every GPU that loads the
+ * library holds until the process exits.  Supports the FP64 WT functional on
+ * 7-smooth grids with dimensions <= 128 and at most 262144 points; larger
+ * requests return OFDFT_EINVAL.  rho, kernel (keKernel plane, (n1/2+1,n2,n3)),
+ * ion_pot and potential are DEVICE pointers (x-fastest, FP64); etable (9
+ * doubles, may be NULL) is host memory; stream is a cudaStream_t or NULL.
+ * The first call on a device looks up the array's address (make it before
+ * any stream capture).  Calls share the array, so calls whose work overlaps
+ * on the GPU race; the call returns after its stream has finished. */
+int ofdft_calculate_potential_plus_noalloc(const ofdft_cell_desc* desc, const double* rho, const double* kernel,
+                                           const double* ion_pot, int opt_sqrt, double* potential, double* etable,
+                                           void* stream);
+
 /* ---------------------------------------------------------------- batched / asynchronous */
 /* Keep an input density resident on the device; start calls with rho = NULL use it. */
 int ofdft_slot_set_input(ofdft_engine* e, int slot, const double* rho);

@@ -1431,3 +1431,232 @@ int ofdft_wgc_radial_tables(double alpha, double beta, double gamma, int max, do
 }
 
 }  // extern "C"
+
+// ------------------------------------------------------------ allocation-free evaluation
+// For callers that must not allocate device memory (for example a host code
+// that runs inside a memory pool it does not own, or under a device-memory
+// budget fixed before the solve starts): one CalculatePotentialPlus-style
+// evaluation whose scratch (slot descriptor, controller record, FFT
+// twiddles, spectra, reduction partials and task lists) lives in the
+// file-scope device array below.  Every GPU that loads this library holds
+// the array until the process exits.  Calls share it, so two calls whose
+// work overlaps on the GPU race; each call rewrites everything it reads.
+#if !defined(OFDFT_EMU)
+namespace noalloc {
+constexpr size_t SCRATCH_BYTES = size_t(12) << 20;  // 12 MiB
+constexpr long long MAX_POINTS = 262144;             // 64^3 grid points
+constexpr int MAX_DIM = 128;
+constexpr int MAX_TASKS = 12288;
+static __device__ __align__(256) unsigned char g_scratch[SCRATCH_BYTES];
+static void* g_addr[128];                  // device address of g_scratch per device ordinal
+static Task g_tasks[MAX_TASKS];            // host staging of the task lists
+static cx<double> g_tw[4 * MAX_DIM];       // host staging of the twiddles
+static Ctl g_ctl;
+
+static size_t up256(size_t x) { return (x + 255) & ~size_t(255); }
+
+// Plan of length n with twiddles appended to g_tw at offset *off (no heap use).
+static void make_plan(int n, FftPlan& p, int* off) {
+  memset(&p, 0, sizeof(p));
+  p.n = n;
+  p.tw_base = *off;
+  int r[FFT_MAX_STAGES], nr = 0, m = n, e2 = 0;
+  while (m % 2 == 0) { m /= 2; ++e2; }
+  while (e2 >= 3) { r[nr++] = 8; e2 -= 3; }
+  if (e2 == 2) r[nr++] = 4;
+  if (e2 == 1) r[nr++] = 2;
+  for (int q : {3, 5, 7})
+    while (m % q == 0) { r[nr++] = q; m /= q; }
+  p.nst = nr;
+  int ns = 1, o = 0;
+  for (int s = 0; s < nr; ++s) {
+    const int R = r[s];
+    p.R[s] = R;
+    p.Ns[s] = ns;
+    p.tw[s] = o;
+    p.ns_magic[s] = (unsigned)(((1u << 20) + (unsigned)ns - 1) / (unsigned)ns);
+    for (int k = 0; k < ns; ++k)
+      for (int j = 1; j < R; ++j) {
+        const long double a = -2.0L * 3.141592653589793238462643383279502884L * (long double)(j * k) /
+                              (long double)(ns * R);
+        g_tw[*off + o++] = mk<double>((double)cosl(a), (double)sinl(a));
+      }
+    ns *= R;
+  }
+  *off += o;
+}
+}  // namespace noalloc
+#endif
+
+extern "C" int ofdft_calculate_potential_plus_noalloc(const ofdft_cell_desc* d, const double* rho,
+                                                      const double* kernel, const double* ion_pot, int opt_sqrt,
+                                                      double* potential, double* etable, void* stream_ptr) {
+#if defined(OFDFT_EMU)
+  (void)d; (void)rho; (void)kernel; (void)ion_pot; (void)opt_sqrt; (void)potential; (void)etable; (void)stream_ptr;
+  return fail(OFDFT_EINVAL, "the allocation-free evaluation needs the CUDA build");
+#else
+  using namespace noalloc;
+  if (!d || !rho || !kernel || !ion_pot || !potential) return fail(OFDFT_EINVAL, "null argument");
+  if (d->kinetic != KIN_WT || d->precision != OFDFT_FP64)
+    return fail(OFDFT_EINVAL, "the allocation-free evaluation supports the FP64 WT functional only");
+  const int ns[3] = {d->n1, d->n2, d->n3};
+  for (int k = 0; k < 3; ++k)
+    if (ns[k] < 2 || ns[k] > MAX_DIM || !seven_smooth(ns[k]))
+      return fail(OFDFT_EINVAL, "grid dimensions must be 7-smooth and in [2, 128]");
+  const long long N = (long long)d->n1 * d->n2 * d->n3;
+  if (N > MAX_POINTS)
+    return fail(OFDFT_EINVAL, "grid too large for the allocation-free evaluation (at most 262144 points)");
+  cudaStream_t st = (cudaStream_t)stream_ptr;
+  int dev = 0;
+  int rc = cuda_check(cudaGetDevice(&dev), "cudaGetDevice");
+  if (rc) return rc;
+  if (dev < 0 || dev >= 128) return fail(OFDFT_EINVAL, "device ordinal out of range");
+  if (!g_addr[dev]) {  // once per device, with that device current
+    void* a = nullptr;
+    if ((rc = cuda_check(cudaGetSymbolAddress(&a, g_scratch), "cudaGetSymbolAddress"))) return rc;
+    g_addr[dev] = a;
+  }
+  char* base = (char*)g_addr[dev];
+
+  // slot descriptor (as ofdft_slot_create fills it) pointing at the caller's buffers
+  SlotDev s;
+  memset(&s, 0, sizeof(s));
+  s.n1 = d->n1; s.n2 = d->n2; s.n3 = d->n3;
+  s.k1 = d->n1 / 2 + 1;
+  s.N = N;
+  s.Nc = (long long)s.k1 * d->n2 * d->n3;
+  int twoff = 0;
+  make_plan(d->n1, s.px, &twoff);
+  make_plan(d->n2, s.py, &twoff);
+  make_plan(d->n3, s.pz, &twoff);
+  const double* L = d->lattice;
+  auto A = [&](int r, int c) { return L[3 * c + r]; };
+  const double det = A(0, 0) * (A(1, 1) * A(2, 2) - A(1, 2) * A(2, 1)) - A(0, 1) * (A(1, 0) * A(2, 2) - A(1, 2) * A(2, 0)) +
+                     A(0, 2) * (A(1, 0) * A(2, 1) - A(1, 1) * A(2, 0));
+  if (!(std::fabs(det) > 0)) return fail(OFDFT_EINVAL, "singular lattice");
+  double inv[3][3];
+  inv[0][0] = (A(1, 1) * A(2, 2) - A(1, 2) * A(2, 1)) / det;
+  inv[0][1] = (A(0, 2) * A(2, 1) - A(0, 1) * A(2, 2)) / det;
+  inv[0][2] = (A(0, 1) * A(1, 2) - A(0, 2) * A(1, 1)) / det;
+  inv[1][0] = (A(1, 2) * A(2, 0) - A(1, 0) * A(2, 2)) / det;
+  inv[1][1] = (A(0, 0) * A(2, 2) - A(0, 2) * A(2, 0)) / det;
+  inv[1][2] = (A(0, 2) * A(1, 0) - A(0, 0) * A(1, 2)) / det;
+  inv[2][0] = (A(1, 0) * A(2, 1) - A(1, 1) * A(2, 0)) / det;
+  inv[2][1] = (A(0, 1) * A(2, 0) - A(0, 0) * A(2, 1)) / det;
+  inv[2][2] = (A(0, 0) * A(1, 1) - A(0, 1) * A(1, 0)) / det;
+  for (int c = 0; c < 3; ++c)
+    for (int r = 0; r < 3; ++r) s.recip[3 * c + r] = inv[c][r] * 2.0 * 3.141592653589793238462643;
+  s.vol = std::fabs(det);
+  s.dv = s.vol / (double)N;
+  s.inv_n = 1.0 / (double)N;
+  s.kinetic = KIN_WT;
+  s.lambda = d->lambda; s.mu = d->mu; s.alpha = d->alpha; s.beta = d->beta;
+  s.rho_s = d->rho_s; s.ion_ion = d->ion_ion_energy;
+  s.alpha_eq_beta = d->alpha == d->beta ? 1 : 0;
+  s.pow56 = (s.alpha_eq_beta && std::fabs(d->alpha - 5.0 / 6.0) < 1e-15) ? 1 : 0;
+  s.nf = s.alpha_eq_beta ? 3 : 4;
+  s.ngroups = s.nf;
+  const int kinds[4] = {G_HARTREE, G_KMUL, G_VW, G_KMUL};
+  for (int g = 0; g < s.ngroups; ++g) { s.group_kind[g] = kinds[g]; s.group_f0[g] = g; s.group_nf[g] = 1; }
+  const size_t cs = sizeof(cx<double>);
+  const int nrows = s.n2 * s.n3, nrp = (nrows + 1) / 2;
+  const int rp1 = std::max(1, std::min(32, 2048 / s.n1));
+  s.rp = std::max(1, std::min(32, 1024 / s.n1));
+  while (s.rp > 1 && 2 * (size_t)s.nf * s.rp * s.n1 * cs > 72 * 1024) s.rp--;
+  s.tx = 16;
+  while (s.tx > 2 && 2 * (size_t)s.tx * std::max(s.n2, s.n3) * cs > 100 * 1024) s.tx /= 2;
+  s.ntask[K_X5] = (nrp + s.rp - 1) / s.rp;
+  s.buf[B_PHI] = (void*)rho;         // the input density (read only in EV_RHO mode)
+  s.buf[B_W0] = (void*)potential;    // the output potential
+  s.vion = (void*)ion_pot;
+  s.kern = (void*)kernel;
+  // task lists, packed one pass after the other
+  int nt[6] = {0, 0, 0, 0, 0, 0}, ntot = 0;
+  auto push = [&](int pass, Task t) -> bool {
+    if (ntot >= MAX_TASKS) return false;
+    g_tasks[ntot++] = t;
+    nt[pass]++;
+    return true;
+  };
+  bool ok = true;
+  for (int f = 0; f < s.nf && ok; ++f)
+    for (int r = 0; r < nrp && ok; r += rp1) ok = push(0, {0, f, r, std::min(rp1, nrp - r)});
+  for (int f = 0; f < s.nf && ok; ++f)
+    for (int z = 0; z < s.n3 && ok; ++z)
+      for (int kx = 0; kx < s.k1 && ok; kx += s.tx) ok = push(1, {0, f, z, kx});
+  for (int g = 0; g < s.ngroups && ok; ++g)
+    for (int ky = 0; ky < s.n2 && ok; ++ky)
+      for (int kx = 0; kx < s.k1 && ok; kx += s.tx) ok = push(2, {0, g, ky, kx});
+  int ord = 0;
+  for (int r = 0; r < nrp && ok; r += s.rp) ok = push(3, {0, r, std::min(s.rp, nrp - r), ord++});
+  if (ok) ok = push(4, {0, 0, 0, 0});
+  if (!ok) return fail(OFDFT_EINVAL, "grid needs more tasks than the allocation-free evaluation holds");
+  // scratch layout
+  size_t o = 0;
+  const size_t o_slot = o; o = up256(o + sizeof(SlotDev));
+  const size_t o_ctl = o; o = up256(o + sizeof(Ctl));
+  const size_t o_tw = o; o = up256(o + cs * (size_t)twoff);
+  const size_t o_part = o; o = up256(o + sizeof(double) * NCH * (size_t)s.ntask[K_X5]);
+  const size_t o_task = o; o = up256(o + sizeof(Task) * (size_t)ntot);
+  const size_t o_spec = o; o = up256(o + cs * (size_t)s.nf * (size_t)s.Nc);
+  if (o > SCRATCH_BYTES) return fail(OFDFT_EINVAL, "grid needs more scratch than the allocation-free evaluation holds");
+  s.partials = (double*)(base + o_part);
+  s.spec = (void*)(base + o_spec);
+  memset(&g_ctl, 0, sizeof(g_ctl));
+  g_ctl.status = ST_RUNNING;
+  g_ctl.iphi = B_PHI; g_ctl.itrial = B_TRIAL; g_ctl.iw0 = B_W0; g_ctl.iw1 = B_W1; g_ctl.evb = B_P;
+  g_ctl.ev = EV_RHO;
+  g_ctl.opt_sqrt = opt_sqrt ? 1 : 0;
+  g_ctl.want_energy = etable ? 1 : 0;
+  g_ctl.dscale = 1.0;
+  if ((rc = cuda_check(cudaMemcpyAsync(base + o_slot, &s, sizeof(SlotDev), cudaMemcpyHostToDevice, st), "H2D")))
+    return rc;
+  if ((rc = cuda_check(cudaMemcpyAsync(base + o_ctl, &g_ctl, sizeof(Ctl), cudaMemcpyHostToDevice, st), "H2D")))
+    return rc;
+  if ((rc = cuda_check(cudaMemcpyAsync(base + o_tw, g_tw, cs * (size_t)twoff, cudaMemcpyHostToDevice, st), "H2D")))
+    return rc;
+  if ((rc = cuda_check(cudaMemcpyAsync(base + o_task, g_tasks, sizeof(Task) * (size_t)ntot, cudaMemcpyHostToDevice,
+                                       st), "H2D")))
+    return rc;
+  // launches: passes 1-5 and the controller kernel, as one engine tick does
+  Args<double> a;
+  a.slots = (SlotDev*)(base + o_slot);
+  a.ctl = (Ctl*)(base + o_ctl);
+  a.tw = (const cx<double>*)(base + o_tw);
+  a.vchunk = VCHUNK;
+  const size_t sm1 = 2 * (size_t)rp1 * s.n1 * cs;
+  const size_t sm2 = 2 * (size_t)s.tx * s.n2 * cs;
+  const size_t sm3 = 2 * (size_t)s.tx * s.n3 * cs;
+  const size_t sm5 = 2 * (size_t)s.nf * s.rp * s.n1 * cs + NCH * 33 * sizeof(double) + 16;
+  auto attr = [&](auto kern, size_t sm) -> int {
+    if (sm <= 48 * 1024) return OFDFT_OK;
+    return cuda_check(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm),
+                      "cudaFuncSetAttribute");
+  };
+  if ((rc = attr(k_xfwd<double>, sm1)) || (rc = attr(k_ypass<double>, sm2)) || (rc = attr(k_zpass<double>, sm3)) ||
+      (rc = attr(k_xinv<double>, sm5)))
+    return rc;
+  const Task* tb = (const Task*)(base + o_task);
+  a.tasks = tb;
+  k_xfwd<double><<<nt[0], 256, sm1, st>>>(a);
+  a.tasks = tb + nt[0];
+  k_ypass<double><<<nt[1], 256, sm2, st>>>(a, -1);
+  a.tasks = tb + nt[0] + nt[1];
+  k_zpass<double><<<nt[2], 256, sm3, st>>>(a);
+  a.tasks = tb + nt[0];
+  k_ypass<double><<<nt[1], 256, sm2, st>>>(a, 1);
+  a.tasks = tb + nt[0] + nt[1] + nt[2];
+  k_xinv<double><<<nt[3], 256, sm5, st>>>(a);
+  a.tasks = tb + nt[0] + nt[1] + nt[2] + nt[3];
+  k_ctl<double><<<1, 64, 0, st>>>(a, (int)K_X5);
+  if ((rc = cuda_check(cudaGetLastError(), "kernel launch"))) return rc;
+  if ((rc = cuda_check(cudaMemcpyAsync(&g_ctl, base + o_ctl, sizeof(Ctl), cudaMemcpyDeviceToHost, st), "D2H")))
+    return rc;
+  if ((rc = cuda_check(cudaStreamSynchronize(st), "stream synchronize"))) return rc;
+  if ((rc = status_code(g_ctl))) return rc;
+  if (etable)
+    for (int k = 0; k < 9; ++k) etable[k] = g_ctl.energy[k];
+  return OFDFT_OK;
+#endif
+}
+

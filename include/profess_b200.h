@@ -179,6 +179,8 @@ int ofdft_calculate_potential_plus_noalloc(const ofdft_cell_desc* desc, const do
                                            void* stream);
 
 /* ---------------------------------------------------------------- batched / asynchronous */
+/* Upper bound of the device memory one slot of this description uses (bytes). */
+int ofdft_slot_footprint(const ofdft_cell_desc* desc, unsigned long long* bytes);
 /* Keep an input density resident on the device; start calls with rho = NULL use it. */
 int ofdft_slot_set_input(ofdft_engine* e, int slot, const double* rho);
 /* Start a solve from rho (host) or, with rho = NULL, from the resident input. */

@@ -1213,6 +1213,19 @@ int ofdft_slot_start_solve(ofdft_engine* e, int slot, const double* rho, const o
   return e->eng.start_solve(slot, rho, o);
 }
 
+int ofdft_slot_footprint(const ofdft_cell_desc* d, unsigned long long* bytes) {
+  if (!d || !bytes) return fail(OFDFT_EINVAL, "null argument");
+  const long long N = (long long)d->n1 * d->n2 * d->n3;
+  const long long Nc = (long long)(d->n1 / 2 + 1) * d->n2 * d->n3;
+  const long long es = d->precision == OFDFT_FP32 ? 4 : 8;
+  const long long nf = d->kinetic == KIN_WGC ? 8 : (d->alpha == d->beta ? 3 : 4);
+  const long long planes = d->kinetic == KIN_WGC ? 4 : 1;
+  // NBUF state arrays, ion potential, resident input, kernel planes, spectra, partials
+  *bytes = (unsigned long long)(es * N * (NBUF + 2) + es * Nc * planes + 2 * es * Nc * nf +
+                                8LL * NCH * (N / VCHUNK + 1 + d->n2 * (long long)d->n3) + (1 << 20));
+  return OFDFT_OK;
+}
+
 int ofdft_slot_set_input(ofdft_engine* e, int slot, const double* rho) {
   if (!e || !rho) return fail(OFDFT_EINVAL, "null argument");
   return e->eng.set_input(slot, rho);

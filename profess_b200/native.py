@@ -89,6 +89,7 @@ SIGNATURES = {
     "ofdft_slot_download": [_vp, ctypes.c_int, ctypes.c_int, _dp],
     "ofdft_slot_forces": [_vp, ctypes.c_int, _dp, ctypes.c_int, _dp],
     "ofdft_slot_set_input": [_vp, ctypes.c_int, _dp],
+    "ofdft_slot_footprint": [ctypes.POINTER(CellDesc), ctypes.POINTER(ctypes.c_ulonglong)],
     "ofdft_engine_stream": [_vp, ctypes.POINTER(_vp)],
     "ofdft_engine_counters": [_vp, ctypes.POINTER(ctypes.c_longlong), ctypes.POINTER(ctypes.c_longlong)],
     "ofdft_engine_time_eval": [_vp, ctypes.c_int, _dp],
@@ -112,6 +113,17 @@ def ewald(lib, lattice, frac, charges, want_forces=False):
     if rc:
         raise OfdftError(rc, lib.ofdft_last_error().decode())
     return float(e[0]), f
+
+
+def slot_footprint(lib, n, kinetic, alpha, beta, precision) -> int:
+    """Device bytes of one slot (upper bound), for admission control."""
+    d = CellDesc(int(n[0]), int(n[1]), int(n[2]), (ctypes.c_double * 9)(*([1.0] * 9)), int(kinetic), 1.0, 1.0,
+                 alpha, beta, 2.7, 0.0, 0.0, 0.0, int(precision))
+    b = ctypes.c_ulonglong()
+    rc = lib.ofdft_slot_footprint(ctypes.byref(d), ctypes.byref(b))
+    if rc:
+        raise OfdftError(rc, lib.ofdft_last_error().decode())
+    return int(b.value)
 
 
 def grid_size(lib, ecut_ha, lattice):

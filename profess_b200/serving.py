@@ -1,0 +1,175 @@
+"""Continuous-batching density-solve server on one GPU (one engine).
+
+Requests (a cell plus solve options) arrive over time; the server admits a
+waiting request when its device footprint fits the HBM budget and engine
+slots are free, builds its tables on the device, and starts its solve in the
+engine, where it shares every kernel launch with the solves already running.
+A mixed-precision request runs an FP32 slot until the FP32 line-search floor
+(or the FP32 tolerance), then FP64 refinement iterations in an FP64 slot
+started from the FP32 density on the device; a plain request runs FP64
+throughout.  Densities and solver state stay on the device until the result
+is read.  Finished slots are released at once, so waiting requests enter as
+soon as memory frees up.  Latency is arrival to result.
+
+Multi-GPU serving runs one server per GPU (replicas); ``partition`` assigns
+request ids to ranks with no exchange on the data path.
+"""
+from __future__ import annotations
+
+import dataclasses
+import time
+
+import numpy as np
+
+from . import native
+from .cell import setup_slot, ion_ion_energy
+from .workloads import Cell, initial_density
+
+MODE_MIXED = "mixed"
+MODE_FP64 = "fp64"
+
+
+@dataclasses.dataclass
+class Request:
+    rid: int
+    cell: Cell
+    arrival: float = 0.0          # seconds after the server's start
+    mode: str = MODE_MIXED
+    fp32_tol: float = 1.0e-5
+    refine_iters: int = 2
+    pot_tol: float = 1.0e-6
+    seed: int = 0
+
+
+@dataclasses.dataclass
+class Result:
+    rid: int
+    energy: np.ndarray
+    stats: dict
+    arrival: float
+    admitted: float
+    finished: float
+    nion: int
+    grid: tuple
+    mode: str
+
+    @property
+    def latency(self) -> float:
+        return self.finished - self.arrival
+
+
+def partition(rids, rank: int, world: int):
+    """Replica assignment of request ids to ranks (round robin)."""
+    return [r for r in rids if r % world == rank]
+
+
+def footprint(lib, cell: Cell, mode: str) -> int:
+    b64 = native.slot_footprint(lib, cell.grid, cell.kinetic, cell.alpha, cell.beta, native.FP64)
+    if mode == MODE_FP64:
+        return b64
+    return b64 + native.slot_footprint(lib, cell.grid, cell.kinetic, cell.alpha, cell.beta, native.FP32)
+
+
+class Server:
+    def __init__(self, engine: native.Engine, hbm_budget: int, max_active: int = 24, ticks_per_poll: int = 8,
+                 clock=time.perf_counter):
+        self.eng = engine
+        self.budget = int(hbm_budget)
+        self.max_active = max_active
+        self.ticks = ticks_per_poll
+        self.clock = clock
+        self.t0 = clock()
+        self.waiting = []            # requests that have arrived, FIFO
+        self.future = []             # requests not yet arrived (sorted by arrival)
+        self.active = {}             # rid -> dict(state)
+        self.used = 0
+        self.results = []
+
+    def now(self) -> float:
+        return self.clock() - self.t0
+
+    def submit(self, req: Request):
+        self.future.append(req)
+        self.future.sort(key=lambda r: r.arrival)
+
+    # ------------------------------------------------------------ admission
+    def _arrivals(self):
+        t = self.now()
+        while self.future and self.future[0].arrival <= t:
+            self.waiting.append(self.future.pop(0))
+
+    def _admit(self):
+        while self.waiting and len(self.active) < self.max_active:
+            req = self.waiting[0]
+            need = footprint(self.eng.lib, req.cell, req.mode)
+            if need > self.budget:
+                raise ValueError("request %d needs %d bytes, more than the whole budget" % (req.rid, need))
+            if self.used + need > self.budget:
+                return
+            self.waiting.pop(0)
+            t_adm = self.now()
+            e_ii = ion_ion_energy(self.eng.lib, req.cell)
+            rho0 = initial_density(req.cell, seed=req.seed)
+            st = {"req": req, "need": need, "admitted": t_adm, "phase": None, "s32": None, "s64": None}
+            if req.mode == MODE_FP64:
+                st["s64"] = setup_slot(self.eng, req.cell, native.FP64, ion_ion=e_ii)
+                self.eng.start_solve(st["s64"], rho0, native.ntn_options(
+                    conv_check=native.CONV_POT, pot_tol=req.pot_tol, max_iter=300))
+                st["phase"] = "fp64"
+            else:
+                st["s32"] = setup_slot(self.eng, req.cell, native.FP32, ion_ion=e_ii)
+                st["s64"] = setup_slot(self.eng, req.cell, native.FP64, ion_ion=e_ii)
+                self.eng.start_solve(st["s32"], rho0, native.ntn_options(
+                    conv_check=native.CONV_POT, pot_tol=req.fp32_tol, max_iter=300, stall_line=6))
+                st["phase"] = "fp32"
+            self.used += need
+            self.active[req.rid] = st
+
+    # ------------------------------------------------------------ progress
+    def _advance(self):
+        for rid in list(self.active):
+            st = self.active[rid]
+            req = st["req"]
+            if st["phase"] == "fp32" and self.eng.poll(st["s32"]):
+                self.eng.start_solve_from_slot(st["s64"], st["s32"], native.ntn_options(
+                    conv_check=native.CONV_POT, pot_tol=req.pot_tol, max_iter=req.refine_iters))
+                st["phase"] = "refine"
+            elif st["phase"] in ("refine", "fp64") and self.eng.poll(st["s64"]):
+                _, e, stats = self.eng.result(st["s64"], want_rho=False)
+                if st["s32"] is not None:
+                    _, _, s32 = self.eng.result(st["s32"], want_rho=False)
+                    stats = dict(stats, fp32_evals=s32["num_evals"], fp32_outcome=s32["outcome"])
+                self.results.append(Result(rid, e.copy(), stats, req.arrival, st["admitted"], self.now(),
+                                           req.cell.nion, req.cell.grid, req.mode))
+                for key in ("s32", "s64"):
+                    if st[key] is not None:
+                        self.eng.slot_destroy(st[key])
+                self.used -= st["need"]
+                del self.active[rid]
+
+    def step(self):
+        """Admit arrived requests, run the engine for one poll interval, retire finished phases."""
+        self._arrivals()
+        self._admit()
+        if self.active:
+            self.eng.run(self.ticks)
+            self._advance()
+            self._admit()
+
+    def run_until_done(self, timeout: float = 3600.0):
+        while self.future or self.waiting or self.active:
+            if self.now() > timeout:
+                raise TimeoutError("serving did not finish")
+            if not self.active and not self.waiting and self.future:
+                time.sleep(max(0.0, min(0.01, self.future[0].arrival - self.now())))
+            self.step()
+        return self.results
+
+
+def latency_stats(results):
+    lat = np.array([r.latency for r in results])
+    if len(lat) == 0:
+        return {}
+    span = max(r.finished for r in results) - min(r.arrival for r in results)
+    return {"p50_s": float(np.percentile(lat, 50)), "p99_s": float(np.percentile(lat, 99)),
+            "mean_s": float(lat.mean()), "solves": len(lat), "solves_per_s": len(lat) / span if span > 0 else None}

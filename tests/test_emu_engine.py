@@ -1,0 +1,191 @@
+"""The engine's kernel logic, run by the host-emulation build, against the oracle (CPU).
+
+tests/_emu/libprofess_b200_emu.so compiles the same block functions as the
+CUDA library for the host and runs every block with one thread.  These tests
+check the pass logic (FFT passes, field tables, k-space operators, epilogue,
+reductions, NTN controller, set-up passes) against the FP64 oracle at the
+tolerances the GPU tests use.  The GPU tests (test_gpu_*.py) repeat the
+parity checks on the CUDA build."""
+import numpy as np
+import pytest
+
+import cases
+from oracle import forces as ofo
+from oracle import functional as fn
+from oracle import kedf_kernels as kk
+from oracle import ntn
+from profess_b200 import native
+
+
+def _eval_parity(eng, f, cell, seed=1, opt_sqrt=True, prec=native.FP64, tol_pot=1e-11, tol_e=1e-10):
+    s = cases.engine_slot(eng, f, cell, precision=prec)
+    try:
+        rho = cases.random_density(f.n, cell.num_electrons, cell.vol, seed=seed)
+        pot_o, et_o = fn.calculate_potential_plus(f, rho, opt_sqrt=opt_sqrt)
+        pot_g, et_g = eng.calculate_potential_plus(s, rho, opt_sqrt=opt_sqrt)
+        assert np.abs(pot_g - pot_o).max() / np.abs(pot_o).max() < tol_pot
+        assert np.abs(et_g - et_o).max() < tol_e
+    finally:
+        eng.slot_destroy(s)
+
+
+@pytest.mark.parametrize("name", ["wt_al4_displaced", "wgc_al4_fcc"])
+@pytest.mark.parametrize("opt_sqrt", [True, False])
+def test_eval_golden_cells(emu_engine, name, opt_sqrt):
+    cell, f, _, _ = cases.golden_case(name)
+    _eval_parity(emu_engine, f, cell, opt_sqrt=opt_sqrt)
+
+
+@pytest.mark.parametrize("n", [(16, 18, 20), (15, 21, 14), (25, 12, 27), (7, 10, 9), (8, 14, 49), (2, 3, 5)])
+def test_eval_mixed_radix_and_odd_grids(emu_engine, n):
+    cell, _, _, _ = cases.golden_case("wt_al4_displaced")  # non-orthogonal lattice
+    f = cases.functional_for(cell, n, fn.KEDF_WT, 5 / 6, 5 / 6)
+    _eval_parity(emu_engine, f, cell, seed=2)
+
+
+def test_eval_wt_alpha_ne_beta(emu_engine):
+    cell, _, _, _ = cases.golden_case("wt_al4_displaced")
+    f = cases.functional_for(cell, (16, 16, 18), fn.KEDF_WT, 1.0, 2.0 / 3.0)
+    _eval_parity(emu_engine, f, cell, seed=3)
+
+
+def test_eval_fp32(emu_engine):
+    cell, f, _, _ = cases.golden_case("wgc_al4_fcc")
+    _eval_parity(emu_engine, f, cell, prec=native.FP32, tol_pot=1e-5, tol_e=2e-5)
+
+
+@pytest.mark.parametrize("name", ["wt_al4_displaced", "wgc_al4_fcc"])
+def test_solve_trajectory(emu_engine, name):
+    cell, f, rho_u, _ = cases.golden_case(name)
+    s = cases.engine_slot(emu_engine, f, cell)
+    try:
+        r_o = ntn.NtnSolver(f).solve(rho_u)
+        rho_g, e_g, st = emu_engine.proj_norm_rho_minimization(s, rho_u)
+        hist = emu_engine.history(s)
+        assert st["outcome"] == r_o.outcome == 0
+        assert st["num_evals"] == r_o.num_evals
+        assert [h["ncg"] for h in hist] == [h["ncg"] for h in r_o.history]
+        assert [h["nline"] for h in hist] == [h["nline"] for h in r_o.history]
+        assert np.abs(e_g - r_o.energy).max() < 1e-9
+        assert np.abs(rho_g - r_o.rho).max() < 1e-9
+    finally:
+        emu_engine.slot_destroy(s)
+
+
+def test_solve_pot_convergence_option(emu_engine):
+    cell, f, rho_u, _ = cases.golden_case("wt_al4_cell")
+    s = cases.engine_slot(emu_engine, f, cell)
+    try:
+        r_o = ntn.NtnSolver(f, ntn.NtnOptions(conv_check="POT", pot_tol=1e-7)).solve(rho_u)
+        _, e_g, st = emu_engine.proj_norm_rho_minimization(
+            s, rho_u, native.ntn_options(conv_check=native.CONV_POT, pot_tol=1e-7))
+        assert st["iterations"] == r_o.iterations and st["pot_norm"] < 1e-7
+        assert abs(e_g[0] - r_o.energy[0]) < 1e-10
+    finally:
+        emu_engine.slot_destroy(s)
+
+
+def test_batched_slots_match_single(emu_engine):
+    """Two different cells solved together give the same result as each alone."""
+    cell_a, f_a, rho_a, _ = cases.golden_case("wt_al4_displaced")
+    cell_b, f_b, rho_b, _ = cases.golden_case("wgc_al4_fcc")
+    sa = cases.engine_slot(emu_engine, f_a, cell_a)
+    sb = cases.engine_slot(emu_engine, f_b, cell_b)
+    try:
+        alone_a = emu_engine.proj_norm_rho_minimization(sa, rho_a)
+        alone_b = emu_engine.proj_norm_rho_minimization(sb, rho_b)
+        emu_engine.start_solve(sa, rho_a)
+        emu_engine.start_solve(sb, rho_b)
+        while emu_engine.run(8):
+            pass
+        ra, ea, _ = emu_engine.result(sa)
+        rb, eb, _ = emu_engine.result(sb)
+        assert np.array_equal(ea, alone_a[1]) and np.array_equal(ra, alone_a[0])
+        assert np.array_equal(eb, alone_b[1]) and np.array_equal(rb, alone_b[0])
+    finally:
+        emu_engine.slot_destroy(sa)
+        emu_engine.slot_destroy(sb)
+
+
+@pytest.mark.parametrize("name", ["wt_al4_displaced", "wgc_al4_fcc"])
+def test_device_setup_matches_oracle(emu_engine, name):
+    """WT/WGC kernels and the B-spline ion potential built by the library."""
+    cell, f, _, _ = cases.golden_case(name)
+    lib = emu_engine.lib
+    rho0 = cell.num_electrons / cell.vol
+    s = emu_engine.slot_create(f.n, cell.lattice, kinetic=f.kinetic, alpha=f.alpha, beta=f.beta, rho0=rho0,
+                               rho_s=f.rho_s, ion_ion=f.ion_ion)
+    try:
+        if f.kinetic == fn.KEDF_WT:
+            emu_engine.build_wt_kernel(s)
+        else:
+            tabs = native.wgc_radial_tables(lib, f.alpha, f.beta, 2.7)
+            ref = kk.wgc_radial_tables(f.alpha, f.beta, 2.7)
+            for a, b in zip(tabs, ref):
+                assert np.abs(a - b).max() <= 1e-5 * (1 + np.abs(b).max())
+            emu_engine.build_wgc_kernel(s, ref)  # same tables as the oracle: exact parity below
+        emu_engine.build_ion_potential(s, cell.frac, cell.species_of_ion, cell.species)
+        v = emu_engine.download(s, 2)
+        assert np.abs(v - f.ion_pot).max() < 1e-12
+        rho = cases.random_density(f.n, cell.num_electrons, cell.vol, seed=4)
+        pot_o, et_o = fn.calculate_potential_plus(f, rho)
+        pot_g, et_g = emu_engine.calculate_potential_plus(s, rho)
+        assert np.abs(pot_g - pot_o).max() / np.abs(pot_o).max() < 1e-11
+        assert np.abs(et_g - et_o).max() < 1e-10
+        F = emu_engine.forces(s, len(cell.frac), rho=rho)
+        Fo, _, _ = ofo.total_forces(cell, rho)
+        assert np.abs(F - Fo).max() < 1e-10
+    finally:
+        emu_engine.slot_destroy(s)
+
+
+def test_mixed_precision_refinement(emu_engine):
+    """FP32 solve to its floor, FP64 refinement from the device-resident result."""
+    cell, f, rho_u, _ = cases.golden_case("wt_al4_displaced")
+    s32 = cases.engine_slot(emu_engine, f, cell, precision=native.FP32)
+    s64 = cases.engine_slot(emu_engine, f, cell, precision=native.FP64)
+    try:
+        ref = ntn.NtnSolver(f, ntn.NtnOptions(conv_check="POT", pot_tol=1e-7)).solve(rho_u)
+        emu_engine.start_solve(s32, rho_u, native.ntn_options(conv_check=native.CONV_POT, pot_tol=1e-6,
+                                                              stall_line=6))
+        while emu_engine.run(8):
+            pass
+        _, e32, st32 = emu_engine.result(s32, want_rho=False)
+        emu_engine.start_solve_from_slot(s64, s32, native.ntn_options(conv_check=native.CONV_POT,
+                                                                      pot_tol=1e-7, max_iter=3))
+        while emu_engine.run(8):
+            pass
+        _, e64, st64 = emu_engine.result(s64, want_rho=False)
+        nat = len(cell.frac)
+        ev = 27.2113834
+        assert abs(e64[0] - ref.energy[0]) * ev / nat < 1e-5
+        assert st32["num_evals"] > 0 and st64["iterations"] <= 3
+    finally:
+        emu_engine.slot_destroy(s32)
+        emu_engine.slot_destroy(s64)
+
+
+def test_nan_density_reports_status(emu_engine):
+    cell, f, _, _ = cases.golden_case("wt_al4_displaced")
+    s = cases.engine_slot(emu_engine, f, cell)
+    try:
+        rho = cases.random_density(f.n, cell.num_electrons, cell.vol, seed=1)
+        rho[3, 4, 5] = np.nan
+        with pytest.raises(native.OfdftError) as ei:
+            emu_engine.calculate_potential_plus(s, rho)
+        assert ei.value.code == 5
+    finally:
+        emu_engine.slot_destroy(s)
+
+
+def test_invalid_slot_arguments(emu_engine):
+    cell, f, _, _ = cases.golden_case("wt_al4_displaced")
+    with pytest.raises(native.OfdftError) as ei:
+        emu_engine.slot_create((16, 16, 11), cell.lattice)  # 11 is not 7-smooth
+    assert ei.value.code == 1
+    s = cases.engine_slot(emu_engine, f, cell)
+    try:
+        with pytest.raises(native.OfdftError):
+            emu_engine.set_kernel(s, np.zeros((4,) + f.kernel.shape[1:]))  # WT takes one plane
+    finally:
+        emu_engine.slot_destroy(s)

@@ -3,7 +3,7 @@
 
 Workload (the configuration the headline metric is quoted on): FCC Al 4x4x4
 supercell, 256 atoms, a = 4.05 A, seeded Gaussian displacements sigma =
-0.05 A, GHA-style local pseudopotential (Z = 3, r_c = 1.15 bohr, A = 0.1 Ha),
+0.05 A, Heine-Abarenkov model pseudopotential (Z = 3, r_c = 1.15 bohr, well depth A = 0.1 Ha),
 WT + TF + vW + LDA, 96^3 grid.  One "step" is a batch of B such cells (distinct
 seeds) each solved to convergence by the sqrt-density truncated-Newton method:
 FP32 evaluations until the line search reaches the FP32 precision floor (or
@@ -173,7 +173,7 @@ def run_reference(args):
            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * tot / args.steps,
            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
            "data": "synthetic (seeded)",
-           "config": {"workload": "FCC Al 4x4x4 (256 atoms), 96^3, WT+TF+vW+LDA, GHA psp, NTN to potNorm<1e-6",
+           "config": {"workload": "FCC Al 4x4x4 (256 atoms), 96^3, WT+TF+vW+LDA, Heine-Abarenkov psp, NTN to potNorm<1e-6",
                       "batch_per_step": 1, "parallelism": "cpu"},
            "cpu_baseline": {"value": v, "unit": UNIT, "cores": cores, "kind": "port",
                             "sample": "%d full FP64 NTN solve(s) of the workload by the oracle "
@@ -187,6 +187,33 @@ def run_reference(args):
 
 
 # --------------------------------------------------------------------------- GPU arm
+WORKLOADS = {
+    "cfg2": "FCC Al 4x4x4 (256 atoms), a=4.05 A, sigma=0.05 A, 96^3, WT(alpha=beta=5/6)+TF+vW+LDA, Heine-Abarenkov psp",
+    "cfg1": "FCC Al conventional cell (4 atoms), sigma=0.02 A, 32^3, WT+TF+vW+LDA, Heine-Abarenkov psp",
+    "cfg3": "64 FCC Al cells n^3 (n~U{2..5}, 32-500 atoms), a=4.05 A (1+-2%), 48^3-120^3, WT, one batch",
+    "cfg4": "hcp Mg 8x8x9 (1152 atoms), a=3.21 A, c/a=1.624, sigma=0.05 A, 160x160x256, WGC 2nd order",
+}
+
+
+def make_cells(args, rank):
+    from profess_b200 import workloads as wl
+    if args.workload == "cfg3":
+        return [wl.config_cell(3, seed=1 + rank, index=i) for i in range(args.batch or 64)]
+    cfg = {"cfg1": 1, "cfg2": 2, "cfg4": 4}[args.workload]
+    default_b = {"cfg1": 16, "cfg2": 16, "cfg4": 1}[args.workload]
+    return [wl.config_cell(cfg, seed=1000 * rank + b) for b in range(args.batch or default_b)]
+
+
+def eval_bytes(cell, s):
+    """Algorithmic bytes of one potential evaluation: s N (2F + 4 + k/2)."""
+    n = float(np.prod(cell.grid))
+    if cell.kinetic == 5:
+        F, k = 16, 4
+    else:
+        F, k = (6 if cell.alpha == cell.beta else 8), 1
+    return s * n * (2 * F + 4 + k / 2.0)
+
+
 def run_ours(args):
     import torch
     ws, rank, local = _dist()
@@ -200,9 +227,12 @@ def run_ours(args):
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
     from profess_b200 import cell as pcell
     from profess_b200 import native, workloads as wl
+    from profess_b200.recpot import HARTREE_TO_EV
+    if args.workload == "serving":
+        return run_serving(args, ws, rank, local, dist)
     eng = native.Engine()
-    B = args.batch
-    cells = [wl.config_cell(2, seed=1000 * rank + b) for b in range(B)]
+    cells = make_cells(args, rank)
+    B = len(cells)
     rho0 = [wl.initial_density(c, seed=1000 * rank + b) for b, c in enumerate(cells)]
     s32, s64 = [], []
     for c, r in zip(cells, rho0):
@@ -213,9 +243,13 @@ def run_ours(args):
         eng.set_input(b, r)
         s32.append(a)
         s64.append(b)
-    o32 = native.ntn_options(conv_check=native.CONV_POT, pot_tol=args.fp32_tol, max_iter=200, stall_line=6)
+    o32 = native.ntn_options(conv_check=native.CONV_POT, pot_tol=args.fp32_tol, max_iter=300, stall_line=6)
     oref = native.ntn_options(conv_check=native.CONV_POT, pot_tol=1.0e-6, max_iter=args.refine)
-    o64 = native.ntn_options(conv_check=native.CONV_POT, pot_tol=1.0e-6, max_iter=200)
+    # The plain FP64 path runs the same solver rules in FP64 throughout, the
+    # line-search stall exit included: without it a few cells stagnate just
+    # above potNorm 1e-6 with the energy already converged to round-off (the
+    # FP64 NTN line search then needs tens of trials per iteration).
+    o64 = native.ntn_options(conv_check=native.CONV_POT, pot_tol=1.0e-6, max_iter=300, stall_line=6)
     stream = torch.cuda.ExternalStream(eng.stream())
 
     def run_all(slots, t0, done_at):
@@ -238,9 +272,10 @@ def run_ours(args):
             eng.start_solve_from_slot(b, a, oref)
         run_all(s64, t0, done)
         res = []
-        for b in s64:
-            rho, e, st = eng.result(b, want_rho=host)
-            res.append((e, st))
+        for a, b in zip(s32, s64):
+            _, e, st = eng.result(b, want_rho=host)
+            _, _, st32 = eng.result(a, want_rho=False)
+            res.append((e, st, st32))
         return res, [done[b] for b in s64]
 
     def fp64_step():
@@ -274,12 +309,11 @@ def run_ours(args):
     ev1 = torch.cuda.Event(enable_timing=True)
     lat = []
     mixed_res = None
-    with torch.cuda.stream(stream):
-        ev0.record(stream)
-        for _ in range(args.steps):
-            mixed_res, l = mixed_step()
-            lat.extend(l)
-        ev1.record(stream)
+    ev0.record(stream)
+    for _ in range(args.steps):
+        mixed_res, l = mixed_step()
+        lat.extend(l)
+    ev1.record(stream)
     barrier()
     l1, _ = eng.counters()
     clk = clocks.stop()
@@ -300,9 +334,10 @@ def run_ours(args):
     barrier()
     t_fp64 = max_over_ranks(ev0.elapsed_time(ev1) / 1e3)
     fp64_value = ws * B * args.steps / t_fp64
-    from profess_b200.recpot import HARTREE_TO_EV as hartree_ev
-    errs = [abs(m[0][0] - f[1][0]) * hartree_ev / c.nion for m, f, c in zip(mixed_res, fp64_res, cells)]
-    evals_mixed = [m[1]["num_evals"] for m in mixed_res]
+    errs = [abs(m[0][0] - f[1][0]) * HARTREE_TO_EV / c.nion for m, f, c in zip(mixed_res, fp64_res, cells)]
+    evals32 = [m[2]["num_evals"] for m in mixed_res]
+    evals_ref = [m[1]["num_evals"] for m in mixed_res]
+    evals64 = [f[2]["num_evals"] for f in fp64_res]
 
     # ---------------- end to end through the public API with host buffers
     barrier()
@@ -311,21 +346,18 @@ def run_ours(args):
         mixed_step(host=True)
     barrier()
     t_e2e = max_over_ranks(time.perf_counter() - t0)
-    N = int(np.prod(cells[0].grid))
-    h2d = B * N * 4
-    d2h = B * (N * 8 + 9 * 8)
+    h2d = int(sum(np.prod(c.grid) * 4 for c in cells))
+    d2h = int(sum(np.prod(c.grid) * 8 + 9 * 8 for c in cells))
 
-    # ---------------- roofline probe: batched FP32 potential evaluations
-    ms_eval = eng.time_eval(iters=10)  # every idle slot with an input: B FP32 + B FP64
-    n_fp32, n_fp64 = len(s32), len(s64)
-    b_eval = lambda s: s * N * (2 * 6 + 4 + 0.5)  # bytes per WT (alpha = beta) evaluation
-    alg_bytes = n_fp32 * b_eval(4) + n_fp64 * b_eval(8)
+    # ---------------- roofline probe: batched potential evaluations of every slot
+    ms_eval = eng.time_eval(iters=10)
+    alg_bytes = sum(eval_bytes(c, 4) + eval_bytes(c, 8) for c in cells)
     achieved = alg_bytes / (ms_eval / 1e3) / 1e9
     peak, peak_kind = _peaks()
-    tr = _traffic_per_eval()
+    tr = _traffic_per_eval() if args.workload == "cfg2" else None
 
     cpu = None
-    if rank == 0 and ws == 1 and not args.no_cpu_baseline:
+    if rank == 0 and ws == 1 and not args.no_cpu_baseline and args.workload == "cfg2":
         t_cpu, _ = cpu_solve_time(cells[0], rho0[0])
         cpu = {"value": 1.0 / t_cpu, "unit": UNIT, "cores": os.cpu_count() or 1, "kind": "port",
                "sample": "one FP64 NTN solve (to potNorm < 1e-6) of one cell of the workload by the "
@@ -338,27 +370,27 @@ def run_ours(args):
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": 1e3 * t_mixed / args.steps, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f32+f64",
-        "data": "synthetic (seeded FCC Al cells)",
-        "config": {"workload": "FCC Al 4x4x4 (256 atoms), a=4.05 A, sigma=0.05 A, 96^3, WT(alpha=beta=5/6)+TF+vW"
-                               "+LDA, GHA-style psp; NTN: FP32 to potNorm<%g or the FP32 line-search floor, then <=%d FP64 iterations"
-                               % (args.fp32_tol, args.refine),
+        "data": "synthetic (seeded cells)",
+        "config": {"workload": WORKLOADS[args.workload] + "; NTN: FP32 to potNorm<%g or the FP32 line-search floor, "
+                                                          "then <=%d FP64 iterations" % (args.fp32_tol, args.refine),
                    "batch_per_step": B, "parallelism": "replicas x%d" % ws,
-                   "l2_flush": "not needed: working set %.1f GB > 126 MB L2" % (B * 0.16)},
+                   "l2_flush": "not needed: batch working set above the 126 MB L2"},
         "fp64_gpu": {"value": fp64_value, "unit": UNIT, "ms_per_step": 1e3 * t_fp64 / args.steps,
+                     "evals_per_solve": float(np.mean(evals64)),
                      "latency_ms": {"p50": 1e3 * float(np.percentile(lat64, 50)),
                                     "p99": 1e3 * float(np.percentile(lat64, 99))}},
         "mixed_over_fp64": value / fp64_value,
         "energy_error_ev_per_atom_max": max(errs),
         "latency_ms": {"p50": 1e3 * float(np.percentile(lat, 50)), "p99": 1e3 * float(np.percentile(lat, 99))},
-        "evals_per_solve_mixed": float(np.mean(evals_mixed)),
+        "evals_per_solve_mixed": {"fp32": float(np.mean(evals32)), "fp64_refine": float(np.mean(evals_ref))},
         "e2e": {"value": ws * B * args.steps / t_e2e, "unit": UNIT, "h2d_bytes_per_step": h2d,
                 "d2h_bytes_per_step": d2h},
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                      "frac": achieved / peak, "peak_source": peak_kind,
-                     "kernel": "batched potential evaluation (passes 1-5 + controller), %d FP32 + %d FP64 "
-                               "cells of 96^3" % (n_fp32, n_fp64),
+                     "kernel": "batched potential evaluation (passes 1-5 + controller) of every cell in FP32 and "
+                               "FP64 (%d slots)" % (2 * B),
                      "ms_per_launch": ms_eval,
-                     "traffic": (tr * n_fp32 + 2 * tr * n_fp64) if tr else None},
+                     "traffic": (3 * tr * B) if tr else None},
         "cpu_baseline": cpu,
         "clocks": clk,
         "gpu_launches": l1 - l0,
@@ -369,13 +401,57 @@ def run_ours(args):
     return 0
 
 
+def run_serving(args, ws, rank, local, dist):
+    """Poisson stream of mixed-precision requests at 80% of the measured capacity."""
+    import torch
+    from profess_b200 import native, serving, workloads as wl
+    eng = native.Engine()
+    rng = np.random.default_rng(12345 + rank)
+    nreq = args.requests
+    cells = [wl.serving_cell(rng) for _ in range(nreq)]
+    free, _total = torch.cuda.mem_get_info()
+    budget = int(0.8 * free)
+    # capacity: everything arrives at once (saturated server)
+    srv = serving.Server(eng, budget, max_active=args.max_active)
+    for i, c in enumerate(cells):
+        srv.submit(serving.Request(rid=i, cell=c, arrival=0.0, seed=i, fp32_tol=args.fp32_tol,
+                                   refine_iters=args.refine))
+    res = srv.run_until_done(timeout=3600)
+    cap = serving.latency_stats(res)["solves_per_s"]
+    # 80% load, Poisson arrivals
+    lam = 0.8 * cap
+    t = 0.0
+    srv = serving.Server(eng, budget, max_active=args.max_active)
+    for i, c in enumerate(cells):
+        t += float(rng.exponential(1.0 / lam))
+        srv.submit(serving.Request(rid=i, cell=c, arrival=t, seed=i, fp32_tol=args.fp32_tol,
+                                   refine_iters=args.refine))
+    res = srv.run_until_done(timeout=3600)
+    st = serving.latency_stats(res)
+    if rank != 0:
+        return 0
+    out = {"metric": METRIC, "value": st["solves_per_s"] * ws, "unit": UNIT, "n_gpus": ws, "steps": nreq,
+           "warmup": 0, "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32+f64",
+           "data": "synthetic Poisson request stream (seeded)",
+           "config": {"workload": "serving: Al/Mg cells, 32-2048 atoms (log-uniform), grids 32^3-256^3, "
+                                  "70% WT / 30% WGC, sigma U[0.03,0.1] A; arrivals Poisson at 80% of capacity",
+                      "requests": nreq, "capacity_solves_per_s": cap, "arrival_rate_per_s": lam},
+           "latency_s": {"p50": st["p50_s"], "p99": st["p99_s"], "mean": st["mean_s"]},
+           "atoms_per_request_mean": float(np.mean([c.nion for c in cells]))}
+    print(json.dumps(out), flush=True)
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--batch", type=int, default=16)
+    ap.add_argument("--batch", type=int, default=0, help="cells per step (0: the workload's default)")
+    ap.add_argument("--workload", default="cfg2", choices=["cfg2", "cfg1", "cfg3", "cfg4", "serving"])
+    ap.add_argument("--requests", type=int, default=48, help="serving: number of requests")
+    ap.add_argument("--max-active", type=int, default=24, help="serving: concurrent requests")
     ap.add_argument("--fp32-tol", type=float, default=1.0e-5)
     ap.add_argument("--refine", type=int, default=2)
     ap.add_argument("--no-cpu-baseline", action="store_true")

@@ -62,8 +62,6 @@ static int dmalloc(void** p, size_t n) {
 static void dfree(void* p) { if (p) cudaFree(p); }
 static int h2d(void* d, const void* h, size_t n) { return cuda_check(cudaMemcpy(d, h, n, cudaMemcpyHostToDevice), "H2D"); }
 static int d2h(void* h, const void* d, size_t n) { return cuda_check(cudaMemcpy(h, d, n, cudaMemcpyDeviceToHost), "D2H"); }
-static int d2d(void* d, const void* s, size_t n) { return cuda_check(cudaMemcpy(d, s, n, cudaMemcpyDeviceToDevice), "D2D"); }
-static int dzero(void* d, size_t n) { return cuda_check(cudaMemset(d, 0, n), "cudaMemset"); }
 static int dsync() { return cuda_check(cudaDeviceSynchronize(), "synchronize"); }
 #endif
 
@@ -265,6 +263,30 @@ struct Engine {
     if (rc) return rc;
     return cuda_check(cudaStreamSynchronize(stream), "stream synchronize");
   }
+  // The engine's copies, fills and zeroed allocations go through its own
+  // (non-blocking) stream and return once they are complete.  Plain
+  // cudaMemcpy/cudaMemset run on the legacy default stream, which a
+  // non-blocking stream does not wait for: a kernel launched right after them
+  // could read the old contents (a device-to-device copy or a memset returns
+  // to the host before it has run).
+  int on_stream(cudaError_t e, const char* what) {
+    int rc = cuda_check(e, what);
+    return rc ? rc : cuda_check(cudaStreamSynchronize(stream), "stream synchronize");
+  }
+  int h2d(void* d, const void* h, size_t n) {
+    return on_stream(cudaMemcpyAsync(d, h, n, cudaMemcpyHostToDevice, stream), "H2D");
+  }
+  int d2h(void* h, const void* d, size_t n) {
+    return on_stream(cudaMemcpyAsync(h, d, n, cudaMemcpyDeviceToHost, stream), "D2H");
+  }
+  int d2d(void* d, const void* s, size_t n) {
+    return on_stream(cudaMemcpyAsync(d, s, n, cudaMemcpyDeviceToDevice, stream), "D2D");
+  }
+  int dzero(void* d, size_t n) { return on_stream(cudaMemsetAsync(d, 0, n, stream), "cudaMemsetAsync"); }
+  int dmalloc(void** p, size_t n) {
+    int rc = cuda_check(cudaMalloc(p, n ? n : 1), "cudaMalloc");
+    return rc ? rc : dzero(*p, n ? n : 1);
+  }
 #endif
 
   int init(int capacity) {
@@ -278,7 +300,8 @@ struct Engine {
     if (rc) return rc;
     rc = dmalloc((void**)&d_ctl, sizeof(Ctl) * cap);
     if (rc) return rc;
-    return plans.build();
+    if ((rc = plans.build())) return rc;
+    return dsync();  // the plan tables were copied on the legacy stream
   }
 
   void release() {
@@ -1156,7 +1179,7 @@ int ofdft_version(void) { return 1; }
 int ofdft_engine_create(ofdft_engine** out) {
   if (!out) return fail(OFDFT_EINVAL, "null output");
   ofdft_engine* e = new ofdft_engine();
-  int rc = e->eng.init(64);
+  int rc = e->eng.init(256);
   if (rc) {
     e->eng.release();
     delete e;

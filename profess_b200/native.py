@@ -184,7 +184,7 @@ def ntn_options(max_iter=500, conv_check=CONV_ENE, pot_tol=1.0e-5, tole=1.0e-6, 
 
 
 class Engine:
-    """An engine holding up to 64 slots (cells) on the current GPU."""
+    """An engine holding up to 256 slots (cells) on the current GPU."""
 
     def __init__(self, lib: ctypes.CDLL | str | None = None):
         self.lib = lib if isinstance(lib, ctypes.CDLL) else load_library(lib)

@@ -2,15 +2,18 @@
 
 All inputs are generated, none are read from a dataset:
 
-* ``gha_species``: a Goodwin-Heine-Abarenkov-style local pseudopotential with
-  ionic charge Z, core radius r_c and well depth A, tabulated as a recpot
-  table (q spacing 0.002 bohr^-1 up to 30 bohr^-1, as in al_HC.lda.recpot).
-  Its real-space form is -Z/r outside r_c and, inside, the C1-continuous
-  -(Z / 2 r_c)(3 - r^2/r_c^2) - A (1 - r^2/r_c^2)^2; v(q) = 4 pi int r^2 V(r)
-  j0(qr) dr is evaluated as -4 pi Z/q^2 plus a Gauss-Legendre quadrature of the
-  core correction.  (The exact published GHA form was not available offline;
-  this form keeps the three named parameters and the Coulomb tail the recpot
-  reader needs to infer Z.)
+* ``gha_species``: the Heine-Abarenkov model potential (V. Heine and
+  I. Abarenkov, Phil. Mag. 9, 451 (1964)) that the Goodwin-Heine-Abarenkov
+  local pseudopotential is built on: a constant well of depth A inside the
+  model radius r_c and the bare Coulomb tail -Z/r outside it.  Its transform
+  is analytic, v(q) = -(4 pi / q^2) [Z cos(q r_c) + (A/q)(sin(q r_c) -
+  q r_c cos(q r_c))], with the finite q -> 0 part 2 pi Z r_c^2 -
+  4 pi A r_c^3 / 3 stored at q = 0.  It is tabulated as a recpot table (q
+  spacing 0.002 bohr^-1 up to 30 bohr^-1, as in al_HC.lda.recpot), so the
+  recpot reader's charge inference recovers Z from the -4 pi Z / q^2 tail.
+  (The smoothing that Goodwin, Needs and Heine add on top was not available
+  offline; the shallow well already keeps the valence density smooth at the
+  cores, which the second-order WGC expansion needs.)
 * ``fcc_al``: FCC aluminium supercells of the 4-atom conventional cell.
 * ``hcp_mg``: hexagonal magnesium supercells of the 2-atom primitive cell.
 * ``Cell``: lattice (bohr, columns = lattice vectors), fractional positions,
@@ -59,21 +62,16 @@ _GHA_CACHE = {}
 
 
 def gha_table(z: float, rc: float, a_well: float, dq: float = 0.002, npts: int = 15003):
-    """(max_g in 1/A, values in eV*A^3) of the GHA-style pseudopotential."""
+    """(max_g in 1/A, values in eV*A^3) of the Heine-Abarenkov model potential."""
     key = (z, rc, a_well, dq, npts)
     if key in _GHA_CACHE:
         return _GHA_CACHE[key]
-    x, w = np.polynomial.legendre.leggauss(256)
-    r = 0.5 * rc * (x + 1.0)
-    wr = 0.5 * rc * w
-    vin = -(z / (2.0 * rc)) * (3.0 - (r / rc) ** 2) - a_well * (1.0 - (r / rc) ** 2) ** 2
-    corr = r * r * vin + z * r          # r^2 (V_in + Z/r)
     q = np.arange(npts, dtype=float) * dq
     vals = np.empty(npts)
-    vals[0] = 4.0 * math.pi * float(np.sum(wr * corr))
-    qq = q[1:, None]
-    j0 = np.sin(qq * r[None, :]) / (qq * r[None, :])
-    vals[1:] = -4.0 * math.pi * z / q[1:] ** 2 + 4.0 * math.pi * (j0 * (wr * corr)[None, :]).sum(axis=1)
+    vals[0] = 2.0 * math.pi * z * rc ** 2 - 4.0 * math.pi * a_well * rc ** 3 / 3.0
+    qq = q[1:]
+    x = qq * rc
+    vals[1:] = -(4.0 * math.pi / qq ** 2) * (z * np.cos(x) + (a_well / qq) * (np.sin(x) - x * np.cos(x)))
     max_g_ang = (npts - 1) * dq / BOHR
     out = (max_g_ang, vals * BOHR ** 3 * HARTREE_TO_EV)
     _GHA_CACHE[key] = out
@@ -183,3 +181,43 @@ def config_cell(cfg: int, seed: int = 0, index: int = 0) -> Cell:
     if cfg == 4:
         return hcp_mg((8, 8, 9), sigma_ang=0.05, grid=(160, 160, 256), seed=seed)
     raise ValueError("unknown config %r" % cfg)
+
+
+def _near_cubic_reps(count: int, shape=(1.0, 1.0, 1.0)):
+    """Integer supercell repeats with product close to count and lengths close to a cube."""
+    best = None
+    for a in range(1, 33):
+        for b in range(1, 33):
+            c = max(1, int(round(count / float(a * b))))
+            if a * b * c == 0:
+                continue
+            lens = np.array([a * shape[0], b * shape[1], c * shape[2]])
+            score = abs(a * b * c - count) / count + 0.3 * (lens.max() / lens.min() - 1.0)
+            if best is None or score < best[0]:
+                best = (score, (a, b, c))
+    return best[1]
+
+
+def serving_cell(rng) -> Cell:
+    """One request of the serving mix: Al or Mg, atom count log-uniform in
+    [32, 2048], KEDF 70% WT / 30% WGC, sigma ~ U[0.03, 0.1] A, grids 32-256
+    points per axis (about 6 points per A, 7-smooth)."""
+    species = "Al" if rng.random() < 0.5 else "Mg"
+    natoms = float(np.exp(rng.uniform(np.log(32.0), np.log(2048.0))))
+    kinetic = 4 if rng.random() < 0.7 else 5
+    sigma = float(rng.uniform(0.03, 0.1))
+    seed = int(rng.integers(1 << 30))
+    if species == "Al":
+        reps = _near_cubic_reps(max(1, int(round(natoms / 4.0))))
+        cell = fcc_al(reps, sigma_ang=sigma, seed=seed, kinetic=kinetic)
+    else:
+        reps = _near_cubic_reps(max(1, int(round(natoms / 2.0))), shape=(1.0, 1.0, 1.624))
+        cell = hcp_mg(reps, sigma_ang=sigma, seed=seed, kinetic=kinetic)
+    lengths = np.sqrt((cell.lattice ** 2).sum(axis=0)) * BOHR
+    cell.grid = tuple(min(256, max(32, smooth_size(5.9 * L))) for L in lengths)
+    if kinetic == 5:
+        cell.alpha = (5.0 + math.sqrt(5.0)) / 6.0
+        cell.beta = (5.0 - math.sqrt(5.0)) / 6.0
+    else:
+        cell.alpha = cell.beta = 5.0 / 6.0
+    return cell

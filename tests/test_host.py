@@ -59,6 +59,22 @@ def test_gha_tables_have_the_coulomb_tail():
         assert np.all(np.abs(tail / (-4 * np.pi * z) - 1.0) < 1e-4)
 
 
+def test_gha_table_is_the_transform_of_the_model_potential():
+    """v(q) + 4 pi Z / q^2 = 4 pi int_0^rc r^2 (-A + Z/r) j0(qr) dr (quadrature)."""
+    from profess_b200.recpot import BOHR, HARTREE_TO_EV
+    z, rc, a = 2.0, 1.3, 0.1
+    mx, vals = wl.gha_table(z, rc, a)
+    v = vals / (BOHR ** 3 * HARTREE_TO_EV)
+    x, w = np.polynomial.legendre.leggauss(64)
+    r, wr = 0.5 * rc * (x + 1.0), 0.5 * rc * w
+    for k in [0, 1, 7, 150, 2000, 15002]:
+        q = 0.002 * k
+        j0 = np.sinc(q * r / np.pi)
+        short = 4 * np.pi * float(np.sum(wr * r * r * (-a + z / r) * j0))
+        coul = 0.0 if k == 0 else -4 * np.pi * z / q ** 2
+        assert abs(v[k] - coul - short) < 1e-10 * max(1.0, abs(coul))
+
+
 @pytest.mark.parametrize("name", ["wt_al4_displaced", "wgc_al4_fcc"])
 def test_ewald_matches_oracle(lib, name):
     cell, _, _, _ = cases.golden_case(name)

@@ -14,9 +14,11 @@
 #if defined(__CUDACC__)
 #define HD __host__ __device__ __forceinline__
 #define HDNI __host__ __device__
+#define HDC __host__ __device__ constexpr
 #else
 #define HD inline
 #define HDNI
+#define HDC constexpr
 #endif
 
 #if defined(__CUDA_ARCH__)

@@ -73,55 +73,90 @@ static bool seven_smooth(int n) {
   return n == 1;
 }
 
-// Radix sequence of n: as many 8s as possible, then one 4 or 2, then 3, 5, 7.
-static std::vector<int> radices(int n) {
+// Radix sequence of n: the fewest stages with radices from {2, ..., rmax}
+// (7-smooth), then the smallest largest radix; the largest radix goes first
+// (the first Stockham stage has no twiddles).
+static std::vector<int> radices(int n, int rmax) {
+  static const int kR[] = {16, 15, 14, 12, 10, 9, 8, 7, 6, 5, 4, 3, 2};
+  // best[m] = (stages, largest radix, first radix) for m | n, by increasing m
+  std::map<int, std::pair<int, int>> cost;  // m -> (stages, largest radix)
+  std::map<int, int> first;
+  cost[1] = {0, 0};
+  std::vector<int> divs;
+  for (int m = 2; m <= n; ++m)
+    if (n % m == 0) divs.push_back(m);
+  for (int m : divs) {
+    std::pair<int, int> best = {1 << 20, 1 << 20};
+    int bf = 0;
+    for (int R : kR) {
+      if (R > rmax || m % R || !cost.count(m / R)) continue;
+      const std::pair<int, int> c = {cost[m / R].first + 1, std::max(R, cost[m / R].second)};
+      if (c < best) { best = c; bf = R; }
+    }
+    cost[m] = best;
+    first[m] = bf;
+  }
   std::vector<int> r;
-  int e2 = 0;
-  while (n % 2 == 0) { n /= 2; ++e2; }
-  while (e2 >= 3) { r.push_back(8); e2 -= 3; }
-  if (e2 == 2) r.push_back(4);
-  if (e2 == 1) r.push_back(2);
-  for (int p : {3, 5, 7})
-    while (n % p == 0) { r.push_back(p); n /= p; }
+  for (int m = n; m > 1; m /= first[m]) r.push_back(first[m]);
+  std::sort(r.begin(), r.end(), [](int a, int b) { return a > b; });
   return r;
 }
 
 constexpr int MAX_N = 512;
 
+// Largest radix of the FP32 and FP64 plans (OFDFT_RMAX_* in fft.cuh) and the
+// minimum resident 256-thread blocks per SM of the FFT pass kernels, per
+// precision (it caps their registers at 65536 / (256 * minb)).  The passes are
+// bound by shared-memory and global-memory latency rather than by arithmetic:
+// on 16 cells of 96^3, radix <= 8 with 4 blocks per SM (64 registers) was
+// faster than radix <= 16 with 2 blocks per SM, in both precisions.
+#ifndef OFDFT_MINB_FP32
+#define OFDFT_MINB_FP32 4
+#endif
+#ifndef OFDFT_MINB_FP64
+#define OFDFT_MINB_FP64 4
+#endif
+constexpr int RMAX_FP32 = OFDFT_RMAX_FP32;
+constexpr int RMAX_FP64 = OFDFT_RMAX_FP64;
+template <typename T> struct PassMinBlocks { static constexpr int value = OFDFT_MINB_FP32; };
+template <> struct PassMinBlocks<double> { static constexpr int value = OFDFT_MINB_FP64; };
+static_assert(OFDFT_RMAX_FP64 >= 8, "the allocation-free evaluation plans radix-8 stages in FP64");
+
 struct PlanTable {
-  std::map<int, FftPlan> plans;
+  std::map<int, FftPlan> plans[2];  // [0] FP64 (OFDFT_FP64), [1] FP32
   std::vector<long double> re, im;
   void* d_tw64 = nullptr;
   void* d_tw32 = nullptr;
 
   int build() {
-    for (int n = 1; n <= MAX_N; ++n) {
-      if (!seven_smooth(n)) continue;
-      FftPlan p;
-      memset(&p, 0, sizeof(p));
-      p.n = n;
-      p.tw_base = (int)re.size();
-      std::vector<int> rs = radices(n);
-      p.nst = (int)rs.size();
-      int ns = 1, off = 0;
-      for (int s = 0; s < p.nst; ++s) {
-        const int R = rs[s];
-        p.R[s] = R;
-        p.Ns[s] = ns;
-        p.tw[s] = off;
-        for (int k = 0; k < ns; ++k)
-          for (int m = 1; m < R; ++m) {
-            const long double ang = -2.0L * 3.141592653589793238462643383279502884L * (long double)(m * k) /
-                                    (long double)(ns * R);
-            re.push_back(cosl(ang));
-            im.push_back(sinl(ang));
-          }
-        p.ns_magic[s] = (unsigned)(((1u << 20) + (unsigned)ns - 1) / (unsigned)ns);
-        off += ns * (R - 1);
-        ns *= R;
+    for (int pi = 0; pi < 2; ++pi)
+      for (int n = 1; n <= MAX_N; ++n) {
+        if (!seven_smooth(n)) continue;
+        FftPlan p;
+        memset(&p, 0, sizeof(p));
+        p.n = n;
+        p.tw_base = (int)re.size();
+        std::vector<int> rs = radices(n, pi == 0 ? RMAX_FP64 : RMAX_FP32);
+        p.nst = (int)rs.size();
+        int ns = 1, off = 0;
+        for (int s = 0; s < p.nst; ++s) {
+          const int R = rs[s];
+          p.R[s] = R;
+          p.Ns[s] = ns;
+          p.tw[s] = off;
+          for (int k = 0; k < ns; ++k)
+            for (int m = 1; m < R; ++m) {
+              const long double ang = -2.0L * 3.141592653589793238462643383279502884L * (long double)(m * k) /
+                                      (long double)(ns * R);
+              re.push_back(cosl(ang));
+              im.push_back(sinl(ang));
+            }
+          p.ns_magic[s] = (unsigned)(((1u << 20) + (unsigned)ns - 1) / (unsigned)ns);
+          off += ns * (R - 1);
+          ns *= R;
+        }
+        plans[pi][n] = p;
       }
-      plans[n] = p;
-    }
     const size_t nt = re.size();
     std::vector<cx<double>> t64(nt);
     std::vector<cx<float>> t32(nt);
@@ -154,19 +189,19 @@ template <typename T> __global__ void __launch_bounds__(256) k_vec(Args<T> a) {
   extern __shared__ __align__(16) char sm[];
   vec_block<T>(a, blockIdx.x, threadIdx.x, blockDim.x, sm);
 }
-template <typename T> __global__ void __launch_bounds__(256) k_xfwd(Args<T> a) {
+template <typename T> __global__ void __launch_bounds__(256, PassMinBlocks<T>::value) k_xfwd(Args<T> a) {
   extern __shared__ __align__(16) char sm[];
   xfwd_block<T>(a, blockIdx.x, threadIdx.x, blockDim.x, sm);
 }
-template <typename T> __global__ void __launch_bounds__(256) k_ypass(Args<T> a, int dir) {
+template <typename T> __global__ void __launch_bounds__(256, PassMinBlocks<T>::value) k_ypass(Args<T> a, int dir) {
   extern __shared__ __align__(16) char sm[];
   ypass_block<T>(a, blockIdx.x, threadIdx.x, blockDim.x, sm, dir);
 }
-template <typename T> __global__ void __launch_bounds__(256) k_zpass(Args<T> a) {
+template <typename T> __global__ void __launch_bounds__(256, PassMinBlocks<T>::value) k_zpass(Args<T> a) {
   extern __shared__ __align__(16) char sm[];
   zpass_block<T>(a, blockIdx.x, threadIdx.x, blockDim.x, sm);
 }
-template <typename T> __global__ void __launch_bounds__(256, 3) k_xinv(Args<T> a) {
+template <typename T> __global__ void __launch_bounds__(256, PassMinBlocks<T>::value) k_xinv(Args<T> a) {
   extern __shared__ __align__(16) char sm[];
   xinv_block<T>(a, blockIdx.x, threadIdx.x, blockDim.x, sm);
 }
@@ -368,9 +403,10 @@ struct Engine {
     s.k1 = d->n1 / 2 + 1;
     s.N = (long long)d->n1 * d->n2 * d->n3;
     s.Nc = (long long)s.k1 * d->n2 * d->n3;
-    s.px = plans.plans[d->n1];
-    s.py = plans.plans[d->n2];
-    s.pz = plans.plans[d->n3];
+    const int pi = d->precision == OFDFT_FP32 ? 1 : 0;
+    s.px = plans.plans[pi][d->n1];
+    s.py = plans.plans[pi][d->n2];
+    s.pz = plans.plans[pi][d->n3];
     // cellRecip = TRANSPOSE(Inverse(cellReal)) * 2 pi  (CellInfo.f90:281)
     const double* L = d->lattice;  // L[3*i + k] = component k of vector i
     auto A = [&](int r, int c) { return L[3 * c + r]; };
@@ -955,14 +991,14 @@ struct Engine {
       for (int pass : {P_Y2, P_Y4}) {
         for (int f = 0; f < s.nf; ++f)
           for (int z = 0; z < s.n3; ++z)
-            for (int kx = 0; kx < s.k1; kx += s.tx) L[pass].h.push_back({i, f, z, kx});
+            for (int t = 0; t < tile_count(s.k1, s.tx); ++t) L[pass].h.push_back({i, f, z, tile_code(s.k1, s.tx, t)});
         L[pass].nthr = 256;
         L[pass].smem = std::max(L[pass].smem, 2 * (size_t)s.tx * s.n2 * cs);
       }
       const int gmax = s.kinetic == KIN_WGC ? 3 : 1;
       for (int g = 0; g < s.ngroups; ++g)
         for (int ky = 0; ky < s.n2; ++ky)
-          for (int kx = 0; kx < s.k1; kx += s.tx) L[P_Z3].h.push_back({i, g, ky, kx});
+          for (int t = 0; t < tile_count(s.k1, s.tx); ++t) L[P_Z3].h.push_back({i, g, ky, tile_code(s.k1, s.tx, t)});
       L[P_Z3].nthr = 256;
       L[P_Z3].smem = std::max(L[P_Z3].smem, 2 * (size_t)std::max(gmax, s.ion.nspec) * s.tx * s.n3 * cs);
       int ord = 0;
@@ -1619,10 +1655,10 @@ extern "C" int ofdft_calculate_potential_plus_noalloc(const ofdft_cell_desc* d, 
     for (int r = 0; r < nrp && ok; r += rp1) ok = push(0, {0, f, r, std::min(rp1, nrp - r)});
   for (int f = 0; f < s.nf && ok; ++f)
     for (int z = 0; z < s.n3 && ok; ++z)
-      for (int kx = 0; kx < s.k1 && ok; kx += s.tx) ok = push(1, {0, f, z, kx});
+      for (int t = 0; t < tile_count(s.k1, s.tx) && ok; ++t) ok = push(1, {0, f, z, tile_code(s.k1, s.tx, t)});
   for (int g = 0; g < s.ngroups && ok; ++g)
     for (int ky = 0; ky < s.n2 && ok; ++ky)
-      for (int kx = 0; kx < s.k1 && ok; kx += s.tx) ok = push(2, {0, g, ky, kx});
+      for (int t = 0; t < tile_count(s.k1, s.tx) && ok; ++t) ok = push(2, {0, g, ky, tile_code(s.k1, s.tx, t)});
   int ord = 0;
   for (int r = 0; r < nrp && ok; r += s.rp) ok = push(3, {0, r, std::min(s.rp, nrp - r), ord++});
   if (ok) ok = push(4, {0, 0, 0, 0});

@@ -1,27 +1,44 @@
 // Batched mixed-radix Stockham FFT over shared memory.
 //
-// A transform of length n = R_0 * R_1 * ... (radices 2, 3, 4, 5, 7, 8) runs as
-// one Stockham stage per radix.  Each stage reads R points at stride n/R,
-// multiplies by the stage twiddles, does a radix-R butterfly in registers and
+// A transform of length n = R_0 * R_1 * ... runs as one Stockham stage per
+// radix.  The radices are 2, 3, 4, 5, 7, 8 and the compound radices 6, 9, 10,
+// 12, 14, 15, 16, whose R-point DFTs run in registers as an A x B
+// Cooley-Tukey split of the small DFTs with compile-time twiddles, so most
+// lengths up to 256 take two stages.  Each stage reads R points at stride n/R,
+// multiplies by the stage twiddles, does the R-point DFT in registers and
 // writes the R outputs in self-sorting order, ping-ponging between two shared
 // buffers; the caller reads the result from whichever buffer fft_batch
 // returns.  Many independent transforms of the same length are done together:
 // element i of transform b lives at buf[b + i*si].  Work items (b, butterfly)
 // are spread over the block's threads with b fastest, so consecutive threads
 // touch consecutive shared-memory words; the index arithmetic uses
-// multiply-high divisions by constants prepared on the host.
+// multiply-high divisions by constants prepared on the host.  The direction
+// (DIR = -1 forward, +1 inverse) is a template parameter.
 //
 // Twiddles are precomputed on the host in long double and stored per plan:
 // stage s with span Ns (product of the earlier radices) and radix R uses
 // tw[off_s + k*(R-1) + (m-1)] = exp(-2*pi*i*m*k/(Ns*R)), k = 0..Ns-1.
 // The inverse transform uses the conjugates.  No scaling is applied here.
 #pragma once
+#include <type_traits>
 #include "cx.cuh"
 
 namespace ofdft {
 
 constexpr int FFT_MAX_STAGES = 12;
-constexpr int FFT_MAX_RADIX = 8;
+constexpr int FFT_MAX_RADIX = 16;
+
+// Largest radix of the FP32 and FP64 plans.  An R-point DFT holds R complex
+// values in registers; only the radices up to the limit are compiled into a
+// precision's kernels, so the limit also bounds their register use.
+#ifndef OFDFT_RMAX_FP32
+#define OFDFT_RMAX_FP32 8
+#endif
+#ifndef OFDFT_RMAX_FP64
+#define OFDFT_RMAX_FP64 8
+#endif
+template <typename T> struct FftMaxRadix { static constexpr int value = OFDFT_RMAX_FP32; };
+template <> struct FftMaxRadix<double> { static constexpr int value = OFDFT_RMAX_FP64; };
 
 struct FftPlan {
   int n;
@@ -39,12 +56,12 @@ HD int magic_div(int j, unsigned magic) { return (int)(((unsigned)j * magic) >> 
 // Exact quotient w / d for 0 <= w < 2^24 and 1 <= d <= 4096 from m32 = ceil(2^32 / d)
 // (d = 1 is encoded as m32 = 0).
 HD int magic_div32(int w, unsigned m32) {
-  if (m32 == 0u) return w;
 #if defined(__CUDA_ARCH__)
-  return (int)__umulhi((unsigned)w, m32);
+  const int q = (int)__umulhi((unsigned)w, m32);
 #else
-  return (int)(((unsigned long long)(unsigned)w * m32) >> 32);
+  const int q = (int)(((unsigned long long)(unsigned)w * m32) >> 32);
 #endif
+  return m32 == 0u ? w : q;
 }
 HD unsigned magic32(int d) {
   return d <= 1 ? 0u : (unsigned)((0x100000000ULL + (unsigned long long)d - 1) / (unsigned long long)d);
@@ -112,14 +129,17 @@ HD void dft7(cx<T>* v, int dir) {
   const T c[4] = {T(1), T(OFDFT_C71), T(OFDFT_C72), T(OFDFT_C73)};
   const T s[4] = {T(0), T(OFDFT_S71), T(OFDFT_S72), T(OFDFT_S73)};
   cx<T> tp[4], tm[4];
+#pragma unroll
   for (int k = 1; k <= 3; ++k) {
     tp[k] = v[k] + v[7 - k];
     tm[k] = v[k] - v[7 - k];
   }
   cx<T> y[7];
   y[0] = v[0] + tp[1] + tp[2] + tp[3];
+#pragma unroll
   for (int j = 1; j <= 3; ++j) {
     cx<T> a = v[0], b = mk<T>(T(0), T(0));
+#pragma unroll
     for (int k = 1; k <= 3; ++k) {
       int m = (j * k) % 7;
       T cc = m <= 3 ? c[m] : c[7 - m];
@@ -131,6 +151,7 @@ HD void dft7(cx<T>* v, int dir) {
     y[j] = a + ib;
     y[7 - j] = a - ib;
   }
+#pragma unroll
   for (int k = 0; k < 7; ++k) v[k] = y[k];
 }
 
@@ -152,19 +173,133 @@ HD void dft8(cx<T>* v, int dir) {
   v[3] = e[3] + t3; v[7] = e[3] - t3;
 }
 
-template <typename T, int R> struct Dft;
-template <typename T> struct Dft<T, 2> { static HD void run(cx<T>* v, int) { dft2(v); } };
-template <typename T> struct Dft<T, 3> { static HD void run(cx<T>* v, int d) { dft3(v, d); } };
-template <typename T> struct Dft<T, 4> { static HD void run(cx<T>* v, int d) { dft4(v, d); } };
-template <typename T> struct Dft<T, 5> { static HD void run(cx<T>* v, int d) { dft5(v, d); } };
-template <typename T> struct Dft<T, 7> { static HD void run(cx<T>* v, int d) { dft7(v, d); } };
-template <typename T> struct Dft<T, 8> { static HD void run(cx<T>* v, int d) { dft8(v, d); } };
+// cos(2 pi e / R) (want_sin = 0) or sin(2 pi e / R) for the compound radices
+// (mathematical constants), evaluated at compile time.
+HDC double root_cs(int R, int e, int want_sin) {
+  switch (R) {
+    case 6: {
+      const double c[6] = {1.0, 0.5, -0.5, -1.0, -0.5, 0.5};
+      const double s[6] = {0.0, 0.8660254037844386467637232, 0.8660254037844386467637232, 0.0, -0.8660254037844386467637232, -0.8660254037844386467637232};
+      return want_sin ? s[e] : c[e];
+    }
+    case 9: {
+      const double c[9] = {1.0, 0.7660444431189780352023927, 0.1736481776669303488517166, -0.5, -0.9396926207859083840541093, -0.9396926207859083840541093, -0.5, 0.1736481776669303488517166, 0.7660444431189780352023927};
+      const double s[9] = {0.0, 0.6427876096865393263226434, 0.984807753012208059366743, 0.8660254037844386467637232, 0.3420201433256687330440996, -0.3420201433256687330440996, -0.8660254037844386467637232, -0.984807753012208059366743, -0.6427876096865393263226434};
+      return want_sin ? s[e] : c[e];
+    }
+    case 10: {
+      const double c[10] = {1.0, 0.8090169943749474241022934, 0.3090169943749474241022934, -0.3090169943749474241022934, -0.8090169943749474241022934, -1.0, -0.8090169943749474241022934, -0.3090169943749474241022934, 0.3090169943749474241022934, 0.8090169943749474241022934};
+      const double s[10] = {0.0, 0.587785252292473129168706, 0.9510565162951535721164393, 0.9510565162951535721164393, 0.587785252292473129168706, 0.0, -0.587785252292473129168706, -0.9510565162951535721164393, -0.9510565162951535721164393, -0.587785252292473129168706};
+      return want_sin ? s[e] : c[e];
+    }
+    case 12: {
+      const double c[12] = {1.0, 0.8660254037844386467637232, 0.5, 0.0, -0.5, -0.8660254037844386467637232, -1.0, -0.8660254037844386467637232, -0.5, 0.0, 0.5, 0.8660254037844386467637232};
+      const double s[12] = {0.0, 0.5, 0.8660254037844386467637232, 1.0, 0.8660254037844386467637232, 0.5, 0.0, -0.5, -0.8660254037844386467637232, -1.0, -0.8660254037844386467637232, -0.5};
+      return want_sin ? s[e] : c[e];
+    }
+    case 14: {
+      const double c[14] = {1.0, 0.9009688679024191262361023, 0.6234898018587335305250049, 0.2225209339563144042889026, -0.2225209339563144042889026, -0.6234898018587335305250049, -0.9009688679024191262361023, -1.0, -0.9009688679024191262361023, -0.6234898018587335305250049, -0.2225209339563144042889026, 0.2225209339563144042889026, 0.6234898018587335305250049, 0.9009688679024191262361023};
+      const double s[14] = {0.0, 0.4338837391175581204757683, 0.7818314824680298087084445, 0.9749279121818236070181317, 0.9749279121818236070181317, 0.7818314824680298087084445, 0.4338837391175581204757683, 0.0, -0.4338837391175581204757683, -0.7818314824680298087084445, -0.9749279121818236070181317, -0.9749279121818236070181317, -0.7818314824680298087084445, -0.4338837391175581204757683};
+      return want_sin ? s[e] : c[e];
+    }
+    case 15: {
+      const double c[15] = {1.0, 0.9135454576426008955021276, 0.6691306063588582138262733, 0.3090169943749474241022934, -0.1045284632676534713998342, -0.5, -0.8090169943749474241022934, -0.9781476007338056379285667, -0.9781476007338056379285667, -0.8090169943749474241022934, -0.5, -0.1045284632676534713998342, 0.3090169943749474241022934, 0.6691306063588582138262733, 0.9135454576426008955021276};
+      const double s[15] = {0.0, 0.406736643075800207753986, 0.743144825477394235014697, 0.9510565162951535721164393, 0.9945218953682733369226919, 0.8660254037844386467637232, 0.587785252292473129168706, 0.2079116908177593371017423, -0.2079116908177593371017423, -0.587785252292473129168706, -0.8660254037844386467637232, -0.9945218953682733369226919, -0.9510565162951535721164393, -0.743144825477394235014697, -0.406736643075800207753986};
+      return want_sin ? s[e] : c[e];
+    }
+    case 16: {
+      const double c[16] = {1.0, 0.9238795325112867561281832, 0.7071067811865475244008444, 0.38268343236508977172846, 0.0, -0.38268343236508977172846, -0.7071067811865475244008444, -0.9238795325112867561281832, -1.0, -0.9238795325112867561281832, -0.7071067811865475244008444, -0.38268343236508977172846, 0.0, 0.38268343236508977172846, 0.7071067811865475244008444, 0.9238795325112867561281832};
+      const double s[16] = {0.0, 0.38268343236508977172846, 0.7071067811865475244008444, 0.9238795325112867561281832, 1.0, 0.9238795325112867561281832, 0.7071067811865475244008444, 0.38268343236508977172846, 0.0, -0.38268343236508977172846, -0.7071067811865475244008444, -0.9238795325112867561281832, -1.0, -0.9238795325112867561281832, -0.7071067811865475244008444, -0.38268343236508977172846};
+      return want_sin ? s[e] : c[e];
+    }
+    default:
+      return 0.0;
+  }
+}
+
+// Compile-time loop: f(std::integral_constant<int, I>()) for I = B .. E-1.
+template <int B, int E>
+struct StaticFor {
+  template <typename F>
+  static HD void run(F&& f) {
+    if constexpr (B < E) {
+      f(std::integral_constant<int, B>());
+      StaticFor<B + 1, E>::run(f);
+    }
+  }
+};
+
+// x * exp(DIR * 2 pi i E / R), with the trivial angles special-cased.
+template <typename T, int R, int E, int DIR>
+HD cx<T> twiddle_const(cx<T> x) {
+  constexpr int e = E % R;
+  if constexpr (e == 0) {
+    return x;
+  } else if constexpr (2 * e == R) {
+    return mk<T>(-x.x, -x.y);
+  } else if constexpr (4 * e == R) {
+    return mul_i(x, DIR);
+  } else if constexpr (4 * e == 3 * R) {
+    return mul_i(x, -DIR);
+  } else {
+    constexpr double c = root_cs(R, e, 0);
+    constexpr double s = root_cs(R, e, 1);
+    return cmul(x, mk<T>(T(c), T(DIR * s)));
+  }
+}
+
+template <typename T, int R, int DIR> struct Dft;
+template <typename T, int A, int B, int DIR> HD void dft_ab(cx<T>* v);
+
+template <typename T, int DIR> struct Dft<T, 2, DIR> { static HD void run(cx<T>* v) { dft2(v); } };
+template <typename T, int DIR> struct Dft<T, 3, DIR> { static HD void run(cx<T>* v) { dft3(v, DIR); } };
+template <typename T, int DIR> struct Dft<T, 4, DIR> { static HD void run(cx<T>* v) { dft4(v, DIR); } };
+template <typename T, int DIR> struct Dft<T, 5, DIR> { static HD void run(cx<T>* v) { dft5(v, DIR); } };
+template <typename T, int DIR> struct Dft<T, 7, DIR> { static HD void run(cx<T>* v) { dft7(v, DIR); } };
+template <typename T, int DIR> struct Dft<T, 8, DIR> { static HD void run(cx<T>* v) { dft8(v, DIR); } };
+template <typename T, int DIR> struct Dft<T, 6, DIR> { static HD void run(cx<T>* v) { dft_ab<T, 3, 2, DIR>(v); } };
+template <typename T, int DIR> struct Dft<T, 9, DIR> { static HD void run(cx<T>* v) { dft_ab<T, 3, 3, DIR>(v); } };
+template <typename T, int DIR> struct Dft<T, 10, DIR> { static HD void run(cx<T>* v) { dft_ab<T, 5, 2, DIR>(v); } };
+template <typename T, int DIR> struct Dft<T, 12, DIR> { static HD void run(cx<T>* v) { dft_ab<T, 4, 3, DIR>(v); } };
+template <typename T, int DIR> struct Dft<T, 14, DIR> { static HD void run(cx<T>* v) { dft_ab<T, 7, 2, DIR>(v); } };
+template <typename T, int DIR> struct Dft<T, 15, DIR> { static HD void run(cx<T>* v) { dft_ab<T, 5, 3, DIR>(v); } };
+template <typename T, int DIR> struct Dft<T, 16, DIR> { static HD void run(cx<T>* v) { dft_ab<T, 4, 4, DIR>(v); } };
+
+// R = A*B point DFT in registers (natural order in and out): with
+// j = B*j1 + j2 and k = k1 + A*k2,
+//   X[k1 + A k2] = sum_j2 W_B^{j2 k2} W_R^{j2 k1} sum_j1 W_A^{j1 k1} x[B j1 + j2],
+// W_M = exp(DIR * 2 pi i / M).
+template <typename T, int A, int B, int DIR>
+HD void dft_ab(cx<T>* v) {
+  constexpr int R = A * B;
+  cx<T> y[R];
+  StaticFor<0, B>::run([&](auto j2c) {
+    constexpr int j2 = decltype(j2c)::value;
+    cx<T> u[A];
+#pragma unroll
+    for (int j1 = 0; j1 < A; ++j1) u[j1] = v[B * j1 + j2];
+    Dft<T, A, DIR>::run(u);
+    StaticFor<0, A>::run([&](auto k1c) {
+      constexpr int k1 = decltype(k1c)::value;
+      y[k1 * B + j2] = twiddle_const<T, R, j2 * k1, DIR>(u[k1]);
+    });
+  });
+#pragma unroll
+  for (int k1 = 0; k1 < A; ++k1) {
+    cx<T> u[B];
+#pragma unroll
+    for (int j2 = 0; j2 < B; ++j2) u[j2] = y[k1 * B + j2];
+    Dft<T, B, DIR>::run(u);
+#pragma unroll
+    for (int k2 = 0; k2 < B; ++k2) v[k1 + A * k2] = u[k2];
+  }
+}
 
 // One Stockham stage of radix R over nb transforms: src -> dst.  Element i of
 // transform b is at [b + i*si] (si >= nb); mnb = magic32(nb).
-template <typename T, int R>
+template <typename T, int R, int DIR>
 HD void fft_stage_r(const cx<T>* __restrict__ src, cx<T>* __restrict__ dst, int nb, unsigned mnb, int si, int n,
-                    int Ns, unsigned magic, const cx<T>* __restrict__ tw, int dir, int tid, int nthr) {
+                    int Ns, unsigned magic, const cx<T>* __restrict__ tw, int tid, int nthr) {
   const int nbf = n / R;  // butterflies per transform
   const int total = nbf * nb;
   for (int w = tid; w < total; w += nthr) {
@@ -181,11 +316,11 @@ HD void fft_stage_r(const cx<T>* __restrict__ src, cx<T>* __restrict__ dst, int 
 #pragma unroll
       for (int m = 1; m < R; ++m) {
         cx<T> f = t[m - 1];
-        if (dir > 0) f.y = -f.y;
+        if (DIR > 0) f.y = -f.y;
         v[m] = cmul(v[m], f);
       }
     }
-    Dft<T, R>::run(v, dir);
+    Dft<T, R, DIR>::run(v);
     cx<T>* d = dst + b;
     const int base = jq * Ns * R + kmod;
 #pragma unroll
@@ -193,39 +328,60 @@ HD void fft_stage_r(const cx<T>* __restrict__ src, cx<T>* __restrict__ dst, int 
   }
 }
 
-template <typename T>
+template <typename T, int DIR>
 HD void fft_stage(const cx<T>* src, cx<T>* dst, int nb, unsigned mnb, int si, int n, int R, int Ns, unsigned magic,
-                  const cx<T>* tw, int dir, int tid, int nthr) {
+                  const cx<T>* tw, int tid, int nthr) {
+  constexpr int RM = FftMaxRadix<T>::value;
+#define OFDFT_STAGE_CASE(r)                                                                 \
+  case r:                                                                                   \
+    if constexpr (r <= RM) fft_stage_r<T, r, DIR>(src, dst, nb, mnb, si, n, Ns, magic, tw, tid, nthr); \
+    break;
   switch (R) {
-    case 2: fft_stage_r<T, 2>(src, dst, nb, mnb, si, n, Ns, magic, tw, dir, tid, nthr); break;
-    case 3: fft_stage_r<T, 3>(src, dst, nb, mnb, si, n, Ns, magic, tw, dir, tid, nthr); break;
-    case 4: fft_stage_r<T, 4>(src, dst, nb, mnb, si, n, Ns, magic, tw, dir, tid, nthr); break;
-    case 5: fft_stage_r<T, 5>(src, dst, nb, mnb, si, n, Ns, magic, tw, dir, tid, nthr); break;
-    case 7: fft_stage_r<T, 7>(src, dst, nb, mnb, si, n, Ns, magic, tw, dir, tid, nthr); break;
-    case 8: fft_stage_r<T, 8>(src, dst, nb, mnb, si, n, Ns, magic, tw, dir, tid, nthr); break;
+    OFDFT_STAGE_CASE(2)
+    OFDFT_STAGE_CASE(3)
+    OFDFT_STAGE_CASE(4)
+    OFDFT_STAGE_CASE(5)
+    OFDFT_STAGE_CASE(6)
+    OFDFT_STAGE_CASE(7)
+    OFDFT_STAGE_CASE(8)
+    OFDFT_STAGE_CASE(9)
+    OFDFT_STAGE_CASE(10)
+    OFDFT_STAGE_CASE(12)
+    OFDFT_STAGE_CASE(14)
+    OFDFT_STAGE_CASE(15)
+    OFDFT_STAGE_CASE(16)
     default: break;
   }
+#undef OFDFT_STAGE_CASE
 }
 
 // Full transform of nb sequences held in buf (tmp is scratch of the same
-// layout), element i of sequence b at [b + i*si].  dir = -1 forward, +1
+// layout), element i of sequence b at [b + i*si].  DIR = -1 forward, +1
 // inverse.  Returns the buffer (buf or tmp) holding the result.  Must be
 // called by every thread of the block.
-template <typename T>
-HD cx<T>* fft_batch(cx<T>* buf, cx<T>* tmp, int nb, int si, const FftPlan& p,
-                    const cx<T>* twtab, int dir, int tid, int nthr) {
+template <typename T, int DIR>
+HD cx<T>* fft_batch(cx<T>* buf, cx<T>* tmp, int nb, int si, const FftPlan& p, const cx<T>* twtab, int tid,
+                    int nthr) {
   cx<T>* a = buf;
   cx<T>* b = tmp;
   const unsigned mnb = magic32(nb);
-  for (int s = 0; s < p.nst; ++s) {
-    fft_stage(a, b, nb, mnb, si, p.n, p.R[s], p.Ns[s], p.ns_magic[s], twtab + p.tw_base + p.tw[s], dir, tid,
-              nthr);
+  const int nst = p.nst, n = p.n;
+  for (int s = 0; s < nst; ++s) {
+    fft_stage<T, DIR>(a, b, nb, mnb, si, n, p.R[s], p.Ns[s], p.ns_magic[s], twtab + p.tw_base + p.tw[s], tid, nthr);
     BLOCK_SYNC();
     cx<T>* t = a;
     a = b;
     b = t;
   }
   return a;
+}
+
+// Runtime direction: dir = -1 forward, +1 inverse.
+template <typename T>
+HD cx<T>* fft_batch(cx<T>* buf, cx<T>* tmp, int nb, int si, const FftPlan& p, const cx<T>* twtab, int dir,
+                    int tid, int nthr) {
+  return dir < 0 ? fft_batch<T, -1>(buf, tmp, nb, si, p, twtab, tid, nthr)
+                 : fft_batch<T, 1>(buf, tmp, nb, si, p, twtab, tid, nthr);
 }
 
 }  // namespace ofdft

@@ -337,7 +337,7 @@ HDNI void xfwd_block(const Args<T>& a, int bid, int tid, int nthr, char* smem) {
     buf[b + i * nb] = mk<T>(v0, v1);
   }
   BLOCK_SYNC();
-  const cx<T>* res = fft_batch(buf, tmp, nb, nb, px, a.tw, -1, tid, nthr);
+  const cx<T>* res = fft_batch<T, -1>(buf, tmp, nb, nb, px, a.tw, tid, nthr);
   const unsigned mk1 = magic32(k1);
   for (int w = tid; w < nb * k1; w += nthr) {
     const int b = magic_div32(w, mk1), k = w - b * k1;
@@ -357,11 +357,10 @@ HDNI void ypass_block(const Args<T>& a, int bid, int tid, int nthr, char* smem, 
   const SlotDev& s = a.slots[t.slot];
   const Ctl& c = a.ctl[t.slot];
   if (c.status != ST_RUNNING || c.ev == EV_NONE) return;
-  const int f = t.a, z = t.b, kx0 = t.c;
+  const int f = t.a, z = t.b, kx0 = tile_kx0(t.c), nb = tile_width(t.c);
   if (c.ev == EV_ION && f >= (dir < 0 ? s.ion.nspec : 1)) return;
   if (c.ev == EV_FORCE && f >= (dir < 0 ? 1 : s.ion.nspec)) return;
-  const int n2 = s.n2, k1 = s.k1, TX = s.tx;
-  const int nb = (k1 - kx0) < TX ? (k1 - kx0) : TX;
+  const int n2 = s.n2, k1 = s.k1;
   cx<T>* buf = (cx<T>*)smem;
   cx<T>* tmp = buf + nb * n2;
   cx<T>* __restrict__ sp = (cx<T>*)s.spec + (size_t)f * (size_t)s.Nc + (size_t)z * n2 * k1 + kx0;
@@ -387,12 +386,11 @@ HDNI void zpass_block(const Args<T>& a, int bid, int tid, int nthr, char* smem) 
   const SlotDev& s = a.slots[t.slot];
   const Ctl& c = a.ctl[t.slot];
   if (c.status != ST_RUNNING || c.ev == EV_NONE) return;
-  const int g = t.a, ky = t.b, kx0 = t.c;
+  const int g = t.a, ky = t.b, kx0 = tile_kx0(t.c), nb = tile_width(t.c);
   const int ev = c.ev;
   const bool setup_mode = ev == EV_ION || ev == EV_FORCE;
   if (setup_mode && g != 0) return;
-  const int n2 = s.n2, n3 = s.n3, k1 = s.k1, TX = s.tx;
-  const int nb = (k1 - kx0) < TX ? (k1 - kx0) : TX;
+  const int n2 = s.n2, n3 = s.n3, k1 = s.k1;
   const int kind = ev == EV_ION ? G_ION : ev == EV_FORCE ? G_FORCE : s.group_kind[g];
   const int gn = setup_mode ? s.ion.nspec : s.group_nf[g];
   const int gin = ev == EV_FORCE ? 1 : gn;  // fields loaded
@@ -411,35 +409,41 @@ HDNI void zpass_block(const Args<T>& a, int bid, int tid, int nthr, char* smem) 
     buf[w] = q < gin ? spec[(size_t)q * Nc + i * plane + b] : mk<T>(T(0), T(0));
   }
   BLOCK_SYNC();
-  cx<T>* res = fft_batch(buf, tmp, NB, NB, s.pz, a.tw, -1, tid, nthr);
+  cx<T>* res = fft_batch<T, -1>(buf, tmp, NB, NB, s.pz, a.tw, tid, nthr);
   cx<T>* oth = res == buf ? tmp : buf;
   const int m2 = ky > n2 / 2 ? ky - n2 : ky;
   const T* __restrict__ kern = (const T*)s.kern + ky * k1 + kx0;
   const T sc = (T)s.inv_n;
-  double rc[9];
+  // |G|^2 of the Hartree and vW operators in the slot's precision; the
+  // set-up modes (ion potential, forces) evaluate |G| in FP64.
+  T rt[9];
 #pragma unroll
-  for (int q = 0; q < 9; ++q) rc[q] = s.recip[q];
-  const double gy0 = rc[3] * m2, gy1 = rc[4] * m2, gy2 = rc[5] * m2;
+  for (int q = 0; q < 9; ++q) rt[q] = (T)s.recip[q];
+  const T ty0 = rt[3] * (T)m2, ty1 = rt[4] * (T)m2, ty2 = rt[5] * (T)m2;
+  const T c4 = (T)(4.0 * PI_D * s.inv_n);
   for (int w = tid; w < nb * n3; w += nthr) {
     const int i = magic_div32(w, mnb), b = w - i * nb;
     const int m1 = kx0 + b;
     const int m3 = i > n3 / 2 ? i - n3 : i;
-    const double gx = rc[0] * m1 + gy0 + rc[6] * m3;
-    const double gy = rc[1] * m1 + gy1 + rc[7] * m3;
-    const double gz = rc[2] * m1 + gy2 + rc[8] * m3;
-    const double q = sqrt(gx * gx + gy * gy + gz * gz);
-    const double q2 = q * q;
     const int kidx = i * plane + b;
     cx<T>* e = res + i * NB + b;
+    if (kind == G_HARTREE || kind == G_VW) {
+      const T tx = rt[0] * (T)m1 + ty0 + rt[6] * (T)m3;
+      const T ty = rt[1] * (T)m1 + ty1 + rt[7] * (T)m3;
+      const T tz = rt[2] * (T)m1 + ty2 + rt[8] * (T)m3;
+      const T g2 = tx * tx + ty * ty + tz * tz;
+      const T m = kind == G_VW ? g2 * sc : ((m1 == 0 && ky == 0 && i == 0) ? T(0) : c4 / g2);
+      e[0] = e[0] * m;
+      continue;
+    }
+    double q = 0.0;
+    if (setup_mode) {
+      const double gx = s.recip[0] * m1 + s.recip[3] * m2 + s.recip[6] * m3;
+      const double gy = s.recip[1] * m1 + s.recip[4] * m2 + s.recip[7] * m3;
+      const double gz = s.recip[2] * m1 + s.recip[5] * m2 + s.recip[8] * m3;
+      q = sqrt(gx * gx + gy * gy + gz * gz);
+    }
     switch (kind) {
-      case G_HARTREE: {
-        const T m = (m1 == 0 && ky == 0 && i == 0) ? T(0) : (T)(4.0 * PI_D / q2) * sc;
-        e[0] = e[0] * m;
-        break;
-      }
-      case G_VW:
-        e[0] = e[0] * ((T)q2 * sc);
-        break;
       case G_KMUL:
         e[0] = e[0] * (kern[kidx] * sc);
         break;
@@ -480,7 +484,7 @@ HDNI void zpass_block(const Args<T>& a, int bid, int tid, int nthr, char* smem) 
     }
   }
   BLOCK_SYNC();
-  const cx<T>* out = fft_batch(res, oth, NB, NB, s.pz, a.tw, 1, tid, nthr);
+  const cx<T>* out = fft_batch<T, 1>(res, oth, NB, NB, s.pz, a.tw, tid, nthr);
   for (int w = tid; w < NB * n3; w += nthr) {
     const int i = magic_div32(w, mNB), qb = w - i * NB;
     const int q = magic_div32(qb, mnb), b = qb - q * nb;
@@ -553,7 +557,7 @@ HDNI void xinv_block(const Args<T>& a, int bid, int tid, int nthr, char* smem) {
     buf[k * NB + fb] = mk<T>(A.x - B.y, A.y + B.x);
   }
   BLOCK_SYNC();
-  const cx<T>* res = fft_batch(buf, tmp, NB, NB, s.px, a.tw, 1, tid, nthr);
+  const cx<T>* res = fft_batch<T, 1>(buf, tmp, NB, NB, s.px, a.tw, tid, nthr);
   if (setup_mode) {
     // EV_ION: ionPotReal; EV_FORCE: the per-species Factor arrays in buf[B_B + s]
     const unsigned m2n1s = magic32(2 * n1);

@@ -142,4 +142,16 @@ struct Task {
   int slot, a, b, c;
 };
 
+// kx tiles of the y and z passes: ceil(k1 / tx) tiles of nearly equal width
+// (a 49-wide half spectrum becomes 13 + 12 + 12 + 12, not 16 + 16 + 16 + 1).
+// A task's c field holds kx0 | (width << 16).
+HD int tile_count(int k1, int tx) { return (k1 + tx - 1) / tx; }
+HD int tile_code(int k1, int tx, int t) {
+  const int nt = tile_count(k1, tx), base = k1 / nt, rem = k1 % nt;
+  const int kx0 = t * base + (t < rem ? t : rem);
+  return kx0 | ((base + (t < rem ? 1 : 0)) << 16);
+}
+HD int tile_kx0(int c) { return c & 0xffff; }
+HD int tile_width(int c) { return c >> 16; }
+
 }  // namespace ofdft

@@ -106,15 +106,16 @@ constexpr int MAX_N = 512;
 
 // Largest radix of the FP32 and FP64 plans (OFDFT_RMAX_* in fft.cuh) and the
 // minimum resident 256-thread blocks per SM of the FFT pass kernels, per
-// precision (it caps their registers at 65536 / (256 * minb)).  The passes are
-// bound by shared-memory and global-memory latency rather than by arithmetic:
-// on 16 cells of 96^3, radix <= 8 with 4 blocks per SM (64 registers) was
-// faster than radix <= 16 with 2 blocks per SM, in both precisions.
+// precision (it caps their registers at 65536 / (256 * minb)).  The passes
+// are latency- and issue-bound: on 16 cells of 96^3, Stockham radices <= 8
+// with 4 blocks per SM (64 registers) beat radix <= 16 with 2 blocks per SM;
+// FP64 runs best with 3 blocks per SM (85 registers, no spills in the
+// two-step transforms).
 #ifndef OFDFT_MINB_FP32
 #define OFDFT_MINB_FP32 4
 #endif
 #ifndef OFDFT_MINB_FP64
-#define OFDFT_MINB_FP64 4
+#define OFDFT_MINB_FP64 3
 #endif
 constexpr int RMAX_FP32 = OFDFT_RMAX_FP32;
 constexpr int RMAX_FP64 = OFDFT_RMAX_FP64;
@@ -155,8 +156,21 @@ struct PlanTable {
           off += ns * (R - 1);
           ns *= R;
         }
+        p.root = -1;
         plans[pi][n] = p;
       }
+    // exp(-2 pi i e / n), e = 0..n-1, for the two-step transforms
+    for (int n = 1; n <= MAX_N; ++n) {
+      if (!seven_smooth(n)) continue;
+      const int off = (int)re.size();
+      for (int e = 0; e < n; ++e) {
+        const long double ang = -2.0L * 3.141592653589793238462643383279502884L * (long double)e / (long double)n;
+        re.push_back(cosl(ang));
+        im.push_back(sinl(ang));
+      }
+      plans[0][n].root = off;
+      plans[1][n].root = off;
+    }
     const size_t nt = re.size();
     std::vector<cx<double>> t64(nt);
     std::vector<cx<float>> t32(nt);
@@ -257,6 +271,7 @@ struct HostSlot {
   SlotDev sd;
   std::vector<void*> allocs;
   int nrowpairs = 0, rp1 = 1;
+  int ty = 1, tz = 1;           // kx tile widths of the y and z passes
   int nplanes = 0;
   int nion = 0;                 // ions of the last ion-potential build
   IonStencil* d_stencil = nullptr;
@@ -280,6 +295,7 @@ struct Engine {
   bool dirty = true;
   std::vector<char> emu_smem;
   long long n_launches = 0, n_ticks = 0;
+  int num_sms = 1;
   long long launches_per_tick() const {
     long long n = 0;
     for (int p = 0; p < 2; ++p)
@@ -330,6 +346,9 @@ struct Engine {
 #if !defined(OFDFT_EMU)
     int rs = cuda_check(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking), "stream create");
     if (rs) return rs;
+    int dev = 0;
+    if ((rs = cuda_check(cudaGetDevice(&dev), "get device"))) return rs;
+    if ((rs = cuda_check(cudaDeviceGetAttribute(&num_sms, cudaDevAttrMultiProcessorCount, dev), "SM count"))) return rs;
 #endif
     int rc = dmalloc((void**)&d_slots, sizeof(SlotDev) * cap);
     if (rc) return rc;
@@ -469,9 +488,19 @@ struct Engine {
     while (h.rp1 > 1 && 2 * (size_t)h.rp1 * s.n1 * csz > 100 * 1024) h.rp1--;
     s.rp = std::max(1, std::min(32, 1024 / s.n1));
     while (s.rp > 1 && 2 * (size_t)s.nf * s.rp * s.n1 * csz > 72 * 1024) s.rp--;
+    // y/z tiles: as many kx columns as fit the two shared buffers of a block
+    // (one field of n2 values per column in the y pass, a group of gmax
+    // fields of n3 values in the z pass) in about 56 KB, four blocks per SM;
+    // at least 4 columns (rows of 32 or 64 bytes) up to 112 KB per block.
     const int gmax = s.kinetic == KIN_WGC ? 3 : 1;
-    s.tx = 16;
-    while (s.tx > 2 && 2 * (size_t)gmax * s.tx * std::max(s.n2, s.n3) * csz > 100 * 1024) s.tx /= 2;
+    auto width = [&](size_t per_col) {
+      size_t w = std::min<size_t>((size_t)s.k1, (56 * 1024) / per_col);
+      if (w < 4) w = std::min<size_t>((size_t)s.k1, std::max<size_t>(1, std::min<size_t>(4, (112 * 1024) / per_col)));
+      return (int)std::max<size_t>(1, w);
+    };
+    h.ty = width(2 * (size_t)s.n2 * csz);
+    h.tz = width(2 * (size_t)gmax * s.n3 * csz);
+    s.tx = h.ty;
     s.ntask[K_VEC] = (int)((s.N + VCHUNK - 1) / VCHUNK);
     s.ntask[K_X5] = (h.nrowpairs + s.rp - 1) / s.rp;
     // buffers
@@ -991,16 +1020,16 @@ struct Engine {
       for (int pass : {P_Y2, P_Y4}) {
         for (int f = 0; f < s.nf; ++f)
           for (int z = 0; z < s.n3; ++z)
-            for (int t = 0; t < tile_count(s.k1, s.tx); ++t) L[pass].h.push_back({i, f, z, tile_code(s.k1, s.tx, t)});
+            for (int t = 0; t < tile_count(s.k1, h.ty); ++t) L[pass].h.push_back({i, f, z, tile_code(s.k1, h.ty, t)});
         L[pass].nthr = 256;
-        L[pass].smem = std::max(L[pass].smem, 2 * (size_t)s.tx * s.n2 * cs);
+        L[pass].smem = std::max(L[pass].smem, 2 * (size_t)h.ty * s.n2 * cs);
       }
       const int gmax = s.kinetic == KIN_WGC ? 3 : 1;
       for (int g = 0; g < s.ngroups; ++g)
         for (int ky = 0; ky < s.n2; ++ky)
-          for (int t = 0; t < tile_count(s.k1, s.tx); ++t) L[P_Z3].h.push_back({i, g, ky, tile_code(s.k1, s.tx, t)});
+          for (int t = 0; t < tile_count(s.k1, h.tz); ++t) L[P_Z3].h.push_back({i, g, ky, tile_code(s.k1, h.tz, t)});
       L[P_Z3].nthr = 256;
-      L[P_Z3].smem = std::max(L[P_Z3].smem, 2 * (size_t)std::max(gmax, s.ion.nspec) * s.tx * s.n3 * cs);
+      L[P_Z3].smem = std::max(L[P_Z3].smem, 2 * (size_t)std::max(gmax, s.ion.nspec) * h.tz * s.n3 * cs);
       int ord = 0;
       for (int r = 0; r < h.nrowpairs; r += s.rp) L[P_X5].h.push_back({i, r, std::min(s.rp, h.nrowpairs - r), ord++});
       L[P_CTL].h.push_back({i, 0, 0, 0});
@@ -1111,8 +1140,7 @@ struct Engine {
     };
     if ((rc = attr(k_vec<T>, P_VEC))) return rc;
     if ((rc = attr(k_xfwd<T>, P_X1))) return rc;
-    if ((rc = attr(k_ypass<T>, P_Y2))) return rc;
-    if ((rc = attr(k_ypass<T>, P_Y4))) return rc;
+    if ((rc = attr(k_ypass<T>, lists[prec][P_Y2].smem >= lists[prec][P_Y4].smem ? P_Y2 : P_Y4))) return rc;
     if ((rc = attr(k_zpass<T>, P_Z3))) return rc;
     return attr(k_xinv<T>, P_X5);
   }
@@ -1531,6 +1559,7 @@ static size_t up256(size_t x) { return (x + 255) & ~size_t(255); }
 static void make_plan(int n, FftPlan& p, int* off) {
   memset(&p, 0, sizeof(p));
   p.n = n;
+  p.root = -1;
   p.tw_base = *off;
   int r[FFT_MAX_STAGES], nr = 0, m = n, e2 = 0;
   while (m % 2 == 0) { m /= 2; ++e2; }

@@ -48,6 +48,7 @@ struct FftPlan {
   int tw[FFT_MAX_STAGES];  // offset of the stage's twiddles in the plan table
   unsigned ns_magic[FFT_MAX_STAGES];  // ceil(2^20 / Ns): j / Ns == (j * magic) >> 20 for j < 2048
   int tw_base;             // offset of this plan in the global twiddle table
+  int root;                // offset of exp(-2 pi i e / n), e = 0..n-1, in that table; -1: none
 };
 
 // Exact quotient j / d for 0 <= j < 2048 and 1 <= d <= 512 from magic = ceil(2^20 / d).
@@ -382,6 +383,205 @@ HD cx<T>* fft_batch(cx<T>* buf, cx<T>* tmp, int nb, int si, const FftPlan& p, co
                     int tid, int nthr) {
   return dir < 0 ? fft_batch<T, -1>(buf, tmp, nb, si, p, twtab, tid, nthr)
                  : fft_batch<T, 1>(buf, tmp, nb, si, p, twtab, tid, nthr);
+}
+
+// ------------------------------------------------------------ transforms between accessors
+// Element i of column b of a batch held in shared memory at p[b + i*si].
+template <typename T>
+struct SmemIO {
+  cx<T>* p;
+  int si;
+  HD cx<T> ld(int i, int b) const { return p[b + i * si]; }
+  HD void st(int i, int b, cx<T> v) const { p[b + i * si] = v; }
+};
+
+// One Stockham stage of radix R whose inputs come from src.ld(i, b) and whose
+// outputs go to dst.st(i, b, v) (same work split as fft_stage_r).
+template <typename T, int R, int DIR, class Src, class Dst>
+HD void fft_stage_io(const Src& src, const Dst& dst, int nb, unsigned mnb, int n, int Ns, unsigned magic,
+                     const cx<T>* __restrict__ tw, int tid, int nthr) {
+  const int nbf = n / R;
+  const int total = nbf * nb;
+  for (int w = tid; w < total; w += nthr) {
+    const int j = magic_div32(w, mnb);
+    const int b = w - j * nb;
+    const int jq = magic_div(j, magic);
+    const int kmod = j - jq * Ns;
+    cx<T> v[R];
+#pragma unroll
+    for (int m = 0; m < R; ++m) v[m] = src.ld(j + m * nbf, b);
+    if (Ns > 1) {
+      const cx<T>* t = tw + kmod * (R - 1);
+#pragma unroll
+      for (int m = 1; m < R; ++m) {
+        cx<T> f = t[m - 1];
+        if (DIR > 0) f.y = -f.y;
+        v[m] = cmul(v[m], f);
+      }
+    }
+    Dft<T, R, DIR>::run(v);
+    const int base = jq * Ns * R + kmod;
+#pragma unroll
+    for (int m = 0; m < R; ++m) dst.st(base + m * Ns, b, v[m]);
+  }
+}
+
+template <typename T, int DIR, class Src, class Dst>
+HD void fft_stage_io_any(const Src& src, const Dst& dst, int nb, unsigned mnb, int n, int R, int Ns, unsigned magic,
+                         const cx<T>* tw, int tid, int nthr) {
+  constexpr int RM = FftMaxRadix<T>::value;
+#define OFDFT_IO_CASE(r)                                                                           \
+  case r:                                                                                          \
+    if constexpr (r <= RM) fft_stage_io<T, r, DIR>(src, dst, nb, mnb, n, Ns, magic, tw, tid, nthr); \
+    break;
+  switch (R) {
+    OFDFT_IO_CASE(2)
+    OFDFT_IO_CASE(3)
+    OFDFT_IO_CASE(4)
+    OFDFT_IO_CASE(5)
+    OFDFT_IO_CASE(6)
+    OFDFT_IO_CASE(7)
+    OFDFT_IO_CASE(8)
+    OFDFT_IO_CASE(9)
+    OFDFT_IO_CASE(10)
+    OFDFT_IO_CASE(12)
+    OFDFT_IO_CASE(14)
+    OFDFT_IO_CASE(15)
+    OFDFT_IO_CASE(16)
+    default: break;
+  }
+#undef OFDFT_IO_CASE
+}
+
+// Full transform of nb columns: stage 0 reads src, stage s (0 <= s < nst-1)
+// writes buffer A (s even) or B (s odd), the last stage writes dst.  src may
+// be A's or B's storage only if it is not the buffer stage 0 writes (A).
+// When dst is shared memory it must be fft_out_buffer(nst, A, B), the buffer
+// the last stage does not read.  No barrier after the last stage.
+template <typename T, int DIR, class Src, class Dst>
+HD void fft_run(const Src& src, const Dst& dst, cx<T>* A, cx<T>* B, int nb, const FftPlan& p, const cx<T>* twtab,
+                int tid, int nthr) {
+  const unsigned mnb = magic32(nb);
+  const int nst = p.nst, n = p.n;
+  const cx<T>* tw0 = twtab + p.tw_base;
+  if (nst == 1) {
+    fft_stage_io_any<T, DIR>(src, dst, nb, mnb, n, p.R[0], p.Ns[0], p.ns_magic[0], tw0 + p.tw[0], tid, nthr);
+    return;
+  }
+  const SmemIO<T> a{A, nb}, b{B, nb};
+  fft_stage_io_any<T, DIR>(src, a, nb, mnb, n, p.R[0], p.Ns[0], p.ns_magic[0], tw0 + p.tw[0], tid, nthr);
+  BLOCK_SYNC();
+  for (int s = 1; s < nst - 1; ++s) {
+    if (s & 1) fft_stage_io_any<T, DIR>(a, b, nb, mnb, n, p.R[s], p.Ns[s], p.ns_magic[s], tw0 + p.tw[s], tid, nthr);
+    else fft_stage_io_any<T, DIR>(b, a, nb, mnb, n, p.R[s], p.Ns[s], p.ns_magic[s], tw0 + p.tw[s], tid, nthr);
+    BLOCK_SYNC();
+  }
+  const int sl = nst - 1;
+  if (sl & 1) fft_stage_io_any<T, DIR>(a, dst, nb, mnb, n, p.R[sl], p.Ns[sl], p.ns_magic[sl], tw0 + p.tw[sl], tid, nthr);
+  else fft_stage_io_any<T, DIR>(b, dst, nb, mnb, n, p.R[sl], p.Ns[sl], p.ns_magic[sl], tw0 + p.tw[sl], tid, nthr);
+}
+
+// The buffer of fft_run that the last stage does not read (A or B).
+template <typename T>
+HD cx<T>* fft_out_buffer(int nst, cx<T>* A, cx<T>* B) { return ((nst - 1) & 1) ? B : A; }
+
+// ------------------------------------------------------------ two-step register FFT
+// A transform of length n = R1 * R2 (both compile-time) over NC columns, with
+// one shared-memory exchange: with j = t + R2*j1 and k = k1 + R1*k2,
+//   X[k1 + R1 k2] = sum_t W_R2^{t k2} W_n^{t k1} sum_j1 W_R1^{j1 k1} x[t + R2 j1],
+// W_m = exp(DIR * 2 pi i / m).  Step 1 (one work item per column and t)
+// loads its R1 inputs from src.ld(i, c) straight into registers, does the
+// R1-point DFT and the twiddles W_n^{t k1} = roots[t*k1] (t*k1 < n), and
+// writes the exchange buffer X (NC * n values); step 2 (one work item per
+// column and k1) does the R2-point DFT and writes the outputs with
+// dst.st(k, c, v).  Consecutive threads take consecutive columns.  src may be
+// the same memory as dst: every input is read before the barrier between the
+// steps and every output is written after it.
+template <typename T, int R1, int R2, int DIR, class Src, class Dst>
+HD void fft2_tile(const Src& src, const Dst& dst, cx<T>* __restrict__ X, int NC, const cx<T>* __restrict__ roots,
+                  int tid, int nthr) {
+  const unsigned mnc = magic32(NC);
+  for (int w = tid; w < NC * R2; w += nthr) {
+    const int t = magic_div32(w, mnc), c = w - t * NC;
+    cx<T> v[R1];
+#pragma unroll
+    for (int j1 = 0; j1 < R1; ++j1) v[j1] = src.ld(t + R2 * j1, c);
+    Dft<T, R1, DIR>::run(v);
+#pragma unroll
+    for (int k1 = 1; k1 < R1; ++k1) {
+      cx<T> f = roots[t * k1];
+      if (DIR > 0) f.y = -f.y;
+      v[k1] = cmul(v[k1], f);
+    }
+    cx<T>* x = X + c + NC * t;
+#pragma unroll
+    for (int k1 = 0; k1 < R1; ++k1) x[NC * R2 * k1] = v[k1];
+  }
+  BLOCK_SYNC();
+  for (int w = tid; w < NC * R1; w += nthr) {
+    const int k1 = magic_div32(w, mnc), c = w - k1 * NC;
+    cx<T> v[R2];
+    const cx<T>* x = X + c + NC * R2 * k1;
+#pragma unroll
+    for (int t = 0; t < R2; ++t) v[t] = x[NC * t];
+    Dft<T, R2, DIR>::run(v);
+#pragma unroll
+    for (int k2 = 0; k2 < R2; ++k2) dst.st(k1 + R1 * k2, c, v[k2]);
+  }
+}
+
+// Largest step-2 radix of the two-step transforms per precision (R2 complex
+// values stay in registers).
+template <typename T> struct Fft2MaxRadix { static constexpr int value = 16; };
+template <> struct Fft2MaxRadix<double> { static constexpr int value = 12; };
+
+// The lengths with a two-step transform and their factors (R1 <= R2).
+#define OFDFT_FFT2_SIZES(X) \
+  X(32, 4, 8)               \
+  X(48, 6, 8)               \
+  X(64, 8, 8)               \
+  X(72, 8, 9)               \
+  X(80, 8, 10)              \
+  X(96, 8, 12)              \
+  X(120, 10, 12)            \
+  X(128, 8, 16)             \
+  X(144, 12, 12)            \
+  X(160, 10, 16)            \
+  X(192, 12, 16)            \
+  X(240, 15, 16)            \
+  X(256, 16, 16)
+
+// Whether length n has a two-step transform in precision T.
+template <typename T>
+HD bool fft2_supported(const FftPlan& p) {
+  if (p.root < 0) return false;
+  switch (p.n) {
+#define OFDFT_FFT2_CASE(N, A, B) \
+  case N:                        \
+    return B <= Fft2MaxRadix<T>::value;
+    OFDFT_FFT2_SIZES(OFDFT_FFT2_CASE)
+#undef OFDFT_FFT2_CASE
+    default:
+      return false;
+  }
+}
+
+// Two-step transform of length p.n (fft2_supported must hold).
+template <typename T, int DIR, class Src, class Dst>
+HD void fft2_run(const Src& src, const Dst& dst, cx<T>* X, int NC, const FftPlan& p, const cx<T>* twtab, int tid,
+                 int nthr) {
+  const cx<T>* roots = twtab + p.root;
+  switch (p.n) {
+#define OFDFT_FFT2_CASE(N, A, B)                                                       \
+  case N:                                                                              \
+    if constexpr (B <= Fft2MaxRadix<T>::value)                                         \
+      fft2_tile<T, A, B, DIR>(src, dst, X, NC, roots, tid, nthr);                      \
+    break;
+    OFDFT_FFT2_SIZES(OFDFT_FFT2_CASE)
+#undef OFDFT_FFT2_CASE
+    default:
+      break;
+  }
 }
 
 }  // namespace ofdft

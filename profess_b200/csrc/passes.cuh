@@ -337,7 +337,14 @@ HDNI void xfwd_block(const Args<T>& a, int bid, int tid, int nthr, char* smem) {
     buf[b + i * nb] = mk<T>(v0, v1);
   }
   BLOCK_SYNC();
-  const cx<T>* res = fft_batch<T, -1>(buf, tmp, nb, nb, px, a.tw, tid, nthr);
+  const cx<T>* res = buf;
+  if (fft2_supported<T>(px)) {  // in place in buf, tmp as the exchange buffer
+    const SmemIO<T> io{buf, nb};
+    fft2_run<T, -1>(io, io, tmp, nb, px, a.tw, tid, nthr);
+    BLOCK_SYNC();
+  } else {
+    res = fft_batch<T, -1>(buf, tmp, nb, nb, px, a.tw, tid, nthr);
+  }
   const unsigned mk1 = magic32(k1);
   for (int w = tid; w < nb * k1; w += nthr) {
     const int b = magic_div32(w, mk1), k = w - b * k1;
@@ -349,6 +356,34 @@ HDNI void xfwd_block(const Args<T>& a, int bid, int tid, int nthr, char* smem) {
     if (j1 < nrows) out[j1 * k1 + k] = mk<T>(dif.y * T(0.5), -dif.x * T(0.5));
   }
 }
+
+// ------------------------------------------------------------ column accessors
+// y pass: element i of column b of a tile at p[i*stride + b].
+template <typename T>
+struct ColIO {
+  cx<T>* p;
+  int stride;
+  HD cx<T> ld(int i, int b) const { return p[(size_t)i * stride + b]; }
+  HD void st(int i, int b, cx<T> v) const { p[(size_t)i * stride + b] = v; }
+};
+
+// z pass: column q*nb + b is field q of the group at p[q*nc + i*plane + b];
+// fields q >= gin read as zero and fields q >= gout are not stored.
+template <typename T>
+struct GroupIO {
+  cx<T>* p;
+  int nb, plane, gin, gout;
+  unsigned mnb;
+  long long nc;
+  HD cx<T> ld(int i, int col) const {
+    const int q = magic_div32(col, mnb), b = col - q * nb;
+    return q < gin ? p[(size_t)q * nc + (size_t)i * plane + b] : mk<T>(T(0), T(0));
+  }
+  HD void st(int i, int col, cx<T> v) const {
+    const int q = magic_div32(col, mnb), b = col - q * nb;
+    if (q < gout) p[(size_t)q * nc + (size_t)i * plane + b] = v;
+  }
+};
 
 // ------------------------------------------------------------ passes 2, 4
 template <typename T>
@@ -364,6 +399,12 @@ HDNI void ypass_block(const Args<T>& a, int bid, int tid, int nthr, char* smem, 
   cx<T>* buf = (cx<T>*)smem;
   cx<T>* tmp = buf + nb * n2;
   cx<T>* __restrict__ sp = (cx<T>*)s.spec + (size_t)f * (size_t)s.Nc + (size_t)z * n2 * k1 + kx0;
+  if (fft2_supported<T>(s.py)) {  // in place, straight from and to the spectra
+    const ColIO<T> io{sp, k1};
+    if (dir < 0) fft2_run<T, -1>(io, io, buf, nb, s.py, a.tw, tid, nthr);
+    else fft2_run<T, 1>(io, io, buf, nb, s.py, a.tw, tid, nthr);
+    return;
+  }
   const unsigned mnb = magic32(nb);
   for (int w = tid; w < nb * n2; w += nthr) {
     const int i = magic_div32(w, mnb), b = w - i * nb;
@@ -378,40 +419,15 @@ HDNI void ypass_block(const Args<T>& a, int bid, int tid, int nthr, char* smem, 
 }
 
 // ------------------------------------------------------------ pass 3
-// All gn fields of a group are transformed as one batch of gn*nb sequences
-// laid out [kz][q*nb + b].
+// The k-space operator of one z-pass tile: res holds the forward z
+// transforms of the group's gn fields, [kz][q*nb + b] (NB = gn*nb), for kx =
+// kx0 + b and ky; the results replace them in place.
 template <typename T>
-HDNI void zpass_block(const Args<T>& a, int bid, int tid, int nthr, char* smem) {
-  const Task t = a.tasks[bid];
-  const SlotDev& s = a.slots[t.slot];
-  const Ctl& c = a.ctl[t.slot];
-  if (c.status != ST_RUNNING || c.ev == EV_NONE) return;
-  const int g = t.a, ky = t.b, kx0 = tile_kx0(t.c), nb = tile_width(t.c);
-  const int ev = c.ev;
-  const bool setup_mode = ev == EV_ION || ev == EV_FORCE;
-  if (setup_mode && g != 0) return;
-  const int n2 = s.n2, n3 = s.n3, k1 = s.k1;
-  const int kind = ev == EV_ION ? G_ION : ev == EV_FORCE ? G_FORCE : s.group_kind[g];
-  const int gn = setup_mode ? s.ion.nspec : s.group_nf[g];
-  const int gin = ev == EV_FORCE ? 1 : gn;  // fields loaded
-  const int gout = ev == EV_ION ? 1 : gn;   // fields stored
-  const int NB = gn * nb;
-  const int plane = n2 * k1;
-  const int Nc = (int)s.Nc;
-  cx<T>* __restrict__ spec =
-      (cx<T>*)s.spec + (size_t)(setup_mode ? 0 : s.group_f0[g]) * (size_t)Nc + ky * k1 + kx0;
-  cx<T>* buf = (cx<T>*)smem;
-  cx<T>* tmp = buf + NB * n3;
-  const unsigned mNB = magic32(NB), mnb = magic32(nb);
-  for (int w = tid; w < NB * n3; w += nthr) {
-    const int i = magic_div32(w, mNB), qb = w - i * NB;
-    const int q = magic_div32(qb, mnb), b = qb - q * nb;
-    buf[w] = q < gin ? spec[(size_t)q * Nc + i * plane + b] : mk<T>(T(0), T(0));
-  }
-  BLOCK_SYNC();
-  cx<T>* res = fft_batch<T, -1>(buf, tmp, NB, NB, s.pz, a.tw, tid, nthr);
-  cx<T>* oth = res == buf ? tmp : buf;
+HD void zpass_operator(const SlotDev& s, int kind, int gn, bool setup_mode, cx<T>* res, int NB, int nb, int kx0,
+                       int ky, int tid, int nthr) {
+  const int n2 = s.n2, n3 = s.n3, k1 = s.k1, plane = n2 * k1, Nc = (int)s.Nc;
   const int m2 = ky > n2 / 2 ? ky - n2 : ky;
+  const unsigned mnb = magic32(nb);
   const T* __restrict__ kern = (const T*)s.kern + ky * k1 + kx0;
   const T sc = (T)s.inv_n;
   // |G|^2 of the Hartree and vW operators in the slot's precision; the
@@ -483,6 +499,52 @@ HDNI void zpass_block(const Args<T>& a, int bid, int tid, int nthr, char* smem) 
       }
     }
   }
+}
+
+// All gn fields of a group are transformed as one batch of gn*nb sequences
+// laid out [kz][q*nb + b].
+template <typename T>
+HDNI void zpass_block(const Args<T>& a, int bid, int tid, int nthr, char* smem) {
+  const Task t = a.tasks[bid];
+  const SlotDev& s = a.slots[t.slot];
+  const Ctl& c = a.ctl[t.slot];
+  if (c.status != ST_RUNNING || c.ev == EV_NONE) return;
+  const int g = t.a, ky = t.b, kx0 = tile_kx0(t.c), nb = tile_width(t.c);
+  const int ev = c.ev;
+  const bool setup_mode = ev == EV_ION || ev == EV_FORCE;
+  if (setup_mode && g != 0) return;
+  const int n2 = s.n2, n3 = s.n3, k1 = s.k1;
+  const int kind = ev == EV_ION ? G_ION : ev == EV_FORCE ? G_FORCE : s.group_kind[g];
+  const int gn = setup_mode ? s.ion.nspec : s.group_nf[g];
+  const int gin = ev == EV_FORCE ? 1 : gn;  // fields loaded
+  const int gout = ev == EV_ION ? 1 : gn;   // fields stored
+  const int NB = gn * nb;
+  const int plane = n2 * k1;
+  const int Nc = (int)s.Nc;
+  cx<T>* __restrict__ spec =
+      (cx<T>*)s.spec + (size_t)(setup_mode ? 0 : s.group_f0[g]) * (size_t)Nc + ky * k1 + kx0;
+  cx<T>* buf = (cx<T>*)smem;
+  cx<T>* tmp = buf + NB * n3;
+  const unsigned mNB = magic32(NB), mnb = magic32(nb);
+  if (fft2_supported<T>(s.pz)) {  // forward into tmp, operator, inverse back to the spectra
+    const GroupIO<T> gio{spec, nb, plane, gin, gout, mnb, (long long)Nc};
+    const SmemIO<T> o{tmp, NB};
+    fft2_run<T, -1>(gio, o, buf, NB, s.pz, a.tw, tid, nthr);
+    BLOCK_SYNC();
+    zpass_operator<T>(s, kind, gn, setup_mode, tmp, NB, nb, kx0, ky, tid, nthr);
+    BLOCK_SYNC();
+    fft2_run<T, 1>(o, gio, buf, NB, s.pz, a.tw, tid, nthr);
+    return;
+  }
+  for (int w = tid; w < NB * n3; w += nthr) {
+    const int i = magic_div32(w, mNB), qb = w - i * NB;
+    const int q = magic_div32(qb, mnb), b = qb - q * nb;
+    buf[w] = q < gin ? spec[(size_t)q * Nc + i * plane + b] : mk<T>(T(0), T(0));
+  }
+  BLOCK_SYNC();
+  cx<T>* res = fft_batch<T, -1>(buf, tmp, NB, NB, s.pz, a.tw, tid, nthr);
+  cx<T>* oth = res == buf ? tmp : buf;
+  zpass_operator<T>(s, kind, gn, setup_mode, res, NB, nb, kx0, ky, tid, nthr);
   BLOCK_SYNC();
   const cx<T>* out = fft_batch<T, 1>(res, oth, NB, NB, s.pz, a.tw, tid, nthr);
   for (int w = tid; w < NB * n3; w += nthr) {
@@ -557,7 +619,14 @@ HDNI void xinv_block(const Args<T>& a, int bid, int tid, int nthr, char* smem) {
     buf[k * NB + fb] = mk<T>(A.x - B.y, A.y + B.x);
   }
   BLOCK_SYNC();
-  const cx<T>* res = fft_batch<T, 1>(buf, tmp, NB, NB, s.px, a.tw, tid, nthr);
+  const cx<T>* res = buf;
+  if (fft2_supported<T>(s.px)) {  // in place in buf, tmp as the exchange buffer
+    const SmemIO<T> io{buf, NB};
+    fft2_run<T, 1>(io, io, tmp, NB, s.px, a.tw, tid, nthr);
+    BLOCK_SYNC();
+  } else {
+    res = fft_batch<T, 1>(buf, tmp, NB, NB, s.px, a.tw, tid, nthr);
+  }
   if (setup_mode) {
     // EV_ION: ionPotReal; EV_FORCE: the per-species Factor arrays in buf[B_B + s]
     const unsigned m2n1s = magic32(2 * n1);

@@ -43,6 +43,26 @@ def test_eval_mixed_radix_and_odd_grids(emu_engine, n):
     _eval_parity(emu_engine, f, cell, seed=2)
 
 
+@pytest.mark.parametrize("n", [(32, 48, 96), (10, 72, 120), (9, 64, 80), (96, 12, 10), (120, 9, 8)])
+def test_eval_two_step_lengths(emu_engine, n):
+    """Lengths with the two-step register transform (R1 x R2) along x, y, z."""
+    cell, _, _, _ = cases.golden_case("wt_al4_displaced")
+    f = cases.functional_for(cell, n, fn.KEDF_WT, 5 / 6, 5 / 6)
+    _eval_parity(emu_engine, f, cell, seed=5)
+
+
+@pytest.mark.parametrize("n", [(8, 128, 160), (6, 256, 192), (5, 240, 144), (160, 6, 5), (256, 4, 6)])
+def test_eval_two_step_lengths_fp32(emu_engine, n):
+    """FP32 two-step lengths with a 16-point second step.  On these random
+    WGC densities FP32 gives a max-relative potential error of 1.6e-4 to
+    5.3e-4 whatever the transform: the generic Stockham lengths next to these
+    show the same (126 x 162: 1.59e-4 vs 128 x 160: 1.58e-4; 252 x 196:
+    5.03e-4 vs 256 x 192: 5.28e-4), hence 1e-3."""
+    cell, _, _, _ = cases.golden_case("wgc_al4_fcc")
+    f = cases.functional_for(cell, n, fn.KEDF_WGC, 1.2060113295832982827, 0.46065533708336838393)
+    _eval_parity(emu_engine, f, cell, seed=6, prec=native.FP32, tol_pot=1e-3, tol_e=5e-5)
+
+
 def test_eval_wt_alpha_ne_beta(emu_engine):
     cell, _, _, _ = cases.golden_case("wt_al4_displaced")
     f = cases.functional_for(cell, (16, 16, 18), fn.KEDF_WT, 1.0, 2.0 / 3.0)

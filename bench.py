@@ -54,16 +54,21 @@ def _peaks():
 
 
 def _traffic_per_eval():
-    """DRAM bytes of one FP32 96^3 potential evaluation from the committed ncu summary."""
+    """DRAM bytes of one 96^3 WT potential evaluation of one FP32 and one FP64
+    slot (passes 1-5, from the committed ncu summary), or None."""
     path = os.path.join(ROOT, "profiles", "eval_traffic.txt")
+    vals = {}
     try:
         with open(path) as fh:
             for ln in fh:
-                if ln.startswith("dram_bytes_per_eval_fp32_96:"):
-                    return float(ln.split(":")[1])
+                for key in ("dram_bytes_per_eval_fp32_96:", "dram_bytes_per_eval_fp64_96:"):
+                    if ln.startswith(key):
+                        vals[key[:-1]] = float(ln.split(":")[1])
     except OSError:
-        pass
-    return None
+        return None
+    if len(vals) < 2:
+        return None
+    return vals["dram_bytes_per_eval_fp32_96"], vals["dram_bytes_per_eval_fp64_96"]
 
 
 class ClockSampler:
@@ -390,7 +395,9 @@ def run_ours(args):
                      "kernel": "batched potential evaluation (passes 1-5 + controller) of every cell in FP32 and "
                                "FP64 (%d slots)" % (2 * B),
                      "ms_per_launch": ms_eval,
-                     "traffic": (3 * tr * B) if tr else None},
+                     "traffic": (B * (tr[0] + tr[1])) if tr else None,
+                     "traffic_source": "profiles/eval_traffic.txt (ncu dram__bytes per slot evaluation x slots)"
+                     if tr else None},
         "cpu_baseline": cpu,
         "clocks": clk,
         "gpu_launches": l1 - l0,

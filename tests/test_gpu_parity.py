@@ -9,6 +9,7 @@ import pytest
 import cases
 from oracle import functional as fn
 from oracle import ntn
+from profess_b200 import native
 
 pytestmark = pytest.mark.gpu
 
@@ -57,6 +58,40 @@ def test_eval_odd_and_mixed_radix_grids(gpu_engine, n):
         pot_g, et_g = gpu_engine.calculate_potential_plus(s, rho)
         assert np.abs(pot_g - pot_o).max() / np.abs(pot_o).max() < 1e-11
         assert np.abs(et_g - et_o).max() < 1e-10
+    finally:
+        gpu_engine.slot_destroy(s)
+
+
+@pytest.mark.parametrize("n", [(32, 48, 96), (96, 12, 10), (10, 72, 120), (9, 64, 80)])
+def test_eval_two_step_lengths(gpu_engine, n):
+    """Lengths with the two-step register transform along x, y and z."""
+    cell, _, _, _ = cases.golden_case("wt_al4_displaced")
+    f = cases.functional_for(cell, n, fn.KEDF_WT, 5 / 6, 5 / 6)
+    s = cases.engine_slot(gpu_engine, f, cell)
+    try:
+        rho = cases.random_density(n, cell.num_electrons, cell.vol, seed=5)
+        pot_o, et_o = fn.calculate_potential_plus(f, rho)
+        pot_g, et_g = gpu_engine.calculate_potential_plus(s, rho)
+        assert np.abs(pot_g - pot_o).max() / np.abs(pot_o).max() < 1e-11
+        assert np.abs(et_g - et_o).max() < 1e-10
+    finally:
+        gpu_engine.slot_destroy(s)
+
+
+@pytest.mark.parametrize("n", [(8, 128, 160), (6, 256, 192), (160, 6, 5)])
+def test_eval_two_step_lengths_fp32(gpu_engine, n):
+    """FP32 two-step lengths with a 16-point second step (WGC).  FP32 gives a
+    max-relative potential error of up to ~5e-4 on these random densities
+    with either transform, hence 1e-3 (energies per term to 5e-5 Ha)."""
+    cell, _, _, _ = cases.golden_case("wgc_al4_fcc")
+    f = cases.functional_for(cell, n, fn.KEDF_WGC, 1.2060113295832982827, 0.46065533708336838393)
+    s = cases.engine_slot(gpu_engine, f, cell, precision=native.FP32)
+    try:
+        rho = cases.random_density(n, cell.num_electrons, cell.vol, seed=6)
+        pot_o, et_o = fn.calculate_potential_plus(f, rho)
+        pot_g, et_g = gpu_engine.calculate_potential_plus(s, rho)
+        assert np.abs(pot_g - pot_o).max() / np.abs(pot_o).max() < 1e-3
+        assert np.abs(et_g - et_o).max() < 5e-5
     finally:
         gpu_engine.slot_destroy(s)
 

@@ -20,7 +20,6 @@
 // tw[off_s + k*(R-1) + (m-1)] = exp(-2*pi*i*m*k/(Ns*R)), k = 0..Ns-1.
 // The inverse transform uses the conjugates.  No scaling is applied here.
 #pragma once
-#include <type_traits>
 #include "cx.cuh"
 
 namespace ofdft {
@@ -218,18 +217,6 @@ HDC double root_cs(int R, int e, int want_sin) {
   }
 }
 
-// Compile-time loop: f(std::integral_constant<int, I>()) for I = B .. E-1.
-template <int B, int E>
-struct StaticFor {
-  template <typename F>
-  static HD void run(F&& f) {
-    if constexpr (B < E) {
-      f(std::integral_constant<int, B>());
-      StaticFor<B + 1, E>::run(f);
-    }
-  }
-};
-
 // x * exp(DIR * 2 pi i E / R), with the trivial angles special-cased.
 template <typename T, int R, int E, int DIR>
 HD cx<T> twiddle_const(cx<T> x) {
@@ -269,22 +256,36 @@ template <typename T, int DIR> struct Dft<T, 16, DIR> { static HD void run(cx<T>
 // R = A*B point DFT in registers (natural order in and out): with
 // j = B*j1 + j2 and k = k1 + A*k2,
 //   X[k1 + A k2] = sum_j2 W_B^{j2 k2} W_R^{j2 k1} sum_j1 W_A^{j1 k1} x[B j1 + j2],
-// W_M = exp(DIR * 2 pi i / M).
+// W_M = exp(DIR * 2 pi i / M).  The loops over j2 and k1 are template
+// recursions, so every index and twiddle angle is a compile-time constant and
+// the arrays stay in registers.
+template <typename T, int A, int B, int DIR, int J2, int K1>
+struct DftAbTwiddle {  // y[k1*B + J2] = W_R^{J2 k1} u[k1] for k1 = K1 .. A-1
+  static HD void run(const cx<T>* u, cx<T>* y) {
+    if constexpr (K1 < A) {
+      y[K1 * B + J2] = twiddle_const<T, A * B, J2 * K1, DIR>(u[K1]);
+      DftAbTwiddle<T, A, B, DIR, J2, K1 + 1>::run(u, y);
+    }
+  }
+};
+template <typename T, int A, int B, int DIR, int J2>
+struct DftAbFirst {  // A-point DFTs over j1 for j2 = J2 .. B-1, with twiddles
+  static HD void run(const cx<T>* v, cx<T>* y) {
+    if constexpr (J2 < B) {
+      cx<T> u[A];
+#pragma unroll
+      for (int j1 = 0; j1 < A; ++j1) u[j1] = v[B * j1 + J2];
+      Dft<T, A, DIR>::run(u);
+      DftAbTwiddle<T, A, B, DIR, J2, 0>::run(u, y);
+      DftAbFirst<T, A, B, DIR, J2 + 1>::run(v, y);
+    }
+  }
+};
+
 template <typename T, int A, int B, int DIR>
 HD void dft_ab(cx<T>* v) {
-  constexpr int R = A * B;
-  cx<T> y[R];
-  StaticFor<0, B>::run([&](auto j2c) {
-    constexpr int j2 = decltype(j2c)::value;
-    cx<T> u[A];
-#pragma unroll
-    for (int j1 = 0; j1 < A; ++j1) u[j1] = v[B * j1 + j2];
-    Dft<T, A, DIR>::run(u);
-    StaticFor<0, A>::run([&](auto k1c) {
-      constexpr int k1 = decltype(k1c)::value;
-      y[k1 * B + j2] = twiddle_const<T, R, j2 * k1, DIR>(u[k1]);
-    });
-  });
+  cx<T> y[A * B];
+  DftAbFirst<T, A, B, DIR, 0>::run(v, y);
 #pragma unroll
   for (int k1 = 0; k1 < A; ++k1) {
     cx<T> u[B];

@@ -12,7 +12,9 @@
 //                       real-space epilogue (potential, chain rule, energies and
 //                       the optimiser's fused sums)
 //
-// Every block processes one task.  Blocks of the vector kernel and of pass 5
+// Every block processes one task.  The block functions are force-inlined into
+// their kernels: each kernel calls one, and a non-inlined call puts the
+// functions' small structs and arrays in local memory.  Blocks of the vector kernel and of pass 5
 // store their per-channel sums in the slot's partials; a controller kernel
 // that follows (one block per slot) reduces them in a fixed order (the result
 // does not depend on block scheduling) and runs the NTN controller.
@@ -129,7 +131,7 @@ HDNI inline void ctl_block(SlotDev* slots, Ctl* ctls, const Task* tasks, int kid
 
 // ------------------------------------------------------------ vector ops
 template <typename T>
-HDNI void vec_block(const Args<T>& a, int bid, int tid, int nthr, char* smem) {
+HD void vec_block(const Args<T>& a, int bid, int tid, int nthr, char* smem) {
   const Task t = a.tasks[bid];
   SlotDev& s = a.slots[t.slot];
   Ctl& c = a.ctl[t.slot];
@@ -299,7 +301,7 @@ HD T field_value(const FieldPar<T>& fp, int f, T rho, T sq) {
 
 // ------------------------------------------------------------ pass 1
 template <typename T>
-HDNI void xfwd_block(const Args<T>& a, int bid, int tid, int nthr, char* smem) {
+HD void xfwd_block(const Args<T>& a, int bid, int tid, int nthr, char* smem) {
   const Task t = a.tasks[bid];
   const SlotDev& s = a.slots[t.slot];
   const Ctl& c = a.ctl[t.slot];
@@ -387,7 +389,7 @@ struct GroupIO {
 
 // ------------------------------------------------------------ passes 2, 4
 template <typename T>
-HDNI void ypass_block(const Args<T>& a, int bid, int tid, int nthr, char* smem, int dir) {
+HD void ypass_block(const Args<T>& a, int bid, int tid, int nthr, char* smem, int dir) {
   const Task t = a.tasks[bid];
   const SlotDev& s = a.slots[t.slot];
   const Ctl& c = a.ctl[t.slot];
@@ -504,7 +506,7 @@ HD void zpass_operator(const SlotDev& s, int kind, int gn, bool setup_mode, cx<T
 // All gn fields of a group are transformed as one batch of gn*nb sequences
 // laid out [kz][q*nb + b].
 template <typename T>
-HDNI void zpass_block(const Args<T>& a, int bid, int tid, int nthr, char* smem) {
+HD void zpass_block(const Args<T>& a, int bid, int tid, int nthr, char* smem) {
   const Task t = a.tasks[bid];
   const SlotDev& s = a.slots[t.slot];
   const Ctl& c = a.ctl[t.slot];
@@ -579,7 +581,7 @@ HD void lda_point(T rho, T r13, T rs, T& vxc, T& exc) {
 // sequences laid out [i][f*nb + b]; then every point of the rows gets the
 // real-space epilogue.
 template <typename T>
-HDNI void xinv_block(const Args<T>& a, int bid, int tid, int nthr, char* smem) {
+HD void xinv_block(const Args<T>& a, int bid, int tid, int nthr, char* smem) {
   const Task t = a.tasks[bid];
   SlotDev& s = a.slots[t.slot];
   Ctl& c = a.ctl[t.slot];

@@ -18,7 +18,8 @@ import os
 import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-DEFAULT_LIB = os.path.join(HERE, "_lib", "libprofess_b200.so")
+# The in-tree CUDA build; PROFESS_B200_LIB names another build of the same ABI.
+DEFAULT_LIB = os.environ.get("PROFESS_B200_LIB") or os.path.join(HERE, "_lib", "libprofess_b200.so")
 
 KEDF_WT = 4
 KEDF_WGC = 5

@@ -484,8 +484,10 @@ struct Engine {
     h.nrowpairs = (int)((nrows + 1) / 2);
     const size_t csz = 2 * elem_size(h.prec);
     // tile sizes: about 1-2 K complex points per block, at most ~100 KB of shared memory
-    h.rp1 = std::max(1, std::min(32, 2048 / s.n1));
-    while (h.rp1 > 1 && 2 * (size_t)h.rp1 * s.n1 * csz > 100 * 1024) h.rp1--;
+    // x-forward tasks: every field (or species) of rp1 row pairs, in about 72 KB
+    const int nfx = std::max(s.nf, MAX_SPECIES);
+    h.rp1 = std::max(1, std::min(32, 1024 / s.n1));
+    while (h.rp1 > 1 && 2 * (size_t)nfx * h.rp1 * s.n1 * csz > 72 * 1024) h.rp1--;
     s.rp = std::max(1, std::min(32, 1024 / s.n1));
     while (s.rp > 1 && 2 * (size_t)s.nf * s.rp * s.n1 * csz > 72 * 1024) s.rp--;
     // y/z tiles: as many kx columns as fit the two shared buffers of a block
@@ -1012,11 +1014,10 @@ struct Engine {
       for (int t = 0; t < s.ntask[K_VEC]; ++t) L[P_VEC].h.push_back({i, t, 0, 0});
       L[P_VEC].nthr = 256;
       L[P_VEC].smem = std::max(L[P_VEC].smem, (size_t)(NCH * 33 * sizeof(double) + 16));
-      for (int f = 0; f < s.nf; ++f)
-        for (int r = 0; r < h.nrowpairs; r += h.rp1)
-          L[P_X1].h.push_back({i, f, r, std::min(h.rp1, h.nrowpairs - r)});
+      for (int r = 0; r < h.nrowpairs; r += h.rp1)
+        L[P_X1].h.push_back({i, 0, r, std::min(h.rp1, h.nrowpairs - r)});
       L[P_X1].nthr = 256;
-      L[P_X1].smem = std::max(L[P_X1].smem, 2 * (size_t)h.rp1 * s.n1 * cs);
+      L[P_X1].smem = std::max(L[P_X1].smem, 2 * (size_t)std::max(s.nf, s.ion.nspec) * h.rp1 * s.n1 * cs);
       for (int pass : {P_Y2, P_Y4}) {
         for (int f = 0; f < s.nf; ++f)
           for (int z = 0; z < s.n3; ++z)
@@ -1661,7 +1662,8 @@ extern "C" int ofdft_calculate_potential_plus_noalloc(const ofdft_cell_desc* d, 
   for (int g = 0; g < s.ngroups; ++g) { s.group_kind[g] = kinds[g]; s.group_f0[g] = g; s.group_nf[g] = 1; }
   const size_t cs = sizeof(cx<double>);
   const int nrows = s.n2 * s.n3, nrp = (nrows + 1) / 2;
-  const int rp1 = std::max(1, std::min(32, 2048 / s.n1));
+  int rp1 = std::max(1, std::min(32, 1024 / s.n1));
+  while (rp1 > 1 && 2 * (size_t)s.nf * rp1 * s.n1 * cs > 72 * 1024) rp1--;
   s.rp = std::max(1, std::min(32, 1024 / s.n1));
   while (s.rp > 1 && 2 * (size_t)s.nf * s.rp * s.n1 * cs > 72 * 1024) s.rp--;
   s.tx = 16;
@@ -1680,8 +1682,7 @@ extern "C" int ofdft_calculate_potential_plus_noalloc(const ofdft_cell_desc* d, 
     return true;
   };
   bool ok = true;
-  for (int f = 0; f < s.nf && ok; ++f)
-    for (int r = 0; r < nrp && ok; r += rp1) ok = push(0, {0, f, r, std::min(rp1, nrp - r)});
+  for (int r = 0; r < nrp && ok; r += rp1) ok = push(0, {0, 0, r, std::min(rp1, nrp - r)});
   for (int f = 0; f < s.nf && ok; ++f)
     for (int z = 0; z < s.n3 && ok; ++z)
       for (int t = 0; t < tile_count(s.k1, s.tx) && ok; ++t) ok = push(1, {0, f, z, tile_code(s.k1, s.tx, t)});
@@ -1725,7 +1726,7 @@ extern "C" int ofdft_calculate_potential_plus_noalloc(const ofdft_cell_desc* d, 
   a.ctl = (Ctl*)(base + o_ctl);
   a.tw = (const cx<double>*)(base + o_tw);
   a.vchunk = VCHUNK;
-  const size_t sm1 = 2 * (size_t)rp1 * s.n1 * cs;
+  const size_t sm1 = 2 * (size_t)s.nf * rp1 * s.n1 * cs;
   const size_t sm2 = 2 * (size_t)s.tx * s.n2 * cs;
   const size_t sm3 = 2 * (size_t)s.tx * s.n3 * cs;
   const size_t sm5 = 2 * (size_t)s.nf * s.rp * s.n1 * cs + NCH * 33 * sizeof(double) + 16;

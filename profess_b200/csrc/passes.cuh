@@ -271,89 +271,99 @@ HD FieldPar<T> field_par(const SlotDev& s) {
   return f;
 }
 
-// Value of forward field f at density rho (sq = sqrt(rho)).  WT fields:
-// rho, rho^beta, sqrt(rho), rho^alpha.  WGC fields: rho, sqrt(rho), then for
-// x = alpha (f = 2..4) and x = beta (f = 5..7): rho^x, theta rho^x,
-// theta^2 rho^x / 2 with theta = rho - rho* (KEDF_WGC.f90:219-270).
+// ------------------------------------------------------------ pass 1
+// All forward fields of one point (WT: rho, rho^beta, sqrt(rho) and, when
+// alpha != beta, rho^alpha; WGC: rho, sqrt(rho), then for x = alpha and
+// x = beta: rho^x, theta rho^x, theta^2 rho^x / 2 with theta = rho - rho*),
+// with each power computed once.
 template <typename T>
-HD T field_value(const FieldPar<T>& fp, int f, T rho, T sq) {
+HD void field_values(const FieldPar<T>& fp, int nf, T rho, T sq, T* v) {
+  v[0] = rho;
   if (fp.wt) {
-    switch (f) {
-      case 0: return rho;
-      case 1: return fp.pow56 ? sq * m_cbrt(rho) : m_pow(rho, fp.beta);
-      case 2: return sq;
-      default: return m_pow(rho, fp.alpha);
-    }
+    v[1] = fp.pow56 ? sq * m_cbrt(rho) : m_pow(rho, fp.beta);
+    v[2] = sq;
+    if (nf > 3) v[3] = m_pow(rho, fp.alpha);
+    return;
   }
-  switch (f) {
-    case 0: return rho;
-    case 1: return sq;
-    default: break;
-  }
-  const T ex = f < 5 ? fp.alpha : fp.beta;
-  const int k = (f - 2) % 3;
-  const T rx = m_pow(rho, ex);
+  v[1] = sq;
   const T th = rho - fp.rho_s;
-  if (k == 0) return rx;
-  if (k == 1) return th * rx;
-  return th * th * rx / T(2);
+#pragma unroll
+  for (int h = 0; h < 2; ++h) {
+    const T rx = m_pow(rho, h == 0 ? fp.alpha : fp.beta);
+    v[2 + 3 * h] = rx;
+    v[3 + 3 * h] = th * rx;
+    v[4 + 3 * h] = th * th * rx / T(2);
+  }
 }
 
-// ------------------------------------------------------------ pass 1
+// Every field of a range of row pairs in one block: the inputs of a point are
+// read and its field values computed once, and the nf * nb x-transforms run
+// as one batch, column f*nb + b, element i at buf[(f*nb + b) + i*NB].
 template <typename T>
 HD void xfwd_block(const Args<T>& a, int bid, int tid, int nthr, char* smem) {
   const Task t = a.tasks[bid];
   const SlotDev& s = a.slots[t.slot];
   const Ctl& c = a.ctl[t.slot];
   if (c.status != ST_RUNNING || c.ev == EV_NONE) return;
-  const int f = t.a, rp0 = t.b, nb = t.c;
+  const int rp0 = t.b, nb = t.c;
   const int ev = c.ev;
-  if (ev == EV_ION && f >= s.ion.nspec) return;
-  if (ev == EV_FORCE && f != 0) return;
+  const int nfe = ev == EV_ION ? s.ion.nspec : ev == EV_FORCE ? 1 : s.nf;
+  const int NB = nfe * nb;
   const int n1 = s.n1, k1 = s.k1;
   const int nrows = s.n2 * s.n3;
+  const long long Nc = s.Nc;
   const EvalIn<T> in = eval_in<T>(s, c);
-  const T* __restrict__ qion = (const T*)s.buf[B_PHI + (f < NBUF ? f : 0)];
   const FieldPar<T> fp = field_par<T>(s);
   const FftPlan& px = s.px;
-  cx<T>* __restrict__ out = (cx<T>*)s.spec + (size_t)f * (size_t)s.Nc;
   cx<T>* buf = (cx<T>*)smem;
-  cx<T>* tmp = buf + nb * n1;
+  cx<T>* tmp = buf + NB * n1;
   const unsigned mn1 = magic32(n1);
   for (int w = tid; w < nb * n1; w += nthr) {
     const int b = magic_div32(w, mn1), i = w - b * n1;
     const int j0 = 2 * (rp0 + b), j1 = j0 + 1;
-    T v0, v1 = T(0);
-    if (ev == EV_ION) {  // B-spline charge of species f (FillQIonTable)
-      v0 = qion[j0 * n1 + i];
-      if (j1 < nrows) v1 = qion[j1 * n1 + i];
-    } else {
-      T phin, rho, sq;
-      in.at(j0 * n1 + i, phin, rho, sq);
-      v0 = ev == EV_FORCE ? rho : field_value(fp, f, rho, sq);
-      if (j1 < nrows) {
-        in.at(j1 * n1 + i, phin, rho, sq);
-        v1 = ev == EV_FORCE ? rho : field_value(fp, f, rho, sq);
+    const bool has1 = j1 < nrows;
+    cx<T>* d = buf + b + i * NB;
+    if (ev == EV_ION) {  // B-spline charge of each species (FillQIonTable)
+      for (int f = 0; f < nfe; ++f) {
+        const T* __restrict__ q = (const T*)s.buf[B_PHI + f];
+        d[f * nb] = mk<T>(q[j0 * n1 + i], has1 ? q[j1 * n1 + i] : T(0));
       }
+      continue;
     }
-    buf[b + i * nb] = mk<T>(v0, v1);
+    T v0[MAX_FIELDS], v1[MAX_FIELDS];
+    T phin, rho, sq;
+    in.at(j0 * n1 + i, phin, rho, sq);
+    if (ev == EV_FORCE) v0[0] = rho;
+    else field_values(fp, nfe, rho, sq, v0);
+#pragma unroll
+    for (int f = 0; f < MAX_FIELDS; ++f) v1[f] = T(0);
+    if (has1) {
+      in.at(j1 * n1 + i, phin, rho, sq);
+      if (ev == EV_FORCE) v1[0] = rho;
+      else field_values(fp, nfe, rho, sq, v1);
+    }
+#pragma unroll
+    for (int f = 0; f < MAX_FIELDS; ++f)
+      if (f < nfe) d[f * nb] = mk<T>(v0[f], v1[f]);
   }
   BLOCK_SYNC();
   const cx<T>* res = buf;
   if (fft2_supported<T>(px)) {  // in place in buf, tmp as the exchange buffer
-    const SmemIO<T> io{buf, nb};
-    fft2_run<T, -1>(io, io, tmp, nb, px, a.tw, tid, nthr);
+    const SmemIO<T> io{buf, NB};
+    fft2_run<T, -1>(io, io, tmp, NB, px, a.tw, tid, nthr);
     BLOCK_SYNC();
   } else {
-    res = fft_batch<T, -1>(buf, tmp, nb, nb, px, a.tw, tid, nthr);
+    res = fft_batch<T, -1>(buf, tmp, NB, NB, px, a.tw, tid, nthr);
   }
-  const unsigned mk1 = magic32(k1);
-  for (int w = tid; w < nb * k1; w += nthr) {
-    const int b = magic_div32(w, mk1), k = w - b * k1;
+  const unsigned mk1 = magic32(k1), mnb = magic32(nb);
+  for (int w = tid; w < NB * k1; w += nthr) {
+    const int col = magic_div32(w, mk1), k = w - col * k1;
+    const int f = magic_div32(col, mnb), b = col - f * nb;
     const int j0 = 2 * (rp0 + b), j1 = j0 + 1;
-    const cx<T> z = res[b + k * nb];
-    const cx<T> zc = conj(res[b + (k == 0 ? 0 : n1 - k) * nb]);
+    const cx<T> z = res[col + k * NB];
+    const cx<T> zc = conj(res[col + (k == 0 ? 0 : n1 - k) * NB]);
     const cx<T> sum = z + zc, dif = z - zc;
+    cx<T>* __restrict__ out = (cx<T>*)s.spec + (size_t)f * (size_t)Nc;
     out[j0 * k1 + k] = mk<T>(sum.x * T(0.5), sum.y * T(0.5));
     if (j1 < nrows) out[j1 * k1 + k] = mk<T>(dif.y * T(0.5), -dif.x * T(0.5));
   }
@@ -384,6 +394,34 @@ struct GroupIO {
   HD void st(int i, int col, cx<T> v) const {
     const int q = magic_div32(col, mnb), b = col - q * nb;
     if (q < gout) p[(size_t)q * nc + (size_t)i * plane + b] = v;
+  }
+};
+
+// z pass, forward: the last step stores element (kz = i, column b) of a
+// single-field group in shared memory, res[b + i*NB], already multiplied by
+// the group's real k-space factor (the same factors as zpass_operator):
+// Hartree 4 pi / |G|^2 (0 at G = 0), vW |G|^2, or the WT kernel plane, each
+// times the 1/N forward scale.
+template <typename T>
+struct ZOpStore {
+  cx<T>* res;
+  int NB, kind, kx0, ky, n3, plane;
+  T rt0, rt1, rt2, rt6, rt7, rt8, ty0, ty1, ty2, sc, c4;
+  const T* kern;  // plane at (ky, kx0)
+  HD void st(int i, int b, cx<T> v) const {
+    T m;
+    if (kind == G_KMUL) {
+      m = kern[i * plane + b] * sc;
+    } else {
+      const int m1 = kx0 + b;
+      const int m3 = i > n3 / 2 ? i - n3 : i;
+      const T tx = rt0 * (T)m1 + ty0 + rt6 * (T)m3;
+      const T ty = rt1 * (T)m1 + ty1 + rt7 * (T)m3;
+      const T tz = rt2 * (T)m1 + ty2 + rt8 * (T)m3;
+      const T g2 = tx * tx + ty * ty + tz * tz;
+      m = kind == G_VW ? g2 * sc : ((m1 == 0 && ky == 0 && i == 0) ? T(0) : c4 / g2);
+    }
+    res[b + i * NB] = v * m;
   }
 };
 
@@ -531,9 +569,29 @@ HD void zpass_block(const Args<T>& a, int bid, int tid, int nthr, char* smem) {
   if (fft2_supported<T>(s.pz)) {  // forward into tmp, operator, inverse back to the spectra
     const GroupIO<T> gio{spec, nb, plane, gin, gout, mnb, (long long)Nc};
     const SmemIO<T> o{tmp, NB};
-    fft2_run<T, -1>(gio, o, buf, NB, s.pz, a.tw, tid, nthr);
-    BLOCK_SYNC();
-    zpass_operator<T>(s, kind, gn, setup_mode, tmp, NB, nb, kx0, ky, tid, nthr);
+    if (!setup_mode && gn == 1 && (kind == G_HARTREE || kind == G_VW || kind == G_KMUL)) {
+      // single-field groups: the operator is applied as the forward transform stores
+      const int m2 = ky > n2 / 2 ? ky - n2 : ky;
+      ZOpStore<T> zo;
+      zo.res = tmp;
+      zo.NB = NB;
+      zo.kind = kind;
+      zo.kx0 = kx0;
+      zo.ky = ky;
+      zo.n3 = n3;
+      zo.plane = plane;
+      zo.rt0 = (T)s.recip[0]; zo.rt1 = (T)s.recip[1]; zo.rt2 = (T)s.recip[2];
+      zo.rt6 = (T)s.recip[6]; zo.rt7 = (T)s.recip[7]; zo.rt8 = (T)s.recip[8];
+      zo.ty0 = (T)s.recip[3] * (T)m2; zo.ty1 = (T)s.recip[4] * (T)m2; zo.ty2 = (T)s.recip[5] * (T)m2;
+      zo.sc = (T)s.inv_n;
+      zo.c4 = (T)(4.0 * PI_D * s.inv_n);
+      zo.kern = (const T*)s.kern + ky * k1 + kx0;
+      fft2_run<T, -1>(gio, zo, buf, NB, s.pz, a.tw, tid, nthr);
+    } else {
+      fft2_run<T, -1>(gio, o, buf, NB, s.pz, a.tw, tid, nthr);
+      BLOCK_SYNC();
+      zpass_operator<T>(s, kind, gn, setup_mode, tmp, NB, nb, kx0, ky, tid, nthr);
+    }
     BLOCK_SYNC();
     fft2_run<T, 1>(o, gio, buf, NB, s.pz, a.tw, tid, nthr);
     return;

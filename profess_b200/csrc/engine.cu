@@ -194,7 +194,11 @@ struct PlanTable {
 };
 
 // ------------------------------------------------------------ kernels
-enum Pass : int { P_VEC = 0, P_X1 = 1, P_Y2 = 2, P_Z3 = 3, P_Y4 = 4, P_X5 = 5, P_CTL = 6, NPASS = 7 };
+// Launch lists of one tick.  Passes 1, 3 and 5 have one list for the WT slots
+// (P_X1, P_Z3, P_X5) and one for the WGC slots (P_X1G, P_Z3G, P_X5G), each
+// launched with the kernel instantiated for that functional.
+enum Pass : int { P_VEC = 0, P_X1 = 1, P_Y2 = 2, P_Z3 = 3, P_Y4 = 4, P_X5 = 5, P_CTL = 6,
+                  P_X1G = 7, P_Z3G = 8, P_X5G = 9, NPASS = 10 };
 constexpr int VEC_PER_TICK = 2;
 constexpr int VCHUNK = 4096;
 
@@ -203,21 +207,21 @@ template <typename T> __global__ void __launch_bounds__(256) k_vec(Args<T> a) {
   extern __shared__ __align__(16) char sm[];
   vec_block<T>(a, blockIdx.x, threadIdx.x, blockDim.x, sm);
 }
-template <typename T> __global__ void __launch_bounds__(256, PassMinBlocks<T>::value) k_xfwd(Args<T> a) {
+template <typename T, int KS> __global__ void __launch_bounds__(256, PassMinBlocks<T>::value) k_xfwd(Args<T> a) {
   extern __shared__ __align__(16) char sm[];
-  xfwd_block<T>(a, blockIdx.x, threadIdx.x, blockDim.x, sm);
+  xfwd_block<T, KS>(a, blockIdx.x, threadIdx.x, blockDim.x, sm);
 }
 template <typename T> __global__ void __launch_bounds__(256, PassMinBlocks<T>::value) k_ypass(Args<T> a, int dir) {
   extern __shared__ __align__(16) char sm[];
   ypass_block<T>(a, blockIdx.x, threadIdx.x, blockDim.x, sm, dir);
 }
-template <typename T> __global__ void __launch_bounds__(256, PassMinBlocks<T>::value) k_zpass(Args<T> a) {
+template <typename T, int KS> __global__ void __launch_bounds__(256, PassMinBlocks<T>::value) k_zpass(Args<T> a) {
   extern __shared__ __align__(16) char sm[];
-  zpass_block<T>(a, blockIdx.x, threadIdx.x, blockDim.x, sm);
+  zpass_block<T, KS>(a, blockIdx.x, threadIdx.x, blockDim.x, sm);
 }
-template <typename T> __global__ void __launch_bounds__(256, PassMinBlocks<T>::value) k_xinv(Args<T> a) {
+template <typename T, int KS> __global__ void __launch_bounds__(256, PassMinBlocks<T>::value) k_xinv(Args<T> a) {
   extern __shared__ __align__(16) char sm[];
-  xinv_block<T>(a, blockIdx.x, threadIdx.x, blockDim.x, sm);
+  xinv_block<T, KS>(a, blockIdx.x, threadIdx.x, blockDim.x, sm);
 }
 template <typename T> __global__ void __launch_bounds__(256) k_fill_kernel(const SlotDev* sd, KernArgs ka, int kind) {
   const SlotDev& s = *sd;
@@ -1014,10 +1018,12 @@ struct Engine {
       for (int t = 0; t < s.ntask[K_VEC]; ++t) L[P_VEC].h.push_back({i, t, 0, 0});
       L[P_VEC].nthr = 256;
       L[P_VEC].smem = std::max(L[P_VEC].smem, (size_t)(NCH * 33 * sizeof(double) + 16));
+      const bool wgc = s.kinetic == KIN_WGC;
+      const int px1 = wgc ? P_X1G : P_X1, pz3 = wgc ? P_Z3G : P_Z3, px5 = wgc ? P_X5G : P_X5;
       for (int r = 0; r < h.nrowpairs; r += h.rp1)
-        L[P_X1].h.push_back({i, 0, r, std::min(h.rp1, h.nrowpairs - r)});
-      L[P_X1].nthr = 256;
-      L[P_X1].smem = std::max(L[P_X1].smem, 2 * (size_t)std::max(s.nf, s.ion.nspec) * h.rp1 * s.n1 * cs);
+        L[px1].h.push_back({i, 0, r, std::min(h.rp1, h.nrowpairs - r)});
+      L[px1].nthr = 256;
+      L[px1].smem = std::max(L[px1].smem, 2 * (size_t)std::max(s.nf, s.ion.nspec) * h.rp1 * s.n1 * cs);
       for (int pass : {P_Y2, P_Y4}) {
         for (int f = 0; f < s.nf; ++f)
           for (int z = 0; z < s.n3; ++z)
@@ -1028,16 +1034,17 @@ struct Engine {
       const int gmax = s.kinetic == KIN_WGC ? 3 : 1;
       for (int g = 0; g < s.ngroups; ++g)
         for (int ky = 0; ky < s.n2; ++ky)
-          for (int t = 0; t < tile_count(s.k1, h.tz); ++t) L[P_Z3].h.push_back({i, g, ky, tile_code(s.k1, h.tz, t)});
-      L[P_Z3].nthr = 256;
-      L[P_Z3].smem = std::max(L[P_Z3].smem, 2 * (size_t)std::max(gmax, s.ion.nspec) * h.tz * s.n3 * cs);
+          for (int t = 0; t < tile_count(s.k1, h.tz); ++t) L[pz3].h.push_back({i, g, ky, tile_code(s.k1, h.tz, t)});
+      L[pz3].nthr = 256;
+      L[pz3].smem = std::max(L[pz3].smem, 2 * (size_t)std::max(gmax, s.ion.nspec) * h.tz * s.n3 * cs);
       int ord = 0;
-      for (int r = 0; r < h.nrowpairs; r += s.rp) L[P_X5].h.push_back({i, r, std::min(s.rp, h.nrowpairs - r), ord++});
+      for (int r = 0; r < h.nrowpairs; r += s.rp) L[px5].h.push_back({i, r, std::min(s.rp, h.nrowpairs - r), ord++});
       L[P_CTL].h.push_back({i, 0, 0, 0});
       L[P_CTL].nthr = 64;
       L[P_CTL].smem = 0;
-      L[P_X5].nthr = 256;
-      L[P_X5].smem = std::max(L[P_X5].smem, 2 * (size_t)s.nf * s.rp * s.n1 * cs + NCH * 33 * sizeof(double) + 16);
+      L[px5].nthr = 256;
+      L[px5].smem = std::max(L[px5].smem, 2 * (size_t)std::max(s.nf, s.ion.nspec) * s.rp * s.n1 * cs +
+                                              NCH * 33 * sizeof(double) + 16);
     }
 #if defined(OFDFT_EMU)
     for (int p = 0; p < 2; ++p)
@@ -1089,11 +1096,14 @@ struct Engine {
       run(P_VEC, [](Args<T>& a, int b, char* sm) { vec_block<T>(a, b, 0, 1, sm); });
       run(P_CTL, [](Args<T>& a, int b, char*) { ctl_block(a.slots, a.ctl, a.tasks, K_VEC, b, 0, 1, (char*)ctl_sm); });
     }
-    run(P_X1, [](Args<T>& a, int b, char* sm) { xfwd_block<T>(a, b, 0, 1, sm); });
+    run(P_X1, [](Args<T>& a, int b, char* sm) { xfwd_block<T, KS_WT>(a, b, 0, 1, sm); });
+    run(P_X1G, [](Args<T>& a, int b, char* sm) { xfwd_block<T, KS_WGC>(a, b, 0, 1, sm); });
     run(P_Y2, [](Args<T>& a, int b, char* sm) { ypass_block<T>(a, b, 0, 1, sm, -1); });
-    run(P_Z3, [](Args<T>& a, int b, char* sm) { zpass_block<T>(a, b, 0, 1, sm); });
+    run(P_Z3, [](Args<T>& a, int b, char* sm) { zpass_block<T, KS_WT>(a, b, 0, 1, sm); });
+    run(P_Z3G, [](Args<T>& a, int b, char* sm) { zpass_block<T, KS_WGC>(a, b, 0, 1, sm); });
     run(P_Y4, [](Args<T>& a, int b, char* sm) { ypass_block<T>(a, b, 0, 1, sm, 1); });
-    run(P_X5, [](Args<T>& a, int b, char* sm) { xinv_block<T>(a, b, 0, 1, sm); });
+    run(P_X5, [](Args<T>& a, int b, char* sm) { xinv_block<T, KS_WT>(a, b, 0, 1, sm); });
+    run(P_X5G, [](Args<T>& a, int b, char* sm) { xinv_block<T, KS_WGC>(a, b, 0, 1, sm); });
     run(P_CTL, [](Args<T>& a, int b, char*) { ctl_block(a.slots, a.ctl, a.tasks, K_X5, b, 0, 1, (char*)ctl_sm); });
     return OFDFT_OK;
   }
@@ -1112,11 +1122,14 @@ struct Engine {
       if ((rc = launch_one<T>(prec, P_VEC, k_vec<T>))) return rc;
       if ((rc = launch_one<T>(prec, P_CTL, k_ctl<T>, (int)K_VEC))) return rc;
     }
-    if ((rc = launch_one<T>(prec, P_X1, k_xfwd<T>))) return rc;
+    if ((rc = launch_one<T>(prec, P_X1, k_xfwd<T, KS_WT>))) return rc;
+    if ((rc = launch_one<T>(prec, P_X1G, k_xfwd<T, KS_WGC>))) return rc;
     if ((rc = launch_one<T>(prec, P_Y2, k_ypass<T>, -1))) return rc;
-    if ((rc = launch_one<T>(prec, P_Z3, k_zpass<T>))) return rc;
+    if ((rc = launch_one<T>(prec, P_Z3, k_zpass<T, KS_WT>))) return rc;
+    if ((rc = launch_one<T>(prec, P_Z3G, k_zpass<T, KS_WGC>))) return rc;
     if ((rc = launch_one<T>(prec, P_Y4, k_ypass<T>, 1))) return rc;
-    if ((rc = launch_one<T>(prec, P_X5, k_xinv<T>))) return rc;
+    if ((rc = launch_one<T>(prec, P_X5, k_xinv<T, KS_WT>))) return rc;
+    if ((rc = launch_one<T>(prec, P_X5G, k_xinv<T, KS_WGC>))) return rc;
     return launch_one<T>(prec, P_CTL, k_ctl<T>, (int)K_X5);
   }
 #endif
@@ -1140,10 +1153,13 @@ struct Engine {
                         "cudaFuncSetAttribute");
     };
     if ((rc = attr(k_vec<T>, P_VEC))) return rc;
-    if ((rc = attr(k_xfwd<T>, P_X1))) return rc;
+    if ((rc = attr(k_xfwd<T, KS_WT>, P_X1))) return rc;
+    if ((rc = attr(k_xfwd<T, KS_WGC>, P_X1G))) return rc;
+    if ((rc = attr(k_zpass<T, KS_WGC>, P_Z3G))) return rc;
+    if ((rc = attr(k_xinv<T, KS_WGC>, P_X5G))) return rc;
     if ((rc = attr(k_ypass<T>, lists[prec][P_Y2].smem >= lists[prec][P_Y4].smem ? P_Y2 : P_Y4))) return rc;
-    if ((rc = attr(k_zpass<T>, P_Z3))) return rc;
-    return attr(k_xinv<T>, P_X5);
+    if ((rc = attr(k_zpass<T, KS_WT>, P_Z3))) return rc;
+    return attr(k_xinv<T, KS_WT>, P_X5);
   }
 
   // Capture `nticks` ticks into one CUDA graph (re-captured when the set of
@@ -1735,20 +1751,20 @@ extern "C" int ofdft_calculate_potential_plus_noalloc(const ofdft_cell_desc* d, 
     return cuda_check(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm),
                       "cudaFuncSetAttribute");
   };
-  if ((rc = attr(k_xfwd<double>, sm1)) || (rc = attr(k_ypass<double>, sm2)) || (rc = attr(k_zpass<double>, sm3)) ||
-      (rc = attr(k_xinv<double>, sm5)))
+  if ((rc = attr(k_xfwd<double, KS_WT>, sm1)) || (rc = attr(k_ypass<double>, sm2)) || (rc = attr(k_zpass<double, KS_WT>, sm3)) ||
+      (rc = attr(k_xinv<double, KS_WT>, sm5)))
     return rc;
   const Task* tb = (const Task*)(base + o_task);
   a.tasks = tb;
-  k_xfwd<double><<<nt[0], 256, sm1, st>>>(a);
+  k_xfwd<double, KS_WT><<<nt[0], 256, sm1, st>>>(a);
   a.tasks = tb + nt[0];
   k_ypass<double><<<nt[1], 256, sm2, st>>>(a, -1);
   a.tasks = tb + nt[0] + nt[1];
-  k_zpass<double><<<nt[2], 256, sm3, st>>>(a);
+  k_zpass<double, KS_WT><<<nt[2], 256, sm3, st>>>(a);
   a.tasks = tb + nt[0];
   k_ypass<double><<<nt[1], 256, sm2, st>>>(a, 1);
   a.tasks = tb + nt[0] + nt[1] + nt[2];
-  k_xinv<double><<<nt[3], 256, sm5, st>>>(a);
+  k_xinv<double, KS_WT><<<nt[3], 256, sm5, st>>>(a);
   a.tasks = tb + nt[0] + nt[1] + nt[2] + nt[3];
   k_ctl<double><<<1, 64, 0, st>>>(a, (int)K_X5);
   if ((rc = cuda_check(cudaGetLastError(), "kernel launch"))) return rc;

@@ -26,6 +26,12 @@ namespace ofdft {
 constexpr double PI_D = 3.141592653589793238462643;
 constexpr double C_TF = 2.87123400018819;  // Source/KEDF_TF.f90:42
 
+// Kernel instantiations per kinetic functional: the WT kernels carry at most
+// 4 fields and no WGC code, so their register allocation is not set by the
+// 8-field WGC paths.
+enum KinSel : int { KS_WT = 0, KS_WGC = 1 };
+template <int KS> struct KinFields { static constexpr int value = KS == KS_WT ? 4 : MAX_FIELDS; };
+
 template <typename T>
 struct Args {
   SlotDev* slots;
@@ -276,10 +282,10 @@ HD FieldPar<T> field_par(const SlotDev& s) {
 // alpha != beta, rho^alpha; WGC: rho, sqrt(rho), then for x = alpha and
 // x = beta: rho^x, theta rho^x, theta^2 rho^x / 2 with theta = rho - rho*),
 // with each power computed once.
-template <typename T>
+template <typename T, int KS>
 HD void field_values(const FieldPar<T>& fp, int nf, T rho, T sq, T* v) {
   v[0] = rho;
-  if (fp.wt) {
+  if constexpr (KS == KS_WT) {
     v[1] = fp.pow56 ? sq * m_cbrt(rho) : m_pow(rho, fp.beta);
     v[2] = sq;
     if (nf > 3) v[3] = m_pow(rho, fp.alpha);
@@ -299,8 +305,9 @@ HD void field_values(const FieldPar<T>& fp, int nf, T rho, T sq, T* v) {
 // Every field of a range of row pairs in one block: the inputs of a point are
 // read and its field values computed once, and the nf * nb x-transforms run
 // as one batch, column f*nb + b, element i at buf[(f*nb + b) + i*NB].
-template <typename T>
+template <typename T, int KS>
 HD void xfwd_block(const Args<T>& a, int bid, int tid, int nthr, char* smem) {
+  constexpr int NFM = KinFields<KS>::value;
   const Task t = a.tasks[bid];
   const SlotDev& s = a.slots[t.slot];
   const Ctl& c = a.ctl[t.slot];
@@ -330,20 +337,20 @@ HD void xfwd_block(const Args<T>& a, int bid, int tid, int nthr, char* smem) {
       }
       continue;
     }
-    T v0[MAX_FIELDS], v1[MAX_FIELDS];
+    T v0[NFM], v1[NFM];
     T phin, rho, sq;
     in.at(j0 * n1 + i, phin, rho, sq);
     if (ev == EV_FORCE) v0[0] = rho;
-    else field_values(fp, nfe, rho, sq, v0);
+    else field_values<T, KS>(fp, nfe, rho, sq, v0);
 #pragma unroll
-    for (int f = 0; f < MAX_FIELDS; ++f) v1[f] = T(0);
+    for (int f = 0; f < NFM; ++f) v1[f] = T(0);
     if (has1) {
       in.at(j1 * n1 + i, phin, rho, sq);
       if (ev == EV_FORCE) v1[0] = rho;
-      else field_values(fp, nfe, rho, sq, v1);
+      else field_values<T, KS>(fp, nfe, rho, sq, v1);
     }
 #pragma unroll
-    for (int f = 0; f < MAX_FIELDS; ++f)
+    for (int f = 0; f < NFM; ++f)
       if (f < nfe) d[f * nb] = mk<T>(v0[f], v1[f]);
   }
   BLOCK_SYNC();
@@ -462,7 +469,7 @@ HD void ypass_block(const Args<T>& a, int bid, int tid, int nthr, char* smem, in
 // The k-space operator of one z-pass tile: res holds the forward z
 // transforms of the group's gn fields, [kz][q*nb + b] (NB = gn*nb), for kx =
 // kx0 + b and ky; the results replace them in place.
-template <typename T>
+template <typename T, int KS>
 HD void zpass_operator(const SlotDev& s, int kind, int gn, bool setup_mode, cx<T>* res, int NB, int nb, int kx0,
                        int ky, int tid, int nthr) {
   const int n2 = s.n2, n3 = s.n3, k1 = s.k1, plane = n2 * k1, Nc = (int)s.Nc;
@@ -504,11 +511,13 @@ HD void zpass_operator(const SlotDev& s, int kind, int gn, bool setup_mode, cx<T
         e[0] = e[0] * (kern[kidx] * sc);
         break;
       case G_WGC3: {  // second-order WGC triple (KEDF_WGC.f90:219-236)
-        const T K1 = kern[kidx], K2 = kern[Nc + kidx], K3 = kern[2 * Nc + kidx], K4 = kern[3 * Nc + kidx];
-        const cx<T> F0 = e[0], F1 = e[nb], F2 = e[2 * nb];
-        e[0] = (F0 * K1 + F1 * K2 + F2 * K3) * sc;
-        e[nb] = (F0 * K2 + F1 * K4) * sc;
-        e[2 * nb] = F0 * (K3 * sc);
+        if constexpr (KS == KS_WGC) {
+          const T K1 = kern[kidx], K2 = kern[Nc + kidx], K3 = kern[2 * Nc + kidx], K4 = kern[3 * Nc + kidx];
+          const cx<T> F0 = e[0], F1 = e[nb], F2 = e[2 * nb];
+          e[0] = (F0 * K1 + F1 * K2 + F2 * K3) * sc;
+          e[nb] = (F0 * K2 + F1 * K4) * sc;
+          e[2 * nb] = F0 * (K3 * sc);
+        }
         break;
       }
       case G_ION: {  // conj(sum_s V_s(|G|) b1 b2 b3 S_s) N / vol, times the 1/N forward scale
@@ -543,7 +552,7 @@ HD void zpass_operator(const SlotDev& s, int kind, int gn, bool setup_mode, cx<T
 
 // All gn fields of a group are transformed as one batch of gn*nb sequences
 // laid out [kz][q*nb + b].
-template <typename T>
+template <typename T, int KS>
 HD void zpass_block(const Args<T>& a, int bid, int tid, int nthr, char* smem) {
   const Task t = a.tasks[bid];
   const SlotDev& s = a.slots[t.slot];
@@ -590,7 +599,7 @@ HD void zpass_block(const Args<T>& a, int bid, int tid, int nthr, char* smem) {
     } else {
       fft2_run<T, -1>(gio, o, buf, NB, s.pz, a.tw, tid, nthr);
       BLOCK_SYNC();
-      zpass_operator<T>(s, kind, gn, setup_mode, tmp, NB, nb, kx0, ky, tid, nthr);
+      zpass_operator<T, KS>(s, kind, gn, setup_mode, tmp, NB, nb, kx0, ky, tid, nthr);
     }
     BLOCK_SYNC();
     fft2_run<T, 1>(o, gio, buf, NB, s.pz, a.tw, tid, nthr);
@@ -604,7 +613,7 @@ HD void zpass_block(const Args<T>& a, int bid, int tid, int nthr, char* smem) {
   BLOCK_SYNC();
   cx<T>* res = fft_batch<T, -1>(buf, tmp, NB, NB, s.pz, a.tw, tid, nthr);
   cx<T>* oth = res == buf ? tmp : buf;
-  zpass_operator<T>(s, kind, gn, setup_mode, res, NB, nb, kx0, ky, tid, nthr);
+  zpass_operator<T, KS>(s, kind, gn, setup_mode, res, NB, nb, kx0, ky, tid, nthr);
   BLOCK_SYNC();
   const cx<T>* out = fft_batch<T, 1>(res, oth, NB, NB, s.pz, a.tw, tid, nthr);
   for (int w = tid; w < NB * n3; w += nthr) {
@@ -638,8 +647,9 @@ HD void lda_point(T rho, T r13, T rs, T& vxc, T& exc) {
 // All nf fields of a row-pair range are transformed as one batch of nf*nb
 // sequences laid out [i][f*nb + b]; then every point of the rows gets the
 // real-space epilogue.
-template <typename T>
+template <typename T, int KS>
 HD void xinv_block(const Args<T>& a, int bid, int tid, int nthr, char* smem) {
+  constexpr int NFM = KinFields<KS>::value;
   const Task t = a.tasks[bid];
   SlotDev& s = a.slots[t.slot];
   Ctl& c = a.ctl[t.slot];
@@ -764,9 +774,9 @@ HD void xinv_block(const Args<T>& a, int bid, int tid, int nthr, char* smem) {
       const int idx = idxs[u];
       const int half = rb[u] >> 30;
       const cx<T>* rv = res + (rb[u] & ((1 << 30) - 1));
-      T o[MAX_FIELDS];
+      T o[NFM];
 #pragma unroll
-      for (int f = 0; f < MAX_FIELDS; ++f) {
+      for (int f = 0; f < NFM; ++f) {
         if (f < nf) {
           const cx<T> z = rv[f * nb];
           o[f] = half == 0 ? z.x : z.y;
@@ -791,7 +801,7 @@ HD void xinv_block(const Args<T>& a, int bid, int tid, int nthr, char* smem) {
       T vxc, exc;
       lda_point(rho, r13, cC * x, vxc, exc);
       T vnl, enl, lap;
-      if (fp.wt) {
+      if constexpr (KS == KS_WT) {
         const T rbeta = fp.pow56 ? sq * r13 : m_pow(rho, be);
         const T ralpha = fp.aeqb ? rbeta : m_pow(rho, al);
         const T pa = nf > 3 ? o[3] : o[1];

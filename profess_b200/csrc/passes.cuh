@@ -58,15 +58,19 @@ HD double psp_value(const IonAux& x, int sp, double q) {
 }
 
 // ------------------------------------------------------------ reductions
-// Reduce acc[NCH] over the block; the block totals end up in sred[0..NCH-1].
-// On the device: warp shuffles, then one warp over the per-warp sums (sred
-// needs NCH * 33 doubles).  In the host emulation the block has one thread.
+// Reduce channels [LO, HI) of acc[NCH] over the block; the block totals end
+// up in sred[LO..HI-1] and the other channels of sred[0..NCH-1] are zero.  On
+// the device: warp shuffles, then one warp over the per-warp sums (sred needs
+// NCH * 33 doubles).  In the host emulation the block has one thread.  Passes
+// whose sums use few channels (a CG evaluation one, the vector operations
+// three) reduce only those.
+template <int LO = 0, int HI = NCH>
 HDNI inline void block_reduce(double* sred, const double* acc, int tid, int nthr) {
 #if defined(__CUDA_ARCH__)
   const int lane = tid & 31, warp = tid >> 5, nw = (nthr + 31) >> 5;
   double v[NCH];
 #pragma unroll
-  for (int ch = 0; ch < NCH; ++ch) {
+  for (int ch = LO; ch < HI; ++ch) {
     double x = acc[ch];
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) x += __shfl_down_sync(0xffffffffu, x, o);
@@ -74,12 +78,16 @@ HDNI inline void block_reduce(double* sred, const double* acc, int tid, int nthr
   }
   if (lane == 0) {
 #pragma unroll
-    for (int ch = 0; ch < NCH; ++ch) sred[NCH + ch * 32 + warp] = v[ch];
+    for (int ch = LO; ch < HI; ++ch) sred[NCH + ch * 32 + warp] = v[ch];
   }
   __syncthreads();
   if (warp == 0) {
 #pragma unroll
     for (int ch = 0; ch < NCH; ++ch) {
+      if (ch < LO || ch >= HI) {
+        if (lane == 0) sred[ch] = 0.0;
+        continue;
+      }
       double x = lane < nw ? sred[NCH + ch * 32 + lane] : 0.0;
 #pragma unroll
       for (int o = 16; o > 0; o >>= 1) x += __shfl_down_sync(0xffffffffu, x, o);
@@ -90,13 +98,15 @@ HDNI inline void block_reduce(double* sred, const double* acc, int tid, int nthr
 #else
   (void)tid;
   (void)nthr;
-  for (int ch = 0; ch < NCH; ++ch) sred[ch] = acc[ch];
+  for (int ch = 0; ch < NCH; ++ch) sred[ch] = (ch >= LO && ch < HI) ? acc[ch] : 0.0;
 #endif
 }
 
-// Store this task's per-channel sums in the slot's partials.
+// Store this task's per-channel sums (channels [LO, HI), the rest zero) in
+// the slot's partials.
+template <int LO = 0, int HI = NCH>
 HDNI inline void store_partials(SlotDev& s, int task_idx, const double* acc, double* sred, int tid, int nthr) {
-  block_reduce(sred, acc, tid, nthr);
+  block_reduce<LO, HI>(sred, acc, tid, nthr);
   if (tid == 0) {
 #pragma unroll
     for (int ch = 0; ch < NCH; ++ch) s.partials[(size_t)task_idx * NCH + ch] = sred[ch];
@@ -221,7 +231,7 @@ HD void vec_block(const Args<T>& a, int bid, int tid, int nthr, char* smem) {
     default:
       break;
   }
-  store_partials(s, t.a, acc, (double*)smem, tid, nthr);
+  store_partials<0, 3>(s, t.a, acc, (double*)smem, tid, nthr);  // vector ops use channels 0-2
 }
 
 // ------------------------------------------------------------ evaluation inputs
@@ -714,7 +724,7 @@ HD void xinv_block(const Args<T>& a, int bid, int tid, int nthr, char* smem) {
     double zero[NCH];
 #pragma unroll
     for (int ch = 0; ch < NCH; ++ch) zero[ch] = 0.0;
-    store_partials(s, ordinal, zero, (double*)(tmp + NB * n1), tid, nthr);
+    store_partials<0, 0>(s, ordinal, zero, (double*)(tmp + NB * n1), tid, nthr);
     return;
   }
 
@@ -861,7 +871,8 @@ HD void xinv_block(const Args<T>& a, int bid, int tid, int nthr, char* smem) {
       }
     }
   }
-  store_partials(s, ordinal, acc, (double*)(tmp + NB * n1), tid, nthr);
+  if (ev == EV_CG) store_partials<CH_M0, CH_M0 + 1>(s, ordinal, acc, (double*)(tmp + NB * n1), tid, nthr);
+  else store_partials(s, ordinal, acc, (double*)(tmp + NB * n1), tid, nthr);
 }
 
 }  // namespace ofdft

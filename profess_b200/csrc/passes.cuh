@@ -731,13 +731,10 @@ HD void xinv_block(const Args<T>& a, int bid, int tid, int nthr, char* smem) {
   const EvalIn<T> in = eval_in<T>(s, c);
   const FieldPar<T> fp = field_par<T>(s);
   const T* __restrict__ vion = (const T*)s.vion;
-  const T* __restrict__ phi = (const T*)s.buf[c.iphi];
   T* __restrict__ w0 = (T*)s.buf[c.iw0];
   T* __restrict__ w1 = (T*)s.buf[c.iw1];
   T* __restrict__ trial = (T*)s.buf[c.itrial];
   const T* __restrict__ bb = (const T*)s.buf[B_B];
-  const T* __restrict__ p = (const T*)s.buf[B_P];
-  const T* __restrict__ d = (const T*)s.buf[B_D];
   const bool energy = (ev != EV_CG) && (ev != EV_RHO || c.want_energy);
   const bool opt_sqrt = c.opt_sqrt != 0 || ev != EV_RHO;
   const T lam = (T)s.lambda, muv = (T)s.mu, al = fp.alpha, be = fp.beta, cTF = (T)C_TF;
@@ -770,12 +767,13 @@ HD void xinv_block(const Args<T>& a, int bid, int tid, int nthr, char* smem) {
       bx[u] = in.rho_mode ? T(0) : in.B[idx];
       ex[u] = T(0);
       ey[u] = T(0);
+      // the CG evaluation's second input is p, the line search's are phi and d
       if (ev == EV_CG) {
         ex[u] = bb[idx];
-        ey[u] = p[idx];
+        ey[u] = bx[u];
       } else if (ev == EV_LS) {
-        ex[u] = phi[idx];
-        ey[u] = d[idx];
+        ex[u] = aa[u];
+        ey[u] = bx[u];
       }
     }
 #pragma unroll

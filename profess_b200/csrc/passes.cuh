@@ -657,9 +657,160 @@ HD void lda_point(T rho, T r13, T rs, T& vxc, T& exc) {
 // All nf fields of a row-pair range are transformed as one batch of nf*nb
 // sequences laid out [i][f*nb + b]; then every point of the rows gets the
 // real-space epilogue.
+// Inputs of the real-space epilogue of pass 5 (one task).
+template <typename T>
+struct XinvEpi {
+  EvalIn<T> in;
+  FieldPar<T> fp;
+  const T* vion;
+  T* w0;
+  T* w1;
+  T* trial;
+  const T* bb;
+  const cx<T>* res;  // the c2r outputs, column f*nb + b, element i at res[i*NB + f*nb + b]
+  int NB, nb, nf, n1, nrows, rp0;
+  bool opt_sqrt;
+  T lam, muv, al, be, cTF, mu0, ieps, st, ctd, ctf53;
+};
+
+// The epilogue over every point of the task, compiled per evaluation mode EV
+// (ENERGY: the six energy channels are summed), so that each loop keeps only
+// its own inputs and FP64 accumulators live.  The sums go to acc_out[NCH].
+template <typename T, int KS, int EV, bool ENERGY>
+HD void xinv_points(const XinvEpi<T>& e, double* acc_out, int tid, int nthr) {
+  constexpr int NFM = KinFields<KS>::value;
+  constexpr bool RHO = EV == EV_RHO;  // the input is rho itself
+  const T* __restrict__ vion = e.vion;
+  const T* __restrict__ A = e.in.A;
+  const T* __restrict__ B = e.in.B;
+  const T* __restrict__ bb = e.bb;
+  T* __restrict__ w0 = e.w0;
+  T* __restrict__ w1 = e.w1;
+  T* __restrict__ trial = e.trial;
+  const FieldPar<T> fp = e.fp;
+  const int NB = e.NB, nb = e.nb, nf = e.nf, n1 = e.n1, nrows = e.nrows, rp0 = e.rp0;
+  const T cC = T(0.62035049089940009);
+  double acc[NCH];
+#pragma unroll
+  for (int ch = 0; ch < NCH; ++ch) acc[ch] = 0.0;
+  const unsigned m2n1 = magic32(2 * n1);
+  const int total = nb * 2 * n1;
+  for (int w0i = tid; w0i < total; w0i += 2 * nthr) {
+    // two points per iteration: all global loads of both are issued first
+    int idxs[2];
+    bool ok[2];
+    T vi[2], aa[2], bx[2], ex[2], ey[2];
+    int rb[2];
+#pragma unroll
+    for (int u = 0; u < 2; ++u) {
+      const int w = w0i + u * nthr;
+      const int b = magic_div32(w, m2n1), rem = w - b * 2 * n1;
+      const int half = rem >= n1 ? 1 : 0, i = rem - half * n1;
+      const int j = 2 * (rp0 + b) + half;
+      ok[u] = w < total && j < nrows;
+      const int idx = ok[u] ? j * n1 + i : 0;
+      idxs[u] = idx;
+      rb[u] = i * NB + b + (half << 30);
+      vi[u] = vion[idx];
+      aa[u] = A[idx];
+      bx[u] = RHO ? T(0) : B[idx];
+      // the CG evaluation's second input is p, the line search's are phi and d
+      ex[u] = EV == EV_CG ? bb[idx] : EV == EV_LS ? aa[u] : T(0);
+      ey[u] = (EV == EV_CG || EV == EV_LS) ? bx[u] : T(0);
+    }
+#pragma unroll
+    for (int u = 0; u < 2; ++u) {
+      if (!ok[u]) continue;
+      const int idx = idxs[u];
+      const int half = rb[u] >> 30;
+      const cx<T>* rv = e.res + (rb[u] & ((1 << 30) - 1));
+      T o[NFM];
+#pragma unroll
+      for (int f = 0; f < NFM; ++f) {
+        if (f < nf) {
+          const cx<T> z = rv[f * nb];
+          o[f] = half == 0 ? z.x : z.y;
+        } else {
+          o[f] = T(0);
+        }
+      }
+      T phin, rho, sq;
+      if (RHO) {
+        rho = aa[u];
+        sq = m_sqrt(rho);
+        phin = sq;
+      } else {
+        phin = e.in.ca * aa[u] + e.in.cb * bx[u];
+        rho = phin * phin;
+        sq = phin < T(0) ? -phin : phin;
+      }
+      const T x = m_rcbrt(rho);        // rho^(-1/3)
+      const T r13 = rho * x * x;       // rho^(1/3)
+      const T r23 = r13 * r13;
+      const T rinv = x * x * x;        // 1/rho
+      T vxc, exc;
+      lda_point(rho, r13, cC * x, vxc, exc);
+      T vnl, enl, lap;
+      const T al = e.al, be = e.be, cTF = e.cTF;
+      if constexpr (KS == KS_WT) {
+        const T rbeta = fp.pow56 ? sq * r13 : m_pow(rho, be);
+        const T ralpha = fp.aeqb ? rbeta : m_pow(rho, al);
+        const T pa = nf > 3 ? o[3] : o[1];
+        vnl = cTF * (al * (ralpha * rinv) * o[1] + be * (rbeta * rinv) * pa);
+        enl = cTF * ralpha * o[1];
+        lap = o[2];
+      } else {
+        const T th = rho - fp.rho_s;
+        const T ralpha = m_pow(rho, al);
+        const T rbeta = fp.sum53 ? rho * r23 / ralpha : m_pow(rho, be);
+        vnl = cTF * ((rbeta * rinv) * (be * o[2] + (rho + be * th) * o[3] + th * (rho + be * th * T(0.5)) * o[4]) +
+                     (ralpha * rinv) * (al * o[5] + (rho + al * th) * o[6] + th * (rho + al * th * T(0.5)) * o[7]));
+        enl = cTF * rbeta * (o[2] + th * o[3] + th * th * T(0.5) * o[4]);
+        lap = o[1];
+      }
+      const T potr = vi[u] + o[0] + vxc + e.ctf53 * r23 + vnl;
+      const T muv = e.muv;
+      const T pot = e.opt_sqrt ? T(2) * sq * potr + muv * lap : potr + muv * lap * (T(0.5) * sq * rinv);
+      if constexpr (ENERGY) {
+        acc[CH_EIE] += (double)rho * (double)vi[u];
+        acc[CH_EH] += 0.5 * (double)o[0] * (double)rho;
+        acc[CH_EXC] += (double)exc;
+        acc[CH_ETF] += (double)(e.lam * cTF) * (double)(rho * r23);
+        acc[CH_EVW] += 0.5 * (double)muv * (double)sq * (double)lap;
+        acc[CH_ENL] += (double)enl;
+      }
+      const T sg = phin < T(0) ? T(-1) : T(1);
+      if constexpr (EV == EV_RHO) {
+        w0[idx] = pot;
+      } else if constexpr (EV == EV_PHI) {
+        const T gg = pot * sg;
+        w0[idx] = gg;
+        acc[CH_M0] += (double)gg * (double)phin;
+        acc[CH_M1] += (double)phin * (double)phin;
+      } else if constexpr (EV == EV_CG) {
+        const T gg = pot * sg;
+        const T ap = ((gg - e.mu0 * T(2) * phin) - ex[u]) * e.ieps;
+        w1[idx] = ap;
+        acc[CH_M0] += (double)ey[u] * (double)ap;
+      } else {  // EV_LS
+        const T gg = pot * sg;
+        w1[idx] = gg;
+        trial[idx] = phin;
+        const T dir = -ex[u] * e.st + ey[u] * e.ctd;
+        const T dl = gg - T(2) * phin * e.mu0;
+        acc[CH_M0] += (double)gg * (double)dir;
+        acc[CH_M1] += (double)dl * (double)dl;
+        acc[CH_M2] += (double)gg * (double)phin;
+        acc[CH_M3] += (double)phin * (double)phin;
+      }
+    }
+  }
+#pragma unroll
+  for (int ch = 0; ch < NCH; ++ch) acc_out[ch] = acc[ch];
+}
+
 template <typename T, int KS>
 HD void xinv_block(const Args<T>& a, int bid, int tid, int nthr, char* smem) {
-  constexpr int NFM = KinFields<KS>::value;
   const Task t = a.tasks[bid];
   SlotDev& s = a.slots[t.slot];
   Ctl& c = a.ctl[t.slot];
@@ -728,146 +879,47 @@ HD void xinv_block(const Args<T>& a, int bid, int tid, int nthr, char* smem) {
     return;
   }
 
-  const EvalIn<T> in = eval_in<T>(s, c);
-  const FieldPar<T> fp = field_par<T>(s);
-  const T* __restrict__ vion = (const T*)s.vion;
-  T* __restrict__ w0 = (T*)s.buf[c.iw0];
-  T* __restrict__ w1 = (T*)s.buf[c.iw1];
-  T* __restrict__ trial = (T*)s.buf[c.itrial];
-  const T* __restrict__ bb = (const T*)s.buf[B_B];
-  const bool energy = (ev != EV_CG) && (ev != EV_RHO || c.want_energy);
-  const bool opt_sqrt = c.opt_sqrt != 0 || ev != EV_RHO;
-  const T lam = (T)s.lambda, muv = (T)s.mu, al = fp.alpha, be = fp.beta, cTF = (T)C_TF;
-  const T mu0 = (T)c.mu, ieps = (T)(ev == EV_CG ? 1.0 / c.eps : 0.0), st = (T)c.st, ctd = (T)(c.ct * c.dscale);
-  const T ctf53 = T(5) / T(3) * cTF * lam;
-  const T cC = T(0.62035049089940009);
+  XinvEpi<T> e;
+  e.in = eval_in<T>(s, c);
+  e.fp = field_par<T>(s);
+  e.vion = (const T*)s.vion;
+  e.w0 = (T*)s.buf[c.iw0];
+  e.w1 = (T*)s.buf[c.iw1];
+  e.trial = (T*)s.buf[c.itrial];
+  e.bb = (const T*)s.buf[B_B];
+  e.res = res;
+  e.NB = NB;
+  e.nb = nb;
+  e.nf = nf;
+  e.n1 = n1;
+  e.nrows = nrows;
+  e.rp0 = rp0;
+  e.opt_sqrt = c.opt_sqrt != 0 || ev != EV_RHO;
+  e.lam = (T)s.lambda;
+  e.muv = (T)s.mu;
+  e.al = e.fp.alpha;
+  e.be = e.fp.beta;
+  e.cTF = (T)C_TF;
+  e.mu0 = (T)c.mu;
+  e.ieps = (T)(ev == EV_CG ? 1.0 / c.eps : 0.0);
+  e.st = (T)c.st;
+  e.ctd = (T)(c.ct * c.dscale);
+  e.ctf53 = T(5) / T(3) * e.cTF * e.lam;
   double acc[NCH];
-#pragma unroll
-  for (int ch = 0; ch < NCH; ++ch) acc[ch] = 0.0;
-  const unsigned m2n1 = magic32(2 * n1);
-  const int total = nb * 2 * n1;
-  for (int w0i = tid; w0i < total; w0i += 2 * nthr) {
-    // two points per iteration: all global loads of both are issued first
-    int idxs[2];
-    bool ok[2];
-    T vi[2], aa[2], bx[2], ex[2], ey[2];
-    int rb[2];
-#pragma unroll
-    for (int u = 0; u < 2; ++u) {
-      const int w = w0i + u * nthr;
-      const int b = magic_div32(w, m2n1), rem = w - b * 2 * n1;
-      const int half = rem >= n1 ? 1 : 0, i = rem - half * n1;
-      const int j = 2 * (rp0 + b) + half;
-      ok[u] = w < total && j < nrows;
-      const int idx = ok[u] ? j * n1 + i : 0;
-      idxs[u] = idx;
-      rb[u] = i * NB + b + (half << 30);
-      vi[u] = vion[idx];
-      aa[u] = in.A[idx];
-      bx[u] = in.rho_mode ? T(0) : in.B[idx];
-      ex[u] = T(0);
-      ey[u] = T(0);
-      // the CG evaluation's second input is p, the line search's are phi and d
-      if (ev == EV_CG) {
-        ex[u] = bb[idx];
-        ey[u] = bx[u];
-      } else if (ev == EV_LS) {
-        ex[u] = aa[u];
-        ey[u] = bx[u];
-      }
-    }
-#pragma unroll
-    for (int u = 0; u < 2; ++u) {
-      if (!ok[u]) continue;
-      const int idx = idxs[u];
-      const int half = rb[u] >> 30;
-      const cx<T>* rv = res + (rb[u] & ((1 << 30) - 1));
-      T o[NFM];
-#pragma unroll
-      for (int f = 0; f < NFM; ++f) {
-        if (f < nf) {
-          const cx<T> z = rv[f * nb];
-          o[f] = half == 0 ? z.x : z.y;
-        } else {
-          o[f] = T(0);
-        }
-      }
-      T phin, rho, sq;
-      if (in.rho_mode) {
-        rho = aa[u];
-        sq = m_sqrt(rho);
-        phin = sq;
-      } else {
-        phin = in.ca * aa[u] + in.cb * bx[u];
-        rho = phin * phin;
-        sq = phin < T(0) ? -phin : phin;
-      }
-      const T x = m_rcbrt(rho);        // rho^(-1/3)
-      const T r13 = rho * x * x;       // rho^(1/3)
-      const T r23 = r13 * r13;
-      const T rinv = x * x * x;        // 1/rho
-      T vxc, exc;
-      lda_point(rho, r13, cC * x, vxc, exc);
-      T vnl, enl, lap;
-      if constexpr (KS == KS_WT) {
-        const T rbeta = fp.pow56 ? sq * r13 : m_pow(rho, be);
-        const T ralpha = fp.aeqb ? rbeta : m_pow(rho, al);
-        const T pa = nf > 3 ? o[3] : o[1];
-        vnl = cTF * (al * (ralpha * rinv) * o[1] + be * (rbeta * rinv) * pa);
-        enl = cTF * ralpha * o[1];
-        lap = o[2];
-      } else {
-        const T th = rho - fp.rho_s;
-        const T ralpha = m_pow(rho, al);
-        const T rbeta = fp.sum53 ? rho * r23 / ralpha : m_pow(rho, be);
-        vnl = cTF * ((rbeta * rinv) * (be * o[2] + (rho + be * th) * o[3] + th * (rho + be * th * T(0.5)) * o[4]) +
-                     (ralpha * rinv) * (al * o[5] + (rho + al * th) * o[6] + th * (rho + al * th * T(0.5)) * o[7]));
-        enl = cTF * rbeta * (o[2] + th * o[3] + th * th * T(0.5) * o[4]);
-        lap = o[1];
-      }
-      const T potr = vi[u] + o[0] + vxc + ctf53 * r23 + vnl;
-      const T pot = opt_sqrt ? T(2) * sq * potr + muv * lap : potr + muv * lap * (T(0.5) * sq * rinv);
-      if (energy) {
-        acc[CH_EIE] += (double)rho * (double)vi[u];
-        acc[CH_EH] += 0.5 * (double)o[0] * (double)rho;
-        acc[CH_EXC] += (double)exc;
-        acc[CH_ETF] += (double)(lam * cTF) * (double)(rho * r23);
-        acc[CH_EVW] += 0.5 * (double)muv * (double)sq * (double)lap;
-        acc[CH_ENL] += (double)enl;
-      }
-      const T sg = phin < T(0) ? T(-1) : T(1);
-      switch (ev) {
-        case EV_RHO:
-          w0[idx] = pot;
-          break;
-        case EV_PHI: {
-          const T gg = pot * sg;
-          w0[idx] = gg;
-          acc[CH_M0] += (double)gg * (double)phin;
-          acc[CH_M1] += (double)phin * (double)phin;
-          break;
-        }
-        case EV_CG: {
-          const T gg = pot * sg;
-          const T ap = ((gg - mu0 * T(2) * phin) - ex[u]) * ieps;
-          w1[idx] = ap;
-          acc[CH_M0] += (double)ey[u] * (double)ap;
-          break;
-        }
-        default: {  // EV_LS
-          const T gg = pot * sg;
-          w1[idx] = gg;
-          trial[idx] = phin;
-          const T dir = -ex[u] * st + ey[u] * ctd;
-          const T dl = gg - T(2) * phin * mu0;
-          acc[CH_M0] += (double)gg * (double)dir;
-          acc[CH_M1] += (double)dl * (double)dl;
-          acc[CH_M2] += (double)gg * (double)phin;
-          acc[CH_M3] += (double)phin * (double)phin;
-          break;
-        }
-      }
-    }
+  switch (ev) {
+    case EV_CG:
+      xinv_points<T, KS, EV_CG, false>(e, acc, tid, nthr);
+      break;
+    case EV_LS:
+      xinv_points<T, KS, EV_LS, true>(e, acc, tid, nthr);
+      break;
+    case EV_PHI:
+      xinv_points<T, KS, EV_PHI, true>(e, acc, tid, nthr);
+      break;
+    default:
+      if (c.want_energy) xinv_points<T, KS, EV_RHO, true>(e, acc, tid, nthr);
+      else xinv_points<T, KS, EV_RHO, false>(e, acc, tid, nthr);
+      break;
   }
   if (ev == EV_CG) store_partials<CH_M0, CH_M0 + 1>(s, ordinal, acc, (double*)(tmp + NB * n1), tid, nthr);
   else store_partials(s, ordinal, acc, (double*)(tmp + NB * n1), tid, nthr);

@@ -506,6 +506,10 @@ struct Engine {
     };
     h.ty = width(2 * (size_t)s.n2 * csz);
     h.tz = width(2 * (size_t)gmax * s.n3 * csz);
+    // two-step lengths: at most 256 / R2 columns, so that the first step's
+    // work items (columns x R2) fit the 256 threads of a block in one round
+    if (fft2_r2(s.n2) > 0) h.ty = std::max(1, std::min(h.ty, 256 / fft2_r2(s.n2)));
+    if (fft2_r2(s.n3) > 0) h.tz = std::max(1, std::min(h.tz, 256 / (gmax * fft2_r2(s.n3))));
     s.tx = h.ty;
     s.ntask[K_VEC] = (int)((s.N + VCHUNK - 1) / VCHUNK);
     s.ntask[K_X5] = (h.nrowpairs + s.rp - 1) / s.rp;

@@ -552,6 +552,19 @@ template <> struct Fft2MaxRadix<double> { static constexpr int value = 12; };
   X(240, 15, 16)            \
   X(256, 16, 16)
 
+// Second-step radix R2 of the two-step transform of length n (0: none).
+HD int fft2_r2(int n) {
+  switch (n) {
+#define OFDFT_FFT2_R2(N, A, B) \
+  case N:                      \
+    return B;
+    OFDFT_FFT2_SIZES(OFDFT_FFT2_R2)
+#undef OFDFT_FFT2_R2
+    default:
+      return 0;
+  }
+}
+
 // Whether length n has a two-step transform in precision T.
 template <typename T>
 HD bool fft2_supported(const FftPlan& p) {

@@ -146,6 +146,36 @@ HDNI inline void ctl_block(SlotDev* slots, Ctl* ctls, const Task* tasks, int kid
 }
 
 // ------------------------------------------------------------ vector ops
+// 16-byte packs (4 floats or 2 doubles): the vector operations stream their
+// arrays with one 16-byte load or store per pack and array.
+template <typename T> struct Pack { static constexpr int n = 16 / (int)sizeof(T); };
+template <typename T>
+HD void ld_pack(T* v, const T* p) {
+#if defined(__CUDA_ARCH__)
+  if constexpr (sizeof(T) == 4) {
+    const float4 x = *(const float4*)p;
+    v[0] = x.x; v[1] = x.y; v[2] = x.z; v[3] = x.w;
+  } else {
+    const double2 x = *(const double2*)p;
+    v[0] = x.x; v[1] = x.y;
+  }
+#else
+  for (int l = 0; l < Pack<T>::n; ++l) v[l] = p[l];
+#endif
+}
+template <typename T>
+HD void st_pack(T* p, const T* v) {
+#if defined(__CUDA_ARCH__)
+  if constexpr (sizeof(T) == 4) *(float4*)p = make_float4(v[0], v[1], v[2], v[3]);
+  else *(double2*)p = make_double2(v[0], v[1]);
+#else
+  for (int l = 0; l < Pack<T>::n; ++l) p[l] = v[l];
+#endif
+}
+
+// One task of a vector operation over points [i0, i1) of a slot: packs of
+// Pack<T>::n points first (i0 is a multiple of the chunk size, so packs are
+// 16-byte aligned), then the points after the last full pack one at a time.
 template <typename T>
 HD void vec_block(const Args<T>& a, int bid, int tid, int nthr, char* smem) {
   const Task t = a.tasks[bid];
@@ -164,19 +194,51 @@ HD void vec_block(const Args<T>& a, int bid, int tid, int nthr, char* smem) {
   const int i0 = t.a * a.vchunk;
   const int n = (int)s.N;
   const int i1 = i0 + a.vchunk < n ? i0 + a.vchunk : n;
+  constexpr int VP = Pack<T>::n;
+  const int npk = (i1 - i0) / VP;  // full packs
+  const int it = i0 + npk * VP;    // first point after them
   double acc[NCH];
 #pragma unroll
   for (int ch = 0; ch < NCH; ++ch) acc[ch] = 0.0;
   switch (op) {
     case OP_SQRT_INIT:
-      for (int i = i0 + tid; i < i1; i += nthr) {
+      for (int q = tid; q < npk; q += nthr) {
+        const int i = i0 + q * VP;
+        T v[VP];
+        ld_pack(v, phi + i);
+#pragma unroll
+        for (int l = 0; l < VP; ++l) {
+          acc[0] += (double)v[l];
+          v[l] = m_sqrt(v[l] < T(0) ? -v[l] : v[l]);
+        }
+        st_pack(phi + i, v);
+      }
+      for (int i = it + tid; i < i1; i += nthr) {
         const T rho = phi[i];
         acc[0] += (double)rho;
         phi[i] = m_sqrt(rho < T(0) ? -rho : rho);
       }
       break;
     case OP_DLDPHI:
-      for (int i = i0 + tid; i < i1; i += nthr) {
+      for (int q = tid; q < npk; q += nthr) {
+        const int i = i0 + q * VP;
+        T wv[VP], fv[VP], bv[VP], rv[VP], zv[VP];
+        ld_pack(wv, w0 + i);
+        ld_pack(fv, phi + i);
+#pragma unroll
+        for (int l = 0; l < VP; ++l) {
+          const T v = wv[l] - k * T(2) * fv[l];
+          bv[l] = v;
+          rv[l] = -v;
+          zv[l] = T(0);
+          acc[0] += (double)v * (double)v;
+        }
+        st_pack(bb + i, bv);
+        st_pack(r + i, rv);
+        st_pack(p + i, rv);
+        st_pack(d + i, zv);
+      }
+      for (int i = it + tid; i < i1; i += nthr) {
         const T v = w0[i] - k * T(2) * phi[i];
         bb[i] = v;
         r[i] = -v;
@@ -186,7 +248,29 @@ HD void vec_block(const Args<T>& a, int bid, int tid, int nthr, char* smem) {
       }
       break;
     case OP_CGSTEP:
-      for (int i = i0 + tid; i < i1; i += nthr) {
+      for (int q = tid; q < npk; q += nthr) {
+        const int i = i0 + q * VP;
+        T dv[VP], pv[VP], rv[VP], wv[VP], fv[VP];
+        ld_pack(dv, d + i);
+        ld_pack(pv, p + i);
+        ld_pack(rv, r + i);
+        ld_pack(wv, w1 + i);
+        ld_pack(fv, phi + i);
+#pragma unroll
+        for (int l = 0; l < VP; ++l) {
+          const T dn = dv[l] + k * pv[l];
+          const T rn = rv[l] - k * wv[l];
+          dv[l] = dn;
+          rv[l] = rn;
+          const T pd = fv[l] + dn;
+          acc[0] += (double)rn * (double)rn;
+          acc[1] += (double)pd * (double)pd;
+          acc[2] += (double)fv[l] * (double)dn;
+        }
+        st_pack(d + i, dv);
+        st_pack(r + i, rv);
+      }
+      for (int i = it + tid; i < i1; i += nthr) {
         const T dn = d[i] + k * p[i];
         const T rn = r[i] - k * w1[i];
         d[i] = dn;
@@ -199,7 +283,19 @@ HD void vec_block(const Args<T>& a, int bid, int tid, int nthr, char* smem) {
       }
       break;
     case OP_PUPD:
-      for (int i = i0 + tid; i < i1; i += nthr) {
+      for (int q = tid; q < npk; q += nthr) {
+        const int i = i0 + q * VP;
+        T rv[VP], pv[VP];
+        ld_pack(rv, r + i);
+        ld_pack(pv, p + i);
+#pragma unroll
+        for (int l = 0; l < VP; ++l) {
+          pv[l] = rv[l] + k * pv[l];
+          acc[0] += (double)pv[l] * (double)pv[l];
+        }
+        st_pack(p + i, pv);
+      }
+      for (int i = it + tid; i < i1; i += nthr) {
         const T pn = r[i] + k * p[i];
         p[i] = pn;
         acc[0] += (double)pn * (double)pn;
@@ -208,7 +304,32 @@ HD void vec_block(const Args<T>& a, int bid, int tid, int nthr, char* smem) {
     case OP_DIRNEG:
     case OP_NG1:
     case OP_SD:
-      for (int i = i0 + tid; i < i1; i += nthr) {
+      for (int q = tid; q < npk; q += nthr) {
+        const int i = i0 + q * VP;
+        T dv[VP], fv[VP], xv[VP];
+        if (op == OP_DIRNEG) {
+          ld_pack(dv, d + i);
+          ld_pack(xv, p + i);
+        } else if (op == OP_SD) {
+          ld_pack(xv, bb + i);
+        } else {
+          ld_pack(dv, d + i);
+        }
+        ld_pack(fv, phi + i);
+#pragma unroll
+        for (int l = 0; l < VP; ++l) {
+          T dn;
+          if (op == OP_DIRNEG) dn = -(dv[l] - k * xv[l]);
+          else if (op == OP_SD) dn = -xv[l];
+          else dn = dv[l];
+          dv[l] = dn;
+          const T pd = fv[l] + dn;
+          acc[1] += (double)pd * (double)pd;
+          acc[2] += (double)fv[l] * (double)dn;
+        }
+        if (op != OP_NG1) st_pack(d + i, dv);
+      }
+      for (int i = it + tid; i < i1; i += nthr) {
         T dn;
         if (op == OP_DIRNEG) dn = -(d[i] - k * p[i]);
         else if (op == OP_SD) dn = -bb[i];
@@ -221,7 +342,22 @@ HD void vec_block(const Args<T>& a, int bid, int tid, int nthr, char* smem) {
       }
       break;
     case OP_NG2:
-      for (int i = i0 + tid; i < i1; i += nthr) {
+      for (int q = tid; q < npk; q += nthr) {
+        const int i = i0 + q * VP;
+        T dv[VP], fv[VP], wv[VP];
+        ld_pack(dv, d + i);
+        ld_pack(fv, phi + i);
+        ld_pack(wv, w0 + i);
+#pragma unroll
+        for (int l = 0; l < VP; ++l) {
+          const T dn = dv[l] - fv[l] * k;
+          dv[l] = dn;
+          acc[0] += (double)dn * (double)dn;
+          acc[1] += (double)wv[l] * (double)dn;
+        }
+        st_pack(d + i, dv);
+      }
+      for (int i = it + tid; i < i1; i += nthr) {
         const T dn = d[i] - phi[i] * k;
         d[i] = dn;
         acc[0] += (double)dn * (double)dn;

@@ -741,12 +741,15 @@ HD void zpass_block(const Args<T>& a, int bid, int tid, int nthr, char* smem) {
       zo.sc = (T)s.inv_n;
       zo.c4 = (T)(4.0 * PI_D * s.inv_n);
       zo.kern = (const T*)s.kern + ky * k1 + kx0;
-      fft2_run<T, -1>(gio, zo, buf, NB, s.pz, a.tw, tid, nthr);
-    } else {
-      fft2_run<T, -1>(gio, o, buf, NB, s.pz, a.tw, tid, nthr);
+      const ColIO<T> col{spec, plane};  // one field: column b at spec[i*plane + b]
+      fft2_run<T, -1>(col, zo, buf, NB, s.pz, a.tw, tid, nthr);
       BLOCK_SYNC();
-      zpass_operator<T, KS>(s, kind, gn, setup_mode, tmp, NB, nb, kx0, ky, tid, nthr);
+      fft2_run<T, 1>(o, col, buf, NB, s.pz, a.tw, tid, nthr);
+      return;
     }
+    fft2_run<T, -1>(gio, o, buf, NB, s.pz, a.tw, tid, nthr);
+    BLOCK_SYNC();
+    zpass_operator<T, KS>(s, kind, gn, setup_mode, tmp, NB, nb, kx0, ky, tid, nthr);
     BLOCK_SYNC();
     fft2_run<T, 1>(o, gio, buf, NB, s.pz, a.tw, tid, nthr);
     return;

@@ -7,7 +7,7 @@ supercell, 256 atoms, a = 4.05 A, seeded Gaussian displacements sigma =
 WT + TF + vW + LDA, 96^3 grid.  One "step" is a batch of B such cells (distinct
 seeds) each solved to convergence by the sqrt-density truncated-Newton method:
 FP32 evaluations until the line search reaches the FP32 precision floor (or
-|dL/dphi| < 1e-5), then FP64 refinement iterations (mixed precision).  The plain FP64 GPU path (FP64 throughout, to
+|dL/dphi| < 3e-5), then FP64 refinement iterations (mixed precision).  The plain FP64 GPU path (FP64 throughout, to
 |dL/dphi| < 1e-6) is timed on the same cells for comparison, and the mixed
 energies are checked against it (eV/atom).
 
@@ -459,7 +459,10 @@ def main():
     ap.add_argument("--workload", default="cfg2", choices=["cfg2", "cfg1", "cfg3", "cfg4", "serving"])
     ap.add_argument("--requests", type=int, default=48, help="serving: number of requests")
     ap.add_argument("--max-active", type=int, default=24, help="serving: concurrent requests")
-    ap.add_argument("--fp32-tol", type=float, default=1.0e-5)
+    # FP32 phase tolerance of the mixed solve: 3e-5 gave the same worst energy
+    # error as 1e-5 on every workload (the two FP64 iterations set it) with
+    # ~15 % fewer FP32 evaluations
+    ap.add_argument("--fp32-tol", type=float, default=3.0e-5)
     ap.add_argument("--refine", type=int, default=2)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     args = ap.parse_args()

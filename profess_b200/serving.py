@@ -35,7 +35,7 @@ class Request:
     cell: Cell
     arrival: float = 0.0          # seconds after the server's start
     mode: str = MODE_MIXED
-    fp32_tol: float = 1.0e-5
+    fp32_tol: float = 3.0e-5
     refine_iters: int = 2
     pot_tol: float = 1.0e-6
     seed: int = 0

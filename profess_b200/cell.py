@@ -18,6 +18,17 @@ def ion_ion_energy(lib, cell: Cell) -> float:
     return e
 
 
+_WGC_TABLES = {}
+
+
+def wgc_tables(lib, alpha: float, beta: float, gamma: float):
+    """Radial WGC kernel tables, integrated once per (alpha, beta, gamma) and kept."""
+    key = (float(alpha), float(beta), float(gamma))
+    if key not in _WGC_TABLES:
+        _WGC_TABLES[key] = native.wgc_radial_tables(lib, *key)
+    return _WGC_TABLES[key]
+
+
 def setup_slot(eng: native.Engine, cell: Cell, precision=native.FP64, ion_ion=None) -> int:
     """Create a slot for ``cell`` and build its kernel and ion potential on the device."""
     rho_avg = cell.num_electrons / cell.vol
@@ -29,7 +40,7 @@ def setup_slot(eng: native.Engine, cell: Cell, precision=native.FP64, ion_ion=No
         if cell.kinetic == native.KEDF_WT:
             eng.build_wt_kernel(s)
         else:
-            eng.build_wgc_kernel(s)
+            eng.build_wgc_kernel(s, wgc_tables(eng.lib, cell.alpha, cell.beta, cell.gamma))
         eng.build_ion_potential(s, cell.frac, cell.species_of_ion, cell.species)
     except Exception:
         eng.slot_destroy(s)

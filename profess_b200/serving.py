@@ -4,6 +4,9 @@ Requests (a cell plus solve options) arrive over time; the server admits a
 waiting request when its device footprint fits the HBM budget and engine
 slots are free, builds its tables on the device, and starts its solve in the
 engine, where it shares every kernel launch with the solves already running.
+The host-side inputs of a request (its Ewald energy and initial density) are
+prepared by a small thread pool as soon as it arrives, so the engine keeps
+running the admitted solves meanwhile.
 A mixed-precision request runs an FP32 slot until the FP32 line-search floor
 (or the FP32 tolerance), then FP64 refinement iterations in an FP64 slot
 started from the FP32 density on the device; a plain request runs FP64
@@ -16,6 +19,7 @@ request ids to ranks with no exchange on the data path.
 """
 from __future__ import annotations
 
+import concurrent.futures
 import dataclasses
 import time
 
@@ -84,6 +88,8 @@ class Server:
         self.active = {}             # rid -> dict(state)
         self.used = 0
         self.results = []
+        self.pool = concurrent.futures.ThreadPoolExecutor(max_workers=2)
+        self.prep = {}               # rid -> future of (ion-ion energy, initial density)
 
     def now(self) -> float:
         return self.clock() - self.t0
@@ -93,10 +99,16 @@ class Server:
         self.future.sort(key=lambda r: r.arrival)
 
     # ------------------------------------------------------------ admission
+    @staticmethod
+    def _prepare(lib, req: Request):
+        return ion_ion_energy(lib, req.cell), initial_density(req.cell, seed=req.seed)
+
     def _arrivals(self):
         t = self.now()
         while self.future and self.future[0].arrival <= t:
-            self.waiting.append(self.future.pop(0))
+            req = self.future.pop(0)
+            self.waiting.append(req)
+            self.prep[req.rid] = self.pool.submit(self._prepare, self.eng.lib, req)
 
     def _admit(self):
         while self.waiting and len(self.active) < self.max_active:
@@ -106,10 +118,13 @@ class Server:
                 raise ValueError("request %d needs %d bytes, more than the whole budget" % (req.rid, need))
             if self.used + need > self.budget:
                 return
+            fut = self.prep[req.rid]
+            if not fut.done() and self.active:
+                return  # its inputs are still being prepared; keep serving the others
             self.waiting.pop(0)
             t_adm = self.now()
-            e_ii = ion_ion_energy(self.eng.lib, req.cell)
-            rho0 = initial_density(req.cell, seed=req.seed)
+            e_ii, rho0 = fut.result()
+            del self.prep[req.rid]
             st = {"req": req, "need": need, "admitted": t_adm, "phase": None, "s32": None, "s64": None}
             if req.mode == MODE_FP64:
                 st["s64"] = setup_slot(self.eng, req.cell, native.FP64, ion_ion=e_ii)
@@ -157,12 +172,16 @@ class Server:
             self._admit()
 
     def run_until_done(self, timeout: float = 3600.0):
-        while self.future or self.waiting or self.active:
-            if self.now() > timeout:
-                raise TimeoutError("serving did not finish")
-            if not self.active and not self.waiting and self.future:
-                time.sleep(max(0.0, min(0.01, self.future[0].arrival - self.now())))
-            self.step()
+        try:
+            while self.future or self.waiting or self.active:
+                if self.now() > timeout:
+                    raise TimeoutError("serving did not finish")
+                if not self.active and not self.waiting and self.future:
+                    time.sleep(max(0.0, min(0.01, self.future[0].arrival - self.now())))
+                self.step()
+        finally:
+            self.pool.shutdown(wait=True)
+            self.pool = concurrent.futures.ThreadPoolExecutor(max_workers=2)
         return self.results
 
 

@@ -189,6 +189,11 @@ int ofdft_slot_start_solve(ofdft_engine* e, int slot, const double* rho, const o
  * engine (e.g. an FP32 slot's result refined in an FP64 slot); no host copy. */
 int ofdft_slot_start_solve_from_slot(ofdft_engine* e, int slot, int src_slot, const ofdft_ntn_options* opts);
 int ofdft_slot_start_eval(ofdft_engine* e, int slot, const double* rho, int opt_sqrt, int want_energy);
+/* Stop a running solve or evaluation (no counterpart in the reference): the
+ * slot goes idle and keeps its buffers; a server drops a request with it.  The
+ * blocking calls above do this themselves when they run out of ticks
+ * (OFDFT_ETIMEOUT). */
+int ofdft_slot_cancel(ofdft_engine* e, int slot);
 /* Run up to `ticks` engine ticks over every running slot; *running receives the
  * number of slots still running afterwards. */
 int ofdft_engine_run(ofdft_engine* e, int ticks, int* running);

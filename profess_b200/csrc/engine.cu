@@ -702,6 +702,20 @@ struct Engine {
     return run_one(i);
   }
 
+  // Stop a running slot: its controller goes idle and it leaves the task lists.
+  int cancel(int i) {
+    if (i < 0 || i >= cap || !slots[i].used) return fail(OFDFT_EINVAL, "invalid slot");
+    if (!slots[i].running) return OFDFT_OK;
+    Ctl c;
+    int rc = get_ctl(i, c);
+    if (rc) return rc;
+    c.status = ST_IDLE;
+    if ((rc = put_ctl(i, c))) return rc;
+    slots[i].running = false;
+    dirty = true;
+    return OFDFT_OK;
+  }
+
   // Run a slot that needs a single evaluation tick.
   int run_one(int i) {
     slots[i].running = true;
@@ -1443,7 +1457,10 @@ int ofdft_calculate_potential_plus(ofdft_engine* e, int slot, const double* rho,
   if (rc) return rc;
   int running = 1;
   if ((rc = g.run(8, &running, 1))) return rc;
-  if (g.slots[slot].running) return fail(OFDFT_ETIMEOUT, "evaluation did not finish");
+  if (g.slots[slot].running) {
+    g.cancel(slot);
+    return fail(OFDFT_ETIMEOUT, "evaluation did not finish");
+  }
   Ctl c;
   if ((rc = g.get_ctl(slot, c))) return rc;
   if ((rc = status_code(c))) return rc;
@@ -1463,8 +1480,16 @@ int ofdft_proj_norm_rho_minimization(ofdft_engine* e, int slot, double* rho, dou
   const int max_ticks = (o && o->max_ticks > 0) ? o->max_ticks : 20000;
   int running = 1;
   if ((rc = g.run(max_ticks, &running, 8))) return rc;
-  if (g.slots[slot].running) return fail(OFDFT_ETIMEOUT, "solve exceeded the tick budget");
+  if (g.slots[slot].running) {
+    g.cancel(slot);  // the slot is idle again and can take a new solve
+    return fail(OFDFT_ETIMEOUT, "solve exceeded the tick budget");
+  }
   return ofdft_slot_result(e, slot, rho, energy, st);
+}
+
+int ofdft_slot_cancel(ofdft_engine* e, int slot) {
+  if (!e) return fail(OFDFT_EINVAL, "null engine");
+  return e->eng.cancel(slot);
 }
 
 int ofdft_slot_start_solve_from_slot(ofdft_engine* e, int slot, int src_slot, const ofdft_ntn_options* o) {

@@ -85,6 +85,7 @@ SIGNATURES = {
     "ofdft_slot_start_eval": [_vp, ctypes.c_int, _dp, ctypes.c_int, ctypes.c_int],
     "ofdft_engine_run": [_vp, ctypes.c_int, _ip],
     "ofdft_slot_poll": [_vp, ctypes.c_int, _ip],
+    "ofdft_slot_cancel": [_vp, ctypes.c_int],
     "ofdft_slot_result": [_vp, ctypes.c_int, _dp, _dp, ctypes.POINTER(NtnStats)],
     "ofdft_slot_history": [_vp, ctypes.c_int, ctypes.c_int, _dp, _dp, _dp, _ip, _ip, _ip],
     "ofdft_slot_download": [_vp, ctypes.c_int, ctypes.c_int, _dp],
@@ -340,6 +341,10 @@ class Engine:
         n = ctypes.c_int()
         self._check(self.lib.ofdft_engine_run(self.h, int(ticks), ctypes.byref(n)))
         return n.value
+
+    def cancel(self, slot):
+        """Stop the slot's running solve or evaluation; the slot goes idle."""
+        self._check(self.lib.ofdft_slot_cancel(self.h, slot))
 
     def poll(self, slot) -> bool:
         f = ctypes.c_int()

@@ -209,3 +209,54 @@ def test_invalid_slot_arguments(emu_engine):
             emu_engine.set_kernel(s, np.zeros((4,) + f.kernel.shape[1:]))  # WT takes one plane
     finally:
         emu_engine.slot_destroy(s)
+
+
+def test_tick_budget_timeout_leaves_the_slot_usable(emu_engine):
+    """A blocking solve that runs out of ticks returns OFDFT_ETIMEOUT and stops
+    the slot, which then solves normally."""
+    cell, f, rho_u, _ = cases.golden_case("wt_al4_displaced")
+    s = cases.engine_slot(emu_engine, f, cell)
+    try:
+        with pytest.raises(native.OfdftError) as ei:
+            emu_engine.proj_norm_rho_minimization(s, rho_u, native.ntn_options(max_ticks=3))
+        assert ei.value.code == 8
+        assert emu_engine.poll(s)
+        r_o = ntn.NtnSolver(f).solve(rho_u)
+        _, e_g, st = emu_engine.proj_norm_rho_minimization(s, rho_u)
+        assert st["num_evals"] == r_o.num_evals and abs(e_g[0] - r_o.energy[0]) < 1e-9
+    finally:
+        emu_engine.slot_destroy(s)
+
+
+def test_cancel_a_running_solve(emu_engine):
+    cell, f, rho_u, _ = cases.golden_case("wt_al4_displaced")
+    s = cases.engine_slot(emu_engine, f, cell)
+    try:
+        emu_engine.start_solve(s, rho_u)
+        emu_engine.run(2)
+        assert not emu_engine.poll(s)
+        emu_engine.cancel(s)
+        assert emu_engine.poll(s)
+        assert emu_engine.run(4) == 0  # nothing left running
+    finally:
+        emu_engine.slot_destroy(s)
+
+
+def test_engine_slot_capacity():
+    """The 257th slot of an engine is refused with OFDFT_ENOMEM; freed slots are reused."""
+    from profess_b200 import build
+    eng = native.Engine(build.build_emu())  # an engine of its own: it fills every slot
+    cell, _, _, _ = cases.golden_case("wt_al4_displaced")
+    slots = []
+    try:
+        for _ in range(256):
+            slots.append(eng.slot_create((2, 3, 5), cell.lattice))
+        with pytest.raises(native.OfdftError) as ei:
+            eng.slot_create((2, 3, 5), cell.lattice)
+        assert ei.value.code == 3
+        eng.slot_destroy(slots.pop())
+        slots.append(eng.slot_create((2, 3, 5), cell.lattice))
+    finally:
+        for s in slots:
+            eng.slot_destroy(s)
+        eng.close()

@@ -164,3 +164,49 @@ def test_serving_results_same_alone_and_in_the_mix(gpu_engine):
     for r in reqs:
         a = run([r])[r.rid]
         assert np.array_equal(a.energy, mix[r.rid].energy)
+
+
+@pytest.mark.parametrize("n,kinetic,prec", [((512, 6, 4), fn.KEDF_WT, native.FP64),
+                                             ((4, 512, 6), fn.KEDF_WGC, native.FP64),
+                                             ((6, 4, 512), fn.KEDF_WGC, native.FP64),
+                                             ((8, 6, 512), fn.KEDF_WT, native.FP32)])
+def test_maximum_lengths(gpu_engine, n, kinetic, prec):
+    """512, the longest length a slot takes, along each axis (largest shared-memory
+    tiles).  A 512-point axis over this cell's 7.6 bohr gives large |G|^2 kernel
+    factors, so the potential is ill-conditioned in the density: rounding the
+    density to FP32 alone moves the oracle's WGC potential by 3.7e-3 (relative to
+    its maximum).  The host-emulated kernels give 4e-11 in FP64 (WGC) and 1.3e-3
+    in FP32 (WT), hence 1e-10 and 5e-3."""
+    cell, _, _, _ = cases.golden_case("wgc_al4_fcc")
+    ab = (5 / 6, 5 / 6) if kinetic == fn.KEDF_WT else (1.2060113295832982827, 0.46065533708336838393)
+    f = cases.functional_for(cell, n, kinetic, *ab)
+    s = cases.engine_slot(gpu_engine, f, cell, precision=prec)
+    try:
+        rho = cases.random_density(n, cell.num_electrons, cell.vol, seed=8)
+        pot_o, et_o = fn.calculate_potential_plus(f, rho)
+        pot_g, et_g = gpu_engine.calculate_potential_plus(s, rho)
+        tol_pot, tol_e = (1e-10, 1e-10) if prec == native.FP64 else (5e-3, 5e-5)
+        assert np.abs(pot_g - pot_o).max() / np.abs(pot_o).max() < tol_pot
+        assert np.abs(et_g - et_o).max() < tol_e
+    finally:
+        gpu_engine.slot_destroy(s)
+
+
+def test_cancel_and_tick_budget_on_gpu(gpu_engine):
+    """A solve cut off by its tick budget, or cancelled while running, leaves the
+    slot idle; the next solve on it matches a fresh one."""
+    cell, f, rho_u, _ = cases.golden_case("wt_al4_displaced")
+    s = cases.engine_slot(gpu_engine, f, cell)
+    try:
+        with pytest.raises(native.OfdftError) as ei:
+            gpu_engine.proj_norm_rho_minimization(s, rho_u, native.ntn_options(max_ticks=3))
+        assert ei.value.code == 8 and gpu_engine.poll(s)
+        gpu_engine.start_solve(s, rho_u)
+        gpu_engine.run(2)
+        gpu_engine.cancel(s)
+        assert gpu_engine.poll(s)
+        r_o = ntn.NtnSolver(f).solve(rho_u)
+        _, e_g, st = gpu_engine.proj_norm_rho_minimization(s, rho_u)
+        assert st["num_evals"] == r_o.num_evals and abs(e_g[0] - r_o.energy[0]) < 1e-9
+    finally:
+        gpu_engine.slot_destroy(s)

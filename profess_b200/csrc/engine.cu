@@ -254,6 +254,10 @@ template <typename S, typename D> __global__ void __launch_bounds__(256) k_squar
     dst[i] = (D)(v * v);
   }
 }
+template <typename S, typename D> __global__ void __launch_bounds__(256) k_convert(const S* src, D* dst, long long n) {
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+    dst[i] = (D)src[i];
+}
 template <typename T> __global__ void __launch_bounds__(64) k_ctl(Args<T> a, int kid) {
   __shared__ double sm[NCH * 33 + 2];
   ctl_block(a.slots, a.ctl, a.tasks, kid, blockIdx.x, threadIdx.x, blockDim.x, (char*)sm);
@@ -375,8 +379,8 @@ struct Engine {
     dfree(d_ctl);
     plans.release();
 #if !defined(OFDFT_EMU)
-    if (pinned) cudaFreeHost(pinned);
-    pinned = nullptr;
+    dfree(d_io);
+    d_io = nullptr;
     if (stream) cudaStreamDestroy(stream);
     stream = nullptr;
 #endif
@@ -787,73 +791,68 @@ struct Engine {
     return OFDFT_OK;
   }
 
-  // Host <-> device copies of FP64 host arrays into/out of device arrays of
-  // the slot's precision, staged through a pinned host buffer on the engine
-  // stream.
-  std::vector<char> emu_stage;
-  void* pinned = nullptr;
-  size_t pinned_bytes = 0;
-  int stage(size_t bytes, void** p) {
+  // Host <-> device copies of the caller's FP64 arrays into/out of device
+  // arrays of the slot's precision.  The copies go straight from/to the
+  // caller's (pageable) buffer on the engine stream; a change of precision and
+  // the squaring of phi run on the device, through a device scratch array of
+  // n doubles, so the host does no per-point work.
 #if defined(OFDFT_EMU)
-    if (emu_stage.size() < bytes) emu_stage.resize(bytes);
-    *p = emu_stage.data();
-    return OFDFT_OK;
-#else
-    if (pinned_bytes < bytes) {
-      if (pinned) cudaFreeHost(pinned);
-      pinned = nullptr;
-      pinned_bytes = 0;
-      int rc = cuda_check(cudaMallocHost(&pinned, bytes), "cudaMallocHost");
-      if (rc) return rc;
-      pinned_bytes = bytes;
-    }
-    *p = pinned;
-    return OFDFT_OK;
-#endif
-  }
-  int copy_in(void* dst, const void* src, size_t n) {
-#if defined(OFDFT_EMU)
-    return h2d(dst, src, n);
-#else
-    int rc = cuda_check(cudaMemcpyAsync(dst, src, n, cudaMemcpyHostToDevice, stream), "H2D async");
-    return rc ? rc : cuda_check(cudaStreamSynchronize(stream), "stream synchronize");
-#endif
-  }
-  int copy_out(void* dst, const void* src, size_t n) {
-#if defined(OFDFT_EMU)
-    return d2h(dst, src, n);
-#else
-    int rc = cuda_check(cudaMemcpyAsync(dst, src, n, cudaMemcpyDeviceToHost, stream), "D2H async");
-    return rc ? rc : cuda_check(cudaStreamSynchronize(stream), "stream synchronize");
-#endif
-  }
   int upload_real(int prec, void* dst, const double* src, long long n) {
-    void* st = nullptr;
-    const size_t bytes = elem_size(prec) * (size_t)n;
-    int rc = stage(bytes, &st);
-    if (rc) return rc;
-    if (prec == OFDFT_FP64) {
-      memcpy(st, src, bytes);
-    } else {
-      float* f = (float*)st;
-      for (long long i = 0; i < n; ++i) f[i] = (float)src[i];
-    }
-    return copy_in(dst, st, bytes);
+    if (prec == OFDFT_FP64) return h2d(dst, src, sizeof(double) * (size_t)n);
+    float* f = (float*)dst;
+    for (long long i = 0; i < n; ++i) f[i] = (float)src[i];
+    return OFDFT_OK;
   }
-  int download_real(int prec, double* dst, const void* src, long long n) {
-    void* st = nullptr;
-    const size_t bytes = elem_size(prec) * (size_t)n;
-    int rc = stage(bytes, &st);
-    if (rc) return rc;
-    if ((rc = copy_out(st, src, bytes))) return rc;
-    if (prec == OFDFT_FP64) {
-      memcpy(dst, st, bytes);
-    } else {
-      const float* f = (const float*)st;
-      for (long long i = 0; i < n; ++i) dst[i] = (double)f[i];
+  int download_real(int prec, double* dst, const void* src, long long n, bool square = false) {
+    for (long long i = 0; i < n; ++i) {
+      const double v = prec == OFDFT_FP32 ? (double)((const float*)src)[i] : ((const double*)src)[i];
+      dst[i] = square ? v * v : v;
     }
     return OFDFT_OK;
   }
+#else
+  void* d_io = nullptr;
+  size_t io_bytes = 0;
+  int io_scratch(size_t bytes, void** p) {
+    if (io_bytes < bytes) {
+      dfree(d_io);
+      d_io = nullptr;
+      io_bytes = 0;
+      int rc = cuda_check(cudaMalloc(&d_io, bytes), "cudaMalloc");
+      if (rc) return rc;
+      io_bytes = bytes;
+    }
+    *p = d_io;
+    return OFDFT_OK;
+  }
+  static unsigned io_blocks(long long n) { return (unsigned)std::min<long long>(4 * 148, (n + 255) / 256); }
+  int upload_real(int prec, void* dst, const double* src, long long n) {
+    const size_t bytes = sizeof(double) * (size_t)n;
+    if (prec == OFDFT_FP64) return h2d(dst, src, bytes);
+    void* io = nullptr;
+    int rc = io_scratch(bytes, &io);
+    if (rc) return rc;
+    if ((rc = cuda_check(cudaMemcpyAsync(io, src, bytes, cudaMemcpyHostToDevice, stream), "H2D async"))) return rc;
+    k_convert<double, float><<<io_blocks(n), 256, 0, stream>>>((const double*)io, (float*)dst, n);
+    if ((rc = cuda_check(cudaGetLastError(), "convert launch"))) return rc;
+    return sync_stream();
+  }
+  int download_real(int prec, double* dst, const void* src, long long n, bool square = false) {
+    const size_t bytes = sizeof(double) * (size_t)n;
+    if (prec == OFDFT_FP64 && !square) return d2h(dst, src, bytes);
+    void* io = nullptr;
+    int rc = io_scratch(bytes, &io);
+    if (rc) return rc;
+    if (prec == OFDFT_FP64)
+      k_square_copy<double, double><<<io_blocks(n), 256, 0, stream>>>((const double*)src, (double*)io, n);
+    else if (square)
+      k_square_copy<float, double><<<io_blocks(n), 256, 0, stream>>>((const float*)src, (double*)io, n);
+    else
+      k_convert<float, double><<<io_blocks(n), 256, 0, stream>>>((const float*)src, (double*)io, n);
+    if ((rc = cuda_check(cudaGetLastError(), "convert launch"))) return rc;
+    return d2h(dst, io, bytes);
+  }
+#endif
 
   int get_ctl(int i, Ctl& c) { return d2h(&c, d_ctl + i, sizeof(Ctl)); }
   int put_ctl(int i, const Ctl& c) { return h2d(d_ctl + i, &c, sizeof(Ctl)); }
@@ -1396,8 +1395,8 @@ int ofdft_slot_result(ofdft_engine* e, int slot, double* rho, double* energy, of
   Ctl c;
   if ((rc = g.get_ctl(slot, c))) return rc;
   if (rho) {
-    if ((rc = g.download_real(h.prec, rho, h.sd.buf[c.iphi], h.sd.N))) return rc;
-    for (long long i = 0; i < h.sd.N; ++i) rho[i] = rho[i] * rho[i];  // rhoR = phi**2 (RhoOptN.f90:495)
+    // rhoR = phi**2 (RhoOptN.f90:495), squared on the device
+    if ((rc = g.download_real(h.prec, rho, h.sd.buf[c.iphi], h.sd.N, true))) return rc;
   }
   if (energy)
     for (int k = 0; k < 9; ++k) energy[k] = c.energy[k];

@@ -351,9 +351,15 @@ class Engine:
         self._check(self.lib.ofdft_slot_poll(self.h, slot, ctypes.byref(f)))
         return bool(f.value)
 
-    def result(self, slot, want_rho=True):
+    def result(self, slot, want_rho=True, out=None):
+        """(rho, energies, stats) of a finished slot; `out` (an F-ordered float64
+        array of the slot's shape) receives rho instead of a new array."""
         shp = self.shapes[slot]
-        r = np.zeros(shp, order="F") if want_rho else None
+        r = None
+        if want_rho:
+            r = out if out is not None else np.empty(shp, order="F")
+            if r.shape != tuple(shp) or r.dtype != np.float64 or not r.flags.f_contiguous:
+                raise ValueError("out must be an F-ordered float64 array of the slot's shape")
         e = np.zeros(9)
         st = NtnStats()
         self._check(self.lib.ofdft_slot_result(self.h, slot, _ptr(r) if want_rho else None, _ptr(e),

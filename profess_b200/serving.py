@@ -40,7 +40,7 @@ class Request:
     arrival: float = 0.0          # seconds after the server's start
     mode: str = MODE_MIXED
     fp32_tol: float = 3.0e-5
-    refine_iters: int = 2
+    refine_iters: int = 3
     pot_tol: float = 1.0e-6
     seed: int = 0
 
@@ -147,7 +147,7 @@ class Server:
             req = st["req"]
             if st["phase"] == "fp32" and self.eng.poll(st["s32"]):
                 self.eng.start_solve_from_slot(st["s64"], st["s32"], native.ntn_options(
-                    conv_check=native.CONV_POT, pot_tol=req.pot_tol, max_iter=req.refine_iters))
+                    conv_check=native.CONV_POT, pot_tol=req.pot_tol, max_iter=req.refine_iters, stall_line=6))
                 st["phase"] = "refine"
             elif st["phase"] in ("refine", "fp64") and self.eng.poll(st["s64"]):
                 _, e, stats = self.eng.result(st["s64"], want_rho=False)

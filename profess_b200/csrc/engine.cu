@@ -65,6 +65,18 @@ static int d2h(void* h, const void* d, size_t n) { return cuda_check(cudaMemcpy(
 static int dsync() { return cuda_check(cudaDeviceSynchronize(), "synchronize"); }
 #endif
 
+// Row pairs per x-pass block.  The x passes keep their nf*rp complex columns
+// interleaved in shared memory ([x][column]), and their prologue and epilogue
+// walk x across the threads of a warp, so consecutive threads are nf*rp
+// complex values apart.  In FP64 an even count puts 2, 4 or 8 threads of a
+// quarter-warp on the same banks (8-way at nf*rp = 24); an odd count spreads
+// them over all 32 banks.  With an odd field count, one row pair fewer makes
+// the count odd: -2 % FP64 evaluation time at 96^3.  (In FP32 the same
+// change costs 2 %: the x passes there are bound by issue, not by banks.)
+static int odd_columns(int nf, int rp, size_t csz) {
+  return (csz == 16 && (nf & 1) && !(rp & 1) && rp > 1) ? rp - 1 : rp;
+}
+
 // ------------------------------------------------------------ FFT plans
 static bool seven_smooth(int n) {
   if (n < 1) return false;
@@ -498,6 +510,8 @@ struct Engine {
     while (h.rp1 > 1 && 2 * (size_t)nfx * h.rp1 * s.n1 * csz > 72 * 1024) h.rp1--;
     s.rp = std::max(1, std::min(32, 1024 / s.n1));
     while (s.rp > 1 && 2 * (size_t)s.nf * s.rp * s.n1 * csz > 72 * 1024) s.rp--;
+    h.rp1 = odd_columns(s.nf, h.rp1, csz);
+    s.rp = odd_columns(s.nf, s.rp, csz);
     // y/z tiles: as many kx columns as fit the two shared buffers of a block
     // (one field of n2 values per column in the y pass, a group of gmax
     // fields of n3 values in the z pass) in about 56 KB, four blocks per SM;
@@ -1710,6 +1724,8 @@ extern "C" int ofdft_calculate_potential_plus_noalloc(const ofdft_cell_desc* d, 
   while (rp1 > 1 && 2 * (size_t)s.nf * rp1 * s.n1 * cs > 72 * 1024) rp1--;
   s.rp = std::max(1, std::min(32, 1024 / s.n1));
   while (s.rp > 1 && 2 * (size_t)s.nf * s.rp * s.n1 * cs > 72 * 1024) s.rp--;
+  rp1 = odd_columns(s.nf, rp1, cs);
+  s.rp = odd_columns(s.nf, s.rp, cs);
   s.tx = 16;
   while (s.tx > 2 && 2 * (size_t)s.tx * std::max(s.n2, s.n3) * cs > 100 * 1024) s.tx /= 2;
   s.ntask[K_X5] = (nrp + s.rp - 1) / s.rp;

@@ -504,15 +504,17 @@ HD void fft2_tile(const Src& src, const Dst& dst, cx<T>* __restrict__ X, int NC,
   const unsigned mnc = magic32(NC);
   for (int w = tid; w < NC * R2; w += nthr) {
     const int t = magic_div32(w, mnc), c = w - t * NC;
-    cx<T> v[R1];
+    cx<T> v[R1], f[R1];
 #pragma unroll
     for (int j1 = 0; j1 < R1; ++j1) v[j1] = src.ld(t + R2 * j1, c);
+    // the twiddles are loaded while the data loads are in flight
+#pragma unroll
+    for (int k1 = 1; k1 < R1; ++k1) f[k1] = roots[t * k1];
     Dft<T, R1, DIR>::run(v);
 #pragma unroll
     for (int k1 = 1; k1 < R1; ++k1) {
-      cx<T> f = roots[t * k1];
-      if (DIR > 0) f.y = -f.y;
-      v[k1] = cmul(v[k1], f);
+      if (DIR > 0) f[k1].y = -f[k1].y;
+      v[k1] = cmul(v[k1], f[k1]);
     }
     cx<T>* x = X + c + NC * t;
 #pragma unroll

@@ -179,6 +179,10 @@ int ofdft_calculate_potential_plus_noalloc(const ofdft_cell_desc* desc, const do
                                            void* stream);
 
 /* ---------------------------------------------------------------- batched / asynchronous */
+/* Host arrays (rho, results, downloads) are FP64 whatever the slot's
+ * precision.  They are copied straight from / to the caller's memory on the
+ * engine's stream (page-locked memory copies fastest); the FP32 conversion and
+ * phi^2 run on the device. */
 /* Upper bound of the device memory one slot of this description uses (bytes). */
 int ofdft_slot_footprint(const ofdft_cell_desc* desc, unsigned long long* bytes);
 /* Keep an input density resident on the device; start calls with rho = NULL use it. */

@@ -109,6 +109,9 @@ int ofdft_slot_destroy(ofdft_engine* e, int slot);
 int ofdft_slot_set_kernel(ofdft_engine* e, int slot, const double* kernel, int nplanes);
 /* IonElectronSpline::ionPotReal(n1G,n2G,n3G) (Source/RefreshIons.f90:215-221). */
 int ofdft_slot_set_ion_potential(ofdft_engine* e, int slot, const double* ion_pot);
+/* The ion-ion (Ewald) energy entered as eTable(6) of the slot's energies,
+ * after the ions moved (RefreshIonTerms recomputes it, Source/RefreshIons.f90:125-238). */
+int ofdft_slot_set_ion_ion_energy(ofdft_engine* e, int slot, double energy);
 /* The WT kernel built on the device from LindG (replaces FillWT, KEDF_WTkernel.f90:81-208). */
 int ofdft_slot_build_wt_kernel(ofdft_engine* e, int slot);
 /* The WGC kernel planes from radial tables of w, eta*w', eta^2*w'' on the eta
@@ -189,6 +192,12 @@ int ofdft_slot_footprint(const ofdft_cell_desc* desc, unsigned long long* bytes)
 int ofdft_slot_set_input(ofdft_engine* e, int slot, const double* rho);
 /* Start a solve from rho (host) or, with rho = NULL, from the resident input. */
 int ofdft_slot_start_solve(ofdft_engine* e, int slot, const double* rho, const ofdft_ntn_options* opts);
+/* Keep the slot's current density (phi^2 of its last solve) on the device as
+ * its resident input, so that a later start with rho = NULL resumes from it
+ * (no counterpart in the reference, whose rhoR simply persists between
+ * geometry steps): a geometry step calls it before rebuilding the ion
+ * potential, which reuses the slot's state arrays. */
+int ofdft_slot_hold_density(ofdft_engine* e, int slot);
 /* Start a solve from the density already resident in another slot of the same
  * engine (e.g. an FP32 slot's result refined in an FP64 slot); no host copy. */
 int ofdft_slot_start_solve_from_slot(ofdft_engine* e, int slot, int src_slot, const ofdft_ntn_options* opts);

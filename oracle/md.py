@@ -1,0 +1,93 @@
+"""Test infrastructure (the oracle): a CPU restatement of the reference's NVE
+molecular dynamics, RunNVE (Source/MolecularDynamicsNVE.f90:33-323), on the
+oracle's functional, NTN solver and forces.  Only tests import it.
+
+Per step: RemoveMovementOfCenterOfMass (MolecularDynamics.f90:682-743),
+AdjustCenterOfMass with the shift (MolecularDynamics.f90:1130-1191), half
+kick, drift of the unwrapped Cartesian and the wrapped fractional positions
+(MolecularDynamicsNVE.f90:208-229), RefreshIonTerms (ion potential and Ewald
+energy for the new positions), the density solve warm-started from the last
+density, CalculateForces, half kick, and the conserved energy KE + E_total
+(Conserved, MolecularDynamicsNVE.f90:378-425).
+"""
+from __future__ import annotations
+
+import dataclasses
+
+import numpy as np
+
+from . import cellsetup as cs
+from . import ewald as ew
+from . import forces as ofo
+from . import functional as fn
+from . import kedf_kernels as kk
+from . import ntn
+
+# AtomicMass (Source/Constants.f90:84+): g/mol over Avogadro's number times the
+# electron mass, both single-precision literals in the reference
+# (Source/Constants.f90:60-61).
+_MOL = float(np.float32(6.02214179e23))
+_EMASS = float(np.float32(9.1093826e-28))
+_WEIGHT = {"Al": 26.981539, "Mg": 24.3050}
+
+
+def atomic_mass(symbol: str) -> float:
+    return _WEIGHT[symbol] / (_MOL * _EMASS)
+
+
+def functional_for(cell: cs.Cell, n, alpha: float, beta: float) -> fn.Functional:
+    """The WT functional of ``cell`` on grid n with the B-spline ion potential
+    and the Ewald energy of its current positions (RefreshIonTerms,
+    Source/RefreshIons.f90:125-238)."""
+    n = tuple(int(x) for x in n)
+    qt = cs.q_table(cell.recip, *n)
+    rho_avg = cell.num_electrons / cell.vol
+    kern = kk.wt_kernel(qt, rho_avg, alpha, beta, 1.0, 1.0)[None]
+    vion = cs.ion_potential_real(cell, *n)
+    e_ii, _ = ew.ewald(cell.lattice, cell.frac, cell.charges())
+    return fn.Functional(kinetic=fn.KEDF_WT, n=n, dv=cell.vol / float(np.prod(n)), qtab=qt, kernel=kern,
+                         ion_pot=vion, ion_ion=e_ii, lam=1.0, mu=1.0, alpha=alpha, beta=beta, rho_s=rho_avg)
+
+
+@dataclasses.dataclass
+class NveState:
+    frac: np.ndarray
+    cart: np.ndarray
+    vel: np.ndarray
+    rho: np.ndarray
+    forces: np.ndarray
+    energy: float
+    conserved: float
+
+
+def run_nve(cell: cs.Cell, n, vel0: np.ndarray, dt: float, nsteps: int, opts: ntn.NtnOptions,
+            alpha: float = 5.0 / 6.0, beta: float = 5.0 / 6.0, rho0=None):
+    """Returns the list of states after the initial solve and after each step."""
+    cell = dataclasses.replace(cell, frac=np.array(cell.frac, dtype=float))
+    m = np.array([atomic_mass(cell.species[s].name) for s in cell.species_of_ion])
+    linv = np.linalg.inv(cell.lattice)
+    rho = cs.uniform_density(cell, *n) if rho0 is None else rho0
+    f = functional_for(cell, n, alpha, beta)
+    r = ntn.NtnSolver(f, opts).solve(rho)
+    rho = r.rho
+    forces, _, _ = ofo.total_forces(cell, rho)
+    vel = np.array(vel0, dtype=float)
+    cart = cell.frac @ cell.lattice.T
+    ke = lambda v: 0.5 * float((m[:, None] * v * v).sum())
+    out = [NveState(cell.frac.copy(), cart.copy(), vel.copy(), rho, forces, float(r.energy[0]),
+                    ke(vel) + float(r.energy[0]))]
+    for _ in range(nsteps):
+        vel = vel - (m[:, None] * vel).sum(axis=0) / m.sum()
+        cart = cart - (m[:, None] * cart).sum(axis=0) / m.sum()
+        cell.frac = np.mod(cart @ linv.T, 1.0)
+        vel = vel + forces / m[:, None] * (0.5 * dt)
+        cart = cart + vel * dt
+        cell.frac = np.mod(cell.frac + (vel * dt) @ linv.T, 1.0)
+        f = functional_for(cell, n, alpha, beta)
+        r = ntn.NtnSolver(f, opts).solve(rho)
+        rho = r.rho
+        forces, _, _ = ofo.total_forces(cell, rho)
+        vel = vel + forces / m[:, None] * (0.5 * dt)
+        out.append(NveState(cell.frac.copy(), cart.copy(), vel.copy(), rho, forces, float(r.energy[0]),
+                            ke(vel) + float(r.energy[0])))
+    return out

@@ -945,6 +945,34 @@ struct Engine {
     return OFDFT_OK;
   }
 
+  // Keep the slot's current density phi^2 as its resident input (device to
+  // device), so that a later start with rho = NULL resumes from it after
+  // passes that reuse the state arrays (the ion-potential build does).
+  int hold_density(int i) {
+    int rc = check_slot(i);
+    if (rc) return rc;
+    HostSlot& h = slots[i];
+    Ctl c;
+    if ((rc = get_ctl(i, c))) return rc;
+    if (!h.input && (rc = dmalloc(&h.input, elem_size(h.prec) * h.sd.N))) return rc;
+    const void* sp = h.sd.buf[c.status == ST_IDLE ? B_PHI : c.iphi];
+    const long long n = h.sd.N;
+#if defined(OFDFT_EMU)
+    for (long long k = 0; k < n; ++k) {
+      if (h.prec == OFDFT_FP32) ((float*)h.input)[k] = ((const float*)sp)[k] * ((const float*)sp)[k];
+      else ((double*)h.input)[k] = ((const double*)sp)[k] * ((const double*)sp)[k];
+    }
+    return OFDFT_OK;
+#else
+    if (h.prec == OFDFT_FP32)
+      k_square_copy<float, float><<<io_blocks(n), 256, 0, stream>>>((const float*)sp, (float*)h.input, n);
+    else
+      k_square_copy<double, double><<<io_blocks(n), 256, 0, stream>>>((const double*)sp, (double*)h.input, n);
+    if ((rc = cuda_check(cudaGetLastError(), "square copy launch"))) return rc;
+    return sync_stream();
+#endif
+  }
+
   // Start a solve in slot i from the density phi^2 held by slot src (same grid).
   int start_solve_from(int i, int src, const ofdft_ntn_options* o) {
     int rc = check_slot(i);
@@ -1341,6 +1369,19 @@ int ofdft_slot_set_ion_potential(ofdft_engine* e, int slot, const double* v) {
   if (rc) return rc;
   HostSlot& h = e->eng.slots[slot];
   return e->eng.upload_real(h.prec, h.sd.vion, v, h.sd.N);
+}
+
+int ofdft_slot_hold_density(ofdft_engine* e, int slot) {
+  if (!e) return fail(OFDFT_EINVAL, "null engine");
+  return e->eng.hold_density(slot);
+}
+
+int ofdft_slot_set_ion_ion_energy(ofdft_engine* e, int slot, double energy) {
+  if (!e) return fail(OFDFT_EINVAL, "null engine");
+  int rc = e->eng.check_slot(slot);
+  if (rc) return rc;
+  e->eng.slots[slot].sd.ion_ion = energy;
+  return e->eng.upload_slot(slot);
 }
 
 int ofdft_slot_start_eval(ofdft_engine* e, int slot, const double* rho, int opt_sqrt, int want_energy) {

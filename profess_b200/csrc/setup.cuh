@@ -385,9 +385,12 @@ inline double ewald(const double* L, int nion, const double* frac, const double*
   }
   if (forces)
     for (int i = 0; i < 3 * nion; ++i) forces[i] = 0.0;
-  double e_real = 0.0;
-#pragma omp parallel for reduction(+ : e_real) schedule(dynamic, 4)
+  // Every partial sum lands in its own slot and the slots are added in a fixed
+  // order afterwards, so the result does not depend on the thread schedule.
+  std::vector<double> e_real_i(nion, 0.0);
+#pragma omp parallel for schedule(dynamic, 4)
   for (int i = 0; i < nion; ++i) {
+    double e_i = 0.0;
     double fi[3] = {0, 0, 0};
     for (int a = -nimg[0]; a <= nimg[0]; ++a)
       for (int b = -nimg[1]; b <= nimg[1]; ++b)
@@ -402,7 +405,7 @@ inline double ewald(const double* L, int nion, const double* frac, const double*
             if (r2 < 1e-24 || r2 >= rcut * rcut) continue;
             const double r = std::sqrt(r2);
             const double ec = std::erfc(eta * r) / r;
-            e_real += 0.5 * z[i] * z[j] * ec;
+            e_i += 0.5 * z[i] * z[j] * ec;
             if (forces) {
               const double dterm = -ec / r - 2.0 * eta / std::sqrt(pi) * std::exp(-eta * eta * r2) / r;
               const double g = z[i] * z[j] * dterm / r;
@@ -414,17 +417,22 @@ inline double ewald(const double* L, int nion, const double* frac, const double*
         }
     if (forces)
       for (int k = 0; k < 3; ++k) forces[3 * i + k] += fi[k];
+    e_real_i[i] = e_i;
   }
+  double e_real = 0.0;
+  for (int i = 0; i < nion; ++i) e_real += e_real_i[i];
   double qsum = 0.0, q2 = 0.0;
   for (int i = 0; i < nion; ++i) { qsum += z[i]; q2 += z[i] * z[i]; }
   const double e_self = -eta / std::sqrt(pi) * q2;
   const double e_bg = -0.5 * pi / (eta * eta) / vol * qsum * qsum;
   // reciprocal sum over G = m1 b1 + m2 b2 + m3 b3, b_a = 2 pi (row a of inv)
-  std::vector<double> fr(forces ? 3 * nion : 0, 0.0);
-  double e_rec = 0.0;
-#pragma omp parallel for reduction(+ : e_rec) schedule(dynamic, 1)
+  const int n_m1 = 2 * ng[0] + 1;
+  const size_t nf3 = forces ? 3 * (size_t)nion : 0;
+  std::vector<double> fr_m1(nf3 * n_m1, 0.0), e_rec_m1(n_m1, 0.0);
+#pragma omp parallel for schedule(dynamic, 1)
   for (int m1 = -ng[0]; m1 <= ng[0]; ++m1) {
-    std::vector<double> floc(forces ? 3 * nion : 0, 0.0);
+    double* floc = fr_m1.data() + nf3 * (size_t)(m1 + ng[0]);
+    double e_m = 0.0;
     for (int m2 = -ng[1]; m2 <= ng[1]; ++m2)
       for (int m3 = -ng[2]; m3 <= ng[2]; ++m3) {
         if (m1 == 0 && m2 == 0 && m3 == 0) continue;
@@ -439,7 +447,7 @@ inline double ewald(const double* L, int nion, const double* frac, const double*
           si += z[i] * std::sin(ph);
         }
         const double fg = std::exp(-g2 / (4.0 * eta * eta)) / g2;
-        e_rec += 2.0 * pi / vol * fg * (sr * sr + si * si);
+        e_m += 2.0 * pi / vol * fg * (sr * sr + si * si);
         if (forces) {
           for (int i = 0; i < nion; ++i) {
             const double ph = 2.0 * pi * (m1 * frac[3 * i] + m2 * frac[3 * i + 1] + m3 * frac[3 * i + 2]);
@@ -450,13 +458,13 @@ inline double ewald(const double* L, int nion, const double* frac, const double*
           }
         }
       }
-    if (forces) {
-#pragma omp critical
-      for (int i = 0; i < 3 * nion; ++i) fr[i] += floc[i];
-    }
+    e_rec_m1[m1 + ng[0]] = e_m;
   }
-  if (forces)
-    for (int i = 0; i < 3 * nion; ++i) forces[i] += fr[i];
+  double e_rec = 0.0;
+  for (int k = 0; k < n_m1; ++k) {
+    e_rec += e_rec_m1[k];
+    for (size_t i = 0; i < nf3; ++i) forces[i] += fr_m1[nf3 * (size_t)k + i];
+  }
   return e_real + e_self + e_rec + e_bg;
 }
 

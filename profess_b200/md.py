@@ -1,0 +1,175 @@
+"""NVE molecular dynamics of many independent cells (replicas) on one engine.
+
+This is the reference's velocity-Verlet NVE driver, RunNVE
+(Source/MolecularDynamicsNVE.f90:33-323), run for a batch of replicas in
+lockstep.  Every step, for every replica: the centre-of-mass velocity is
+removed and the centre of mass moved to the origin (MolecularDynamics.f90:
+682-743, 1130-1191), a half kick, a drift, the ion terms are refreshed on the
+device (B-spline ion potential) with the Ewald energy summed on the host, and
+then the densities of all replicas are re-solved together by the engine's NTN
+solver, warm-started from each replica's resident solution.  Forces follow
+(ion-electron on the device, Ewald on the host) and a second half kick.
+
+Units are atomic (bohr, Hartree, electron masses, a.u. of time).  The density
+solves run in FP64 with the options given (the reference's density optimizer
+settings); the positions, velocities and energies stay on the host.
+"""
+from __future__ import annotations
+
+import dataclasses
+
+import numpy as np
+
+from . import cell as pcell
+from . import native
+from .workloads import Cell
+
+# Avogadro's number and the electron mass (g) as the reference stores them:
+# single-precision literals held in double-precision parameters
+# (Source/Constants.f90:60-61), hence the float32 rounding.
+_MOL = float(np.float32(6.02214179e23))
+_EMASS_G = float(np.float32(9.1093826e-28))
+BOLTZMANN = 3.16682e-6              # Ha/K (Source/Constants.f90:65)
+FUNDAMENTAL_TIME = 2.418884326505e-17  # s per a.u. of time (Source/Constants.f90:66)
+
+# Standard atomic weights (g/mol) of AtomicMass (Source/Constants.f90:84+).
+_ATOMIC_WEIGHT = {"H": 1.00794, "He": 4.002602, "Li": 6.9412, "Be": 9.012182, "B": 10.811, "C": 12.0107,
+                  "N": 14.00674, "O": 15.9994, "F": 18.9984032, "Ne": 20.1797, "Na": 22.98976928,
+                  "Mg": 24.3050, "Al": 26.981539, "Si": 28.0855, "P": 30.973762, "S": 32.066,
+                  "Cl": 35.4527, "Ar": 39.948}
+
+
+def atomic_mass(symbol: str) -> float:
+    """Ion mass in electron masses, AtomicMass (Source/Constants.f90:84+)."""
+    return _ATOMIC_WEIGHT[symbol.strip().capitalize()] / (_MOL * _EMASS_G)
+
+
+def masses_of(cell: Cell) -> np.ndarray:
+    return np.array([atomic_mass(cell.species[s].name) for s in cell.species_of_ion], dtype=float)
+
+
+def initial_velocities(cell: Cell, temperature_k: float, seed: int = 0) -> np.ndarray:
+    """Random velocities at a temperature, InitVelocity (MolecularDynamics.f90:575-679):
+    Box-Muller normals divided by the mass, the centre-of-mass velocity removed,
+    then scaled so that KE = 3/2 N k T.  The reference draws from the Fortran
+    RANDOM_NUMBER generator; this one uses a seeded NumPy generator."""
+    n = cell.nion
+    m = masses_of(cell)
+    rng = np.random.default_rng(seed)
+    flat = np.zeros(3 * n)
+    for i in range(1, 3 * n // 2 + 2):
+        r1, r2 = rng.random(2)
+        r1 = max(r1, np.finfo(float).tiny)
+        a, b = np.sqrt(-2.0 * np.log(r1)) * np.cos(2 * np.pi * r2), np.sqrt(-2.0 * np.log(r1)) * np.sin(2 * np.pi * r2)
+        if 2 * i - 2 < 3 * n:
+            flat[2 * i - 2] = a
+        if 2 * i - 1 < 3 * n:
+            flat[2 * i - 1] = b
+    v = flat.reshape(n, 3) / m[:, None]
+    v -= (m[:, None] * v).sum(axis=0) / m.sum()
+    ke = 0.5 * float((m[:, None] * v * v).sum())
+    return v * np.sqrt(temperature_k * BOLTZMANN * 1.5 * n / ke)
+
+
+@dataclasses.dataclass
+class Replica:
+    cell: Cell
+    slot: int
+    mass: np.ndarray
+    vel: np.ndarray          # (nion, 3) bohr per a.u. of time
+    cart: np.ndarray         # (nion, 3) unwrapped Cartesian positions (cartNoWrap)
+    forces: np.ndarray = None
+    f_ewald: np.ndarray = None   # Ewald forces of the current positions (host)
+    energy: np.ndarray = None
+    stats: dict = None
+    history: list = dataclasses.field(default_factory=list)
+
+    def kinetic_energy(self) -> float:
+        return 0.5 * float((self.mass[:, None] * self.vel * self.vel).sum())
+
+    def conserved(self) -> float:
+        return self.kinetic_energy() + float(self.energy[0])
+
+    def temperature(self) -> float:
+        return 2.0 * self.kinetic_energy() / (3.0 * self.cell.nion) / BOLTZMANN
+
+
+class NVE:
+    """Lockstep NVE dynamics of ``cells`` (each gets one FP64 slot).
+
+    ``dt`` in a.u. of time; ``velocities`` a list of (nion, 3) arrays (bohr per
+    a.u. of time), or None for random ones at ``temperature_k``.
+    ``opts``: NTN options of every density solve (native.ntn_options)."""
+
+    def __init__(self, eng: native.Engine, cells, dt: float, velocities=None, temperature_k: float = 300.0,
+                 seed: int = 0, opts=None, rho0=None):
+        self.eng = eng
+        self.dt = float(dt)
+        self.opts = opts or native.ntn_options(conv_check=native.CONV_POT, pot_tol=1.0e-6)
+        self.reps = []
+        try:
+            for k, c in enumerate(cells):
+                c = dataclasses.replace(c, frac=np.array(c.frac, dtype=float))
+                s = pcell.setup_slot(eng, c, native.FP64)
+                v = (np.array(velocities[k], dtype=float) if velocities is not None
+                     else initial_velocities(c, temperature_k, seed + k))
+                self.reps.append(Replica(cell=c, slot=s, mass=masses_of(c), vel=v, cart=c.frac @ c.lattice.T))
+            # the first solve starts from the given (or the uniform) density
+            for k, r in enumerate(self.reps):
+                self._refresh_ewald(r)
+                rho = rho0[k] if rho0 is not None else np.full(r.cell.grid, r.cell.num_electrons / r.cell.vol)
+                self.eng.start_solve(r.slot, np.asfortranarray(rho, dtype=float), self.opts)
+            self._finish_solves()
+        except Exception:
+            self.close()
+            raise
+
+    def close(self):
+        for r in self.reps:
+            self.eng.slot_destroy(r.slot)
+        self.reps = []
+
+    # ------------------------------------------------------------------ steps
+    def _refresh_ewald(self, r: Replica):
+        """Ewald energy (into the slot's energy table) and forces of the current
+        positions, one host sum for both."""
+        c = r.cell
+        e_ii, r.f_ewald = native.ewald(self.eng.lib, c.lattice, c.frac, c.charges(), True)
+        self.eng.set_ion_ion_energy(r.slot, e_ii)
+
+    def _finish_solves(self):
+        while self.eng.run(8):
+            pass
+        for r in self.reps:
+            _, r.energy, r.stats = self.eng.result(r.slot, want_rho=False)
+            if r.stats["outcome"] != 0:
+                raise native.OfdftError(7, "density solve did not converge (replica slot %d)" % r.slot)
+            r.forces = self.eng.forces(r.slot, r.cell.nion, include_ewald=False) + r.f_ewald
+
+    def step(self):
+        """One velocity-Verlet step of every replica (MolecularDynamicsNVE.f90:202-300)."""
+        dt = self.dt
+        for r in self.reps:
+            c, m = r.cell, r.mass
+            r.vel -= (m[:, None] * r.vel).sum(axis=0) / m.sum()          # RemoveMovementOfCenterOfMass
+            linv = np.linalg.inv(c.lattice)
+            r.cart -= (m[:, None] * r.cart).sum(axis=0) / m.sum()        # AdjustCenterOfMass
+            c.frac = np.mod(r.cart @ linv.T, 1.0)
+            r.vel += r.forces / m[:, None] * (0.5 * dt)
+            r.cart += r.vel * dt
+            c.frac = np.mod(c.frac + (r.vel * dt) @ linv.T, 1.0)
+            # RefreshIonTerms: ion potential on the device, Ewald energy on the host;
+            # the density of the last solve is held on the device for the warm start
+            self.eng.hold_density(r.slot)
+            self.eng.build_ion_potential(r.slot, c.frac, c.species_of_ion, c.species)
+            self._refresh_ewald(r)
+            self.eng.start_solve(r.slot, None, self.opts)
+        self._finish_solves()
+        for r in self.reps:
+            r.vel += r.forces / r.mass[:, None] * (0.5 * dt)
+            r.history.append({"energy": float(r.energy[0]), "conserved": r.conserved(),
+                              "temperature": r.temperature(), "num_evals": r.stats["num_evals"]})
+
+    def run(self, nsteps: int):
+        for _ in range(nsteps):
+            self.step()

@@ -73,6 +73,8 @@ SIGNATURES = {
     "ofdft_slot_destroy": [_vp, ctypes.c_int],
     "ofdft_slot_set_kernel": [_vp, ctypes.c_int, _dp, ctypes.c_int],
     "ofdft_slot_set_ion_potential": [_vp, ctypes.c_int, _dp],
+    "ofdft_slot_set_ion_ion_energy": [_vp, ctypes.c_int, ctypes.c_double],
+    "ofdft_slot_hold_density": [_vp, ctypes.c_int],
     "ofdft_slot_build_wt_kernel": [_vp, ctypes.c_int],
     "ofdft_slot_build_wgc_kernel": [_vp, ctypes.c_int, ctypes.c_int, _dp, _dp, _dp, _dp],
     "ofdft_slot_build_ion_potential": [_vp, ctypes.c_int, ctypes.c_int, _dp, _ip, ctypes.c_int, _ip,
@@ -272,6 +274,14 @@ class Engine:
         self._check(self.lib.ofdft_slot_forces(self.h, slot, _ptr(r) if r is not None else None,
                                                int(bool(include_ewald)), _ptr(out)))
         return out
+
+    def hold_density(self, slot):
+        """Keep the slot's solved density as its resident input (start_solve(slot) resumes from it)."""
+        self._check(self.lib.ofdft_slot_hold_density(self.h, slot))
+
+    def set_ion_ion_energy(self, slot, energy):
+        """The Ewald energy (Ha) reported in the slot's energies, after the ions moved."""
+        self._check(self.lib.ofdft_slot_set_ion_ion_energy(self.h, slot, float(energy)))
 
     def set_ion_potential(self, slot, vion):
         v = _fortran(vion, self.shapes[slot])

@@ -1,0 +1,82 @@
+"""NVE molecular dynamics of replicas on the engine (profess_b200.md) against
+the oracle's restatement of RunNVE (oracle/md.py), on the host-emulation
+build (CPU); test_gpu_md.py repeats them on the CUDA build."""
+import numpy as np
+import pytest
+
+from oracle import cellsetup as cs
+from oracle import md as omd
+from oracle import ntn
+from profess_b200 import md, native, workloads as wl
+
+DT = 40.0  # a.u. of time (~0.97 fs)
+
+
+def _cells():
+    c = wl.fcc_al((1, 1, 1), sigma_ang=0.05, grid=(20, 20, 20), seed=3)
+    mx, vals = wl.gha_table(3.0, 1.15, 0.1)
+    ocell = cs.Cell(lattice=c.lattice, frac=c.frac, species_of_ion=c.species_of_ion,
+                    species=[cs.species_from_table(mx, vals, "Al")])
+    return c, ocell
+
+
+def _wrap(d):
+    return d - np.rint(d)
+
+
+def check_nve_matches_oracle(eng, nsteps=3):
+    c, ocell = _cells()
+    v0 = md.initial_velocities(c, 600.0, seed=4)
+    opts = native.ntn_options(conv_check=native.CONV_POT, pot_tol=1.0e-6)
+    run = md.NVE(eng, [c], DT, velocities=[v0], opts=opts)
+    try:
+        run.run(nsteps)
+        rep = run.reps[0]
+        ref = omd.run_nve(ocell, c.grid, v0, DT, nsteps, ntn.NtnOptions(conv_check="POT", pot_tol=1.0e-6))
+        last = ref[-1]
+        assert np.abs(_wrap(rep.cell.frac - last.frac)).max() < 1e-10
+        assert np.abs(rep.vel - last.vel).max() < 1e-10 * np.abs(last.vel).max() + 1e-14
+        assert abs(float(rep.energy[0]) - last.energy) < 1e-8
+        assert np.abs(rep.forces - last.forces).max() < 1e-8
+        cons = [h["conserved"] for h in rep.history]
+        assert max(cons) - min(cons) < 1e-4  # Ha, 3 steps of ~1 fs
+        assert all(abs(h["conserved"] - s.conserved) < 1e-8 for h, s in zip(rep.history, ref[1:]))
+    finally:
+        run.close()
+
+
+def test_atomic_masses():
+    assert abs(md.atomic_mass("Al") - 49184.3) < 1.0  # 26.98 amu in electron masses
+    assert md.atomic_mass("Al") == omd.atomic_mass("Al")
+
+
+def test_initial_velocities_temperature_and_momentum():
+    c, _ = _cells()
+    v = md.initial_velocities(c, 600.0, seed=1)
+    m = md.masses_of(c)
+    assert np.abs((m[:, None] * v).sum(axis=0)).max() < 1e-12
+    ke = 0.5 * float((m[:, None] * v * v).sum())
+    assert abs(ke - 1.5 * c.nion * 600.0 * md.BOLTZMANN) < 1e-12
+
+
+def test_nve_matches_oracle(emu_engine):
+    check_nve_matches_oracle(emu_engine)
+
+
+def test_nve_replicas_batched_as_alone(emu_engine):
+    """Two replicas stepped together give the same trajectories as each alone."""
+    cells = [wl.fcc_al((1, 1, 1), sigma_ang=0.05, grid=(16, 16, 16), seed=s) for s in (1, 2)]
+    vs = [md.initial_velocities(c, 300.0, seed=s) for s, c in enumerate(cells)]
+    alone = []
+    for c, v in zip(cells, vs):
+        r = md.NVE(emu_engine, [c], DT, velocities=[v])
+        r.run(2)
+        alone.append((r.reps[0].cell.frac.copy(), r.reps[0].vel.copy(), float(r.reps[0].energy[0])))
+        r.close()
+    both = md.NVE(emu_engine, cells, DT, velocities=vs)
+    try:
+        both.run(2)
+        for rep, (fr, v, e) in zip(both.reps, alone):
+            assert np.array_equal(rep.cell.frac, fr) and np.array_equal(rep.vel, v) and float(rep.energy[0]) == e
+    finally:
+        both.close()

@@ -109,6 +109,11 @@ int ofdft_slot_destroy(ofdft_engine* e, int slot);
 int ofdft_slot_set_kernel(ofdft_engine* e, int slot, const double* kernel, int nplanes);
 /* IonElectronSpline::ionPotReal(n1G,n2G,n3G) (Source/RefreshIons.f90:215-221). */
 int ofdft_slot_set_ion_potential(ofdft_engine* e, int slot, const double* ion_pot);
+/* Ewald energy (Ha) and forces (Ha/bohr, nion x 3, may be NULL) of the slot's
+ * ions (the positions of its last ofdft_slot_build_ion_potential), summed on
+ * the device (EwaldEnergy / EwaldForces, Source/Ewald.f90:465-1193); the energy
+ * also becomes the slot's eTable(6).  Same splitting and cut-offs as ofdft_ewald. */
+int ofdft_slot_ewald(ofdft_engine* e, int slot, double* energy, double* forces);
 /* The ion-ion (Ewald) energy entered as eTable(6) of the slot's energies,
  * after the ions moved (RefreshIonTerms recomputes it, Source/RefreshIons.f90:125-238). */
 int ofdft_slot_set_ion_ion_energy(ofdft_engine* e, int slot, double energy);

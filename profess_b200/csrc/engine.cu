@@ -21,6 +21,7 @@
 #include <vector>
 
 #include "setup.cuh"
+#include "ewald.cuh"
 #include "profess_b200.h"
 
 #if !defined(OFDFT_EMU)
@@ -306,6 +307,12 @@ struct HostSlot {
   double rho0 = 0, gamma = 2.7;
   std::vector<double> frac, zion;
   void* input = nullptr;        // device-resident input density (ofdft_slot_set_input)
+  // pseudopotential tables and B-spline factors of the last ion-potential build
+  // (device copy, and the host copy they were uploaded from)
+  void* ion_aux = nullptr;
+  size_t ion_aux_bytes = 0;
+  std::vector<double> ion_tab;
+  IonAux ion_ax;
 };
 
 static size_t elem_size(int prec) { return prec == OFDFT_FP32 ? 4 : 8; }
@@ -412,6 +419,10 @@ struct Engine {
     h.nion = 0;
     if (h.input) dfree(h.input);
     h.input = nullptr;
+    if (h.ion_aux) dfree(h.ion_aux);
+    h.ion_aux = nullptr;
+    h.ion_aux_bytes = 0;
+    h.ion_tab.clear();
     h.used = false;
     h.running = false;
     dirty = true;
@@ -669,22 +680,37 @@ struct Engine {
     }
     for (int k = 0; k < nion; ++k)
       if (species[k] < 0 || species[k] >= nspec) return fail(OFDFT_EINVAL, "ion species index out of range");
-    const std::vector<cx<double>> b1 = bspline_b(s.k1, s.n1), b2 = bspline_b(s.n2, s.n2), b3 = bspline_b(s.n3, s.n3);
-    const size_t bytes = sizeof(double) * tab.size() + sizeof(cx<double>) * (b1.size() + b2.size() + b3.size());
-    void* aux = nullptr;
-    if ((rc = alloc(h, &aux, bytes))) return rc;
-    char* cur = (char*)aux;
-    if ((rc = h2d(cur, tab.data(), sizeof(double) * tab.size()))) return rc;
-    ax.tab = (const double*)cur;
-    cur += sizeof(double) * tab.size();
-    if ((rc = h2d(cur, b1.data(), sizeof(cx<double>) * b1.size()))) return rc;
-    ax.b1 = (const cx<double>*)cur;
-    cur += sizeof(cx<double>) * b1.size();
-    if ((rc = h2d(cur, b2.data(), sizeof(cx<double>) * b2.size()))) return rc;
-    ax.b2 = (const cx<double>*)cur;
-    cur += sizeof(cx<double>) * b2.size();
-    if ((rc = h2d(cur, b3.data(), sizeof(cx<double>) * b3.size()))) return rc;
-    ax.b3 = (const cx<double>*)cur;
+    // The tables go to the device once per species set: a geometry step that
+    // only moves the ions reuses them (and their device buffer).
+    const bool same_tables = h.ion_aux && h.ion_tab == tab && h.ion_ax.nspec == nspec &&
+                             memcmp(h.ion_ax.psp, ax.psp, sizeof(ax.psp)) == 0;
+    if (same_tables) {
+      ax = h.ion_ax;
+    } else {
+      const std::vector<cx<double>> b1 = bspline_b(s.k1, s.n1), b2 = bspline_b(s.n2, s.n2), b3 = bspline_b(s.n3, s.n3);
+      const size_t bytes = sizeof(double) * tab.size() + sizeof(cx<double>) * (b1.size() + b2.size() + b3.size());
+      if (h.ion_aux_bytes != bytes) {
+        if (h.ion_aux) dfree(h.ion_aux);
+        h.ion_aux = nullptr;
+        h.ion_aux_bytes = 0;
+        if ((rc = dmalloc(&h.ion_aux, bytes))) return rc;
+        h.ion_aux_bytes = bytes;
+      }
+      char* cur = (char*)h.ion_aux;
+      if ((rc = h2d(cur, tab.data(), sizeof(double) * tab.size()))) return rc;
+      ax.tab = (const double*)cur;
+      cur += sizeof(double) * tab.size();
+      if ((rc = h2d(cur, b1.data(), sizeof(cx<double>) * b1.size()))) return rc;
+      ax.b1 = (const cx<double>*)cur;
+      cur += sizeof(cx<double>) * b1.size();
+      if ((rc = h2d(cur, b2.data(), sizeof(cx<double>) * b2.size()))) return rc;
+      ax.b2 = (const cx<double>*)cur;
+      cur += sizeof(cx<double>) * b2.size();
+      if ((rc = h2d(cur, b3.data(), sizeof(cx<double>) * b3.size()))) return rc;
+      ax.b3 = (const cx<double>*)cur;
+      h.ion_tab = tab;
+      h.ion_ax = ax;
+    }
     s.ion = ax;
     if ((rc = upload_slot(i))) return rc;
     // ion stencils (kept for the forces)
@@ -796,9 +822,9 @@ struct Engine {
       for (int r = 0; r < 3; ++r)
         out[3 * k + r] = -(h.cell_inv_t[3 * r] * q[3 * k] + h.cell_inv_t[3 * r + 1] * q[3 * k + 1] +
                            h.cell_inv_t[3 * r + 2] * q[3 * k + 2]);
-    if (include_ewald) {
+    if (include_ewald) {  // ion-ion forces summed on the device
       std::vector<double> fii(3 * (size_t)h.nion);
-      ewald(h.lattice, h.nion, h.frac.data(), h.zion.data(), fii.data());
+      if ((rc = ewald_device(i, nullptr, fii.data()))) return rc;
       for (size_t k = 0; k < fii.size(); ++k) out[k] += fii[k];
     }
     return OFDFT_OK;
@@ -943,6 +969,78 @@ struct Engine {
     h.running = true;
     dirty = true;
     return OFDFT_OK;
+  }
+
+  // Ewald energy and forces (Ha, Ha/bohr; forces may be NULL) of the slot's
+  // ions, summed on the device.
+  int ewald_device(int i, double* energy, double* forces) {
+    int rc = OFDFT_OK;
+    HostSlot& h = slots[i];
+    const int nion = h.nion;
+    if (nion < 1) return fail(OFDFT_EINVAL, "build the ion potential before the Ewald sum");
+    const EwaldPar p = ewald_par(h.lattice, nion);
+    const int npl = ewald_planes(p), plane = ewald_plane_size(p);
+    std::vector<double> pos(3 * (size_t)nion);
+    for (int k = 0; k < nion; ++k)
+      for (int r = 0; r < 3; ++r)
+        pos[3 * k + r] = p.A[r][0] * h.frac[3 * k] + p.A[r][1] * h.frac[3 * k + 1] + p.A[r][2] * h.frac[3 * k + 2];
+    std::vector<double> real4(4 * (size_t)nion), plane4(4 * (size_t)npl), rec4(4 * (size_t)nion);
+#if defined(OFDFT_EMU)
+    std::vector<cx<double>> sfac((size_t)npl * plane);
+    double red[4];
+    for (int k = 0; k < nion; ++k) ewald_real_block(p, pos.data(), h.zion.data(), k, 0, 1, red, &real4[4 * k]);
+    for (int m = 0; m < npl; ++m) ewald_plane_block(p, h.frac.data(), h.zion.data(), m, 0, 1, red, sfac.data(), &plane4[4 * m]);
+    if (forces)
+      for (int k = 0; k < nion; ++k)
+        ewald_recip_force_block(p, h.frac.data(), h.zion.data(), sfac.data(), k, 0, 1, red, &rec4[4 * k]);
+#else
+    // one scratch array (the engine's transfer scratch): pos, frac, z, the three
+    // 4-value outputs, S(G)
+    const size_t nd = 3 * (size_t)nion * 2 + nion + 4 * (size_t)nion * 2 + 4 * (size_t)npl;
+    double* dbuf = nullptr;
+    if ((rc = io_scratch(sizeof(double) * nd + sizeof(cx<double>) * (size_t)npl * plane, (void**)&dbuf))) return rc;
+    double *dpos = dbuf, *dfrac = dpos + 3 * nion, *dz = dfrac + 3 * nion, *dreal = dz + nion, *drec = dreal + 4 * nion,
+           *dplane = drec + 4 * nion;
+    cx<double>* dsf = (cx<double>*)(dbuf + nd);
+    rc = h2d(dpos, pos.data(), sizeof(double) * 3 * nion);
+    if (!rc) rc = h2d(dfrac, h.frac.data(), sizeof(double) * 3 * nion);
+    if (!rc) rc = h2d(dz, h.zion.data(), sizeof(double) * nion);
+    if (!rc) {
+      k_ewald_real<<<nion, 256, 0, stream>>>(p, dpos, dz, dreal);
+      k_ewald_plane<<<npl, 256, 0, stream>>>(p, dfrac, dz, dsf, dplane);
+      if (forces) k_ewald_recip_force<<<nion, 256, 0, stream>>>(p, dfrac, dz, dsf, drec);
+      rc = cuda_check(cudaGetLastError(), "Ewald launch");
+    }
+    if (!rc) rc = d2h(real4.data(), dreal, sizeof(double) * 4 * nion);
+    if (!rc) rc = d2h(plane4.data(), dplane, sizeof(double) * 4 * npl);
+    if (!rc && forces) rc = d2h(rec4.data(), drec, sizeof(double) * 4 * nion);
+    if (rc) return rc;
+#endif
+    double qsum = 0.0, q2 = 0.0, e_real = 0.0, e_rec = 0.0;
+    for (int k = 0; k < nion; ++k) {
+      qsum += h.zion[k];
+      q2 += h.zion[k] * h.zion[k];
+      e_real += real4[4 * k];
+    }
+    for (int m = 0; m < npl; ++m) e_rec += plane4[4 * m];
+    const double e_self = -p.eta / std::sqrt(PI_D) * q2;
+    const double e_bg = -0.5 * PI_D / (p.eta * p.eta) / p.vol * qsum * qsum;
+    const double e = e_real + e_self + e_rec + e_bg;
+    if (forces)
+      for (int k = 0; k < nion; ++k)
+        for (int r = 0; r < 3; ++r) forces[3 * k + r] = real4[4 * k + 1 + r] + rec4[4 * k + 1 + r];
+    if (energy) *energy = e;
+    return OFDFT_OK;
+  }
+  // The same, with the energy made the slot's eTable(6).
+  int slot_ewald(int i, double* energy, double* forces) {
+    int rc = check_slot(i);
+    if (rc) return rc;
+    double e = 0.0;
+    if ((rc = ewald_device(i, &e, forces))) return rc;
+    if (energy) *energy = e;
+    slots[i].sd.ion_ion = e;
+    return upload_slot(i);
   }
 
   // Keep the slot's current density phi^2 as its resident input (device to
@@ -1250,19 +1348,34 @@ struct Engine {
   }
 #endif
 
-  // Launch `n` ticks (through the captured graph when it covers n).
+  // Launch `n` ticks.  Several ticks go through a captured graph (captured
+  // again when the task lists changed); a single tick (set-up passes, forces,
+  // lone evaluations) is launched directly, since capturing and instantiating
+  // a graph for one tick costs more than it saves.
+  bool graph_stale = true;  // the task lists changed since the graph and the shared-memory limits were set
+  bool attrs_stale = true;
   int launch_ticks(int n) {
     int rc;
     if (dirty) {
       if ((rc = build_lists())) return rc;
-#if !defined(OFDFT_EMU)
-      if ((rc = capture(n))) return rc;
-#endif
+      graph_stale = true;
+      attrs_stale = true;
     }
     n_ticks += n;
     n_launches += (long long)n * launches_per_tick();
 #if !defined(OFDFT_EMU)
-    if (graph_exec && graph_ticks == n) return cuda_check(cudaGraphLaunch(graph_exec, stream), "graph launch");
+    if (n > 1) {
+      if (graph_stale || !graph_exec || graph_ticks != n) {
+        if ((rc = capture(n))) return rc;
+        graph_stale = false;
+        attrs_stale = false;
+      }
+      return cuda_check(cudaGraphLaunch(graph_exec, stream), "graph launch");
+    }
+    if (attrs_stale) {
+      if ((rc = set_smem_attrs<double>(OFDFT_FP64)) || (rc = set_smem_attrs<float>(OFDFT_FP32))) return rc;
+      attrs_stale = false;
+    }
 #endif
     for (int k = 0; k < n; ++k)
       if ((rc = tick())) return rc;
@@ -1369,6 +1482,11 @@ int ofdft_slot_set_ion_potential(ofdft_engine* e, int slot, const double* v) {
   if (rc) return rc;
   HostSlot& h = e->eng.slots[slot];
   return e->eng.upload_real(h.prec, h.sd.vion, v, h.sd.N);
+}
+
+int ofdft_slot_ewald(ofdft_engine* e, int slot, double* energy, double* forces) {
+  if (!e) return fail(OFDFT_EINVAL, "null engine");
+  return e->eng.slot_ewald(slot, energy, forces);
 }
 
 int ofdft_slot_hold_density(ofdft_engine* e, int slot) {

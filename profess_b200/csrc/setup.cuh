@@ -349,15 +349,26 @@ inline int wgc_radial_tables(double alpha, double beta, double gamma, std::vecto
 // (EwaldEnergy, Source/Ewald.f90:465-520, 1150-1190), evaluated directly with
 // splitting eta = sqrt(pi) (N / V^2)^(1/6) and both sums converged to ~1e-14
 // relative; forces are -dE/dR (Ha/bohr).
-inline double ewald(const double* L, int nion, const double* frac, const double* z, double* forces) {
+// Splitting, cut-offs and image / reciprocal-plane ranges of the Ewald sum,
+// shared by the host sum below and the device sum (ewald.cuh).
+struct EwaldPar {
+  double A[3][3];    // A[k][i] = component k of lattice vector i
+  double inv[3][3];  // inverse of A
+  double vol, eta, rcut, gcut;
+  int nimg[3], ng[3];
+  int nion;
+};
+
+inline EwaldPar ewald_par(const double* L, int nion) {
   // L[3*i + k] = component k of lattice vector i
-  double A[3][3];
+  EwaldPar p;
+  double (&A)[3][3] = p.A;
+  double (&inv)[3][3] = p.inv;
   for (int i = 0; i < 3; ++i)
     for (int k = 0; k < 3; ++k) A[k][i] = L[3 * i + k];
   const double det = A[0][0] * (A[1][1] * A[2][2] - A[1][2] * A[2][1]) - A[0][1] * (A[1][0] * A[2][2] - A[1][2] * A[2][0]) +
                      A[0][2] * (A[1][0] * A[2][1] - A[1][1] * A[2][0]);
-  const double vol = std::fabs(det);
-  double inv[3][3];
+  p.vol = std::fabs(det);
   inv[0][0] = (A[1][1] * A[2][2] - A[1][2] * A[2][1]) / det;
   inv[0][1] = (A[0][2] * A[2][1] - A[0][1] * A[2][2]) / det;
   inv[0][2] = (A[0][1] * A[1][2] - A[0][2] * A[1][1]) / det;
@@ -368,21 +379,33 @@ inline double ewald(const double* L, int nion, const double* frac, const double*
   inv[2][1] = (A[0][1] * A[2][0] - A[0][0] * A[2][1]) / det;
   inv[2][2] = (A[0][0] * A[1][1] - A[0][1] * A[1][0]) / det;
   const double pi = PI_D;
-  const double eta = std::sqrt(pi) * std::pow((double)std::max(nion, 1) / (vol * vol), 1.0 / 6.0);
-  const double rcut = 7.0 / eta, gcut = 2.0 * eta * 7.0;
-  std::vector<double> pos(3 * nion);
-  for (int i = 0; i < nion; ++i)
-    for (int k = 0; k < 3; ++k) pos[3 * i + k] = A[k][0] * frac[3 * i] + A[k][1] * frac[3 * i + 1] + A[k][2] * frac[3 * i + 2];
+  p.eta = std::sqrt(pi) * std::pow((double)std::max(nion, 1) / (p.vol * p.vol), 1.0 / 6.0);
+  p.rcut = 7.0 / p.eta;
+  p.gcut = 2.0 * p.eta * 7.0;
   // image ranges: heights of the cell along each reciprocal direction
-  int nimg[3], ng[3];
   for (int a = 0; a < 3; ++a) {
     const double hr = 1.0 / std::sqrt(inv[a][0] * inv[a][0] + inv[a][1] * inv[a][1] + inv[a][2] * inv[a][2]);
-    nimg[a] = (int)std::ceil(rcut / hr) + 1;
+    p.nimg[a] = (int)std::ceil(p.rcut / hr) + 1;
     // reciprocal vector a has length 2 pi |row a of inv|; plane spacing in G space
     double la = 0;
     for (int k = 0; k < 3; ++k) la += A[k][a] * A[k][a];
-    ng[a] = (int)std::ceil(gcut * std::sqrt(la) / (2.0 * pi)) + 1;
+    p.ng[a] = (int)std::ceil(p.gcut * std::sqrt(la) / (2.0 * pi)) + 1;
   }
+  p.nion = nion;
+  return p;
+}
+
+inline double ewald(const double* L, int nion, const double* frac, const double* z, double* forces) {
+  const EwaldPar p = ewald_par(L, nion);
+  const double(&A)[3][3] = p.A;
+  const double(&inv)[3][3] = p.inv;
+  const double vol = p.vol, eta = p.eta, rcut = p.rcut, gcut = p.gcut;
+  const int* nimg = p.nimg;
+  const int* ng = p.ng;
+  const double pi = PI_D;
+  std::vector<double> pos(3 * nion);
+  for (int i = 0; i < nion; ++i)
+    for (int k = 0; k < 3; ++k) pos[3 * i + k] = A[k][0] * frac[3 * i] + A[k][1] * frac[3 * i + 1] + A[k][2] * frac[3 * i + 2];
   if (forces)
     for (int i = 0; i < 3 * nion; ++i) forces[i] = 0.0;
   // Every partial sum lands in its own slot and the slots are added in a fixed

@@ -5,10 +5,10 @@ This is the reference's velocity-Verlet NVE driver, RunNVE
 lockstep.  Every step, for every replica: the centre-of-mass velocity is
 removed and the centre of mass moved to the origin (MolecularDynamics.f90:
 682-743, 1130-1191), a half kick, a drift, the ion terms are refreshed on the
-device (B-spline ion potential) with the Ewald energy summed on the host, and
+device (B-spline ion potential, Ewald energy and forces), and
 then the densities of all replicas are re-solved together by the engine's NTN
 solver, warm-started from each replica's resident solution.  Forces follow
-(ion-electron on the device, Ewald on the host) and a second half kick.
+(ion-electron on the device, plus the Ewald forces) and a second half kick.
 
 Units are atomic (bohr, Hartree, electron masses, a.u. of time).  The density
 solves run in FP64 with the options given (the reference's density optimizer
@@ -131,11 +131,9 @@ class NVE:
 
     # ------------------------------------------------------------------ steps
     def _refresh_ewald(self, r: Replica):
-        """Ewald energy (into the slot's energy table) and forces of the current
-        positions, one host sum for both."""
-        c = r.cell
-        e_ii, r.f_ewald = native.ewald(self.eng.lib, c.lattice, c.frac, c.charges(), True)
-        self.eng.set_ion_ion_energy(r.slot, e_ii)
+        """Ewald energy (into the slot's energy table) and forces of the positions
+        of the slot's last ion-potential build, one device sum for both."""
+        _, r.f_ewald = self.eng.ewald(r.slot, r.cell.nion)
 
     def _finish_solves(self):
         while self.eng.run(8):
@@ -158,7 +156,7 @@ class NVE:
             r.vel += r.forces / m[:, None] * (0.5 * dt)
             r.cart += r.vel * dt
             c.frac = np.mod(c.frac + (r.vel * dt) @ linv.T, 1.0)
-            # RefreshIonTerms: ion potential on the device, Ewald energy on the host;
+            # RefreshIonTerms: ion potential and Ewald sum on the device;
             # the density of the last solve is held on the device for the warm start
             self.eng.hold_density(r.slot)
             self.eng.build_ion_potential(r.slot, c.frac, c.species_of_ion, c.species)

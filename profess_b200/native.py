@@ -75,6 +75,7 @@ SIGNATURES = {
     "ofdft_slot_set_ion_potential": [_vp, ctypes.c_int, _dp],
     "ofdft_slot_set_ion_ion_energy": [_vp, ctypes.c_int, ctypes.c_double],
     "ofdft_slot_hold_density": [_vp, ctypes.c_int],
+    "ofdft_slot_ewald": [_vp, ctypes.c_int, _dp, _dp],
     "ofdft_slot_build_wt_kernel": [_vp, ctypes.c_int],
     "ofdft_slot_build_wgc_kernel": [_vp, ctypes.c_int, ctypes.c_int, _dp, _dp, _dp, _dp],
     "ofdft_slot_build_ion_potential": [_vp, ctypes.c_int, ctypes.c_int, _dp, _ip, ctypes.c_int, _ip,
@@ -274,6 +275,14 @@ class Engine:
         self._check(self.lib.ofdft_slot_forces(self.h, slot, _ptr(r) if r is not None else None,
                                                int(bool(include_ewald)), _ptr(out)))
         return out
+
+    def ewald(self, slot, nion, want_forces=True):
+        """Device Ewald energy (Ha) and forces (nion, 3) of the slot's ions; the
+        energy also becomes the slot's ion-ion energy."""
+        e = np.zeros(1)
+        f = np.zeros((nion, 3)) if want_forces else None
+        self._check(self.lib.ofdft_slot_ewald(self.h, slot, _ptr(e), _ptr(f) if want_forces else None))
+        return float(e[0]), f
 
     def hold_density(self, slot):
         """Keep the slot's solved density as its resident input (start_solve(slot) resumes from it)."""

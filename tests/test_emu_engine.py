@@ -260,3 +260,26 @@ def test_engine_slot_capacity():
         for s in slots:
             eng.slot_destroy(s)
         eng.close()
+
+
+def check_device_ewald(eng):
+    """The engine's device Ewald sum (energy into the slot's table, forces) against the oracle."""
+    from oracle import ewald as oew
+    from profess_b200 import cell as pcell, workloads as wl
+    for c in (wl.fcc_al((2, 1, 1), sigma_ang=0.1, grid=(16, 8, 8), seed=5),
+              wl.hcp_mg((2, 1, 1), sigma_ang=0.05, grid=(12, 6, 10), seed=2)):
+        s = pcell.setup_slot(eng, c)
+        try:
+            e, f = eng.ewald(s, c.nion)
+            eo, fo = oew.ewald(c.lattice, c.frac, c.charges(), True)
+            assert abs(e - eo) < 1e-10 * max(1.0, abs(eo)) and np.abs(f - fo).max() < 1e-10
+            F = eng.forces(s, c.nion, rho=cases.random_density(c.grid, c.num_electrons, c.vol, seed=1))
+            F0 = eng.forces(s, c.nion, rho=cases.random_density(c.grid, c.num_electrons, c.vol, seed=1),
+                            include_ewald=False)
+            assert np.abs((F - F0) - fo).max() < 1e-10
+        finally:
+            eng.slot_destroy(s)
+
+
+def test_device_ewald(emu_engine):
+    check_device_ewald(emu_engine)

@@ -210,3 +210,8 @@ def test_cancel_and_tick_budget_on_gpu(gpu_engine):
         assert st["num_evals"] == r_o.num_evals and abs(e_g[0] - r_o.energy[0]) < 1e-9
     finally:
         gpu_engine.slot_destroy(s)
+
+
+def test_device_ewald_on_gpu(gpu_engine):
+    from test_emu_engine import check_device_ewald
+    check_device_ewald(gpu_engine)

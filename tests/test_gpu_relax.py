@@ -1,0 +1,10 @@
+"""QuickMin relaxation on the CUDA engine against the oracle (GPU)."""
+import pytest
+
+from test_relax import check_quickmin_matches_oracle
+
+pytestmark = pytest.mark.gpu
+
+
+def test_quickmin_matches_oracle_on_gpu(gpu_engine):
+    check_quickmin_matches_oracle(gpu_engine)

@@ -1,0 +1,59 @@
+"""QuickMin relaxation of cells on the engine (profess_b200.relax) against the
+oracle's restatement of QuickMinOptimization (oracle/relax.py), on the
+host-emulation build (CPU); test_gpu_relax.py repeats it on the CUDA build."""
+import numpy as np
+
+from oracle import cellsetup as cs
+from oracle import ntn
+from oracle import relax as orelax
+from profess_b200 import native, relax, workloads as wl
+
+
+def _cell(seed=3, grid=(16, 16, 16)):
+    c = wl.fcc_al((1, 1, 1), sigma_ang=0.1, grid=grid, seed=seed)
+    mx, vals = wl.gha_table(3.0, 1.15, 0.1)
+    ocell = cs.Cell(lattice=c.lattice, frac=c.frac, species_of_ion=c.species_of_ion,
+                    species=[cs.species_from_table(mx, vals, "Al")])
+    return c, ocell
+
+
+def check_quickmin_matches_oracle(eng, max_steps=12):
+    c, ocell = _cell()
+    opts = native.ntn_options(conv_check=native.CONV_POT, pot_tol=1.0e-6)
+    qm = relax.QuickMin(eng, [c], max_steps=max_steps, opts=opts)
+    try:
+        st = qm.run()[0]
+        frac, energy, forces, hist = orelax.quickmin(ocell, c.grid, ntn.NtnOptions(conv_check="POT", pot_tol=1.0e-6),
+                                                     max_steps=max_steps)
+        assert [h["undone"] for h in st.history] == [h[4] for h in hist]
+        assert [h["time_step"] for h in st.history] == [h[3] for h in hist]
+        d = st.cell.frac - frac
+        assert np.abs(d - np.rint(d)).max() < 1e-9
+        assert abs(float(st.energy[0]) - energy) < 1e-8
+        assert np.abs(st.forces - forces).max() < 1e-8
+        # the run takes kept and undone moves, and lowers the largest force
+        assert any(h["undone"] for h in st.history) and not all(h["undone"] for h in st.history)
+        assert st.best_force < 0.5 * st.initial_max_force
+    finally:
+        qm.close()
+
+
+def test_quickmin_matches_oracle(emu_engine):
+    check_quickmin_matches_oracle(emu_engine)
+
+
+def test_quickmin_batch_same_as_alone(emu_engine):
+    cells = [_cell(seed=s, grid=(12, 12, 12))[0] for s in (1, 2)]
+    alone = []
+    for c in cells:
+        q = relax.QuickMin(emu_engine, [c], max_steps=6)
+        st = q.run()[0]
+        alone.append((st.cell.frac.copy(), float(st.energy[0]), [h["time_step"] for h in st.history]))
+        q.close()
+    q = relax.QuickMin(emu_engine, cells, max_steps=6)
+    try:
+        for st, (fr, e, ts) in zip(q.run(), alone):
+            assert np.array_equal(st.cell.frac, fr) and float(st.energy[0]) == e
+            assert [h["time_step"] for h in st.history] == ts
+    finally:
+        q.close()

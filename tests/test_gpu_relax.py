@@ -8,3 +8,8 @@ pytestmark = pytest.mark.gpu
 
 def test_quickmin_matches_oracle_on_gpu(gpu_engine):
     check_quickmin_matches_oracle(gpu_engine)
+
+
+def test_cg2_matches_oracle_on_gpu(gpu_engine):
+    from test_relax import check_cg2_matches_oracle
+    check_cg2_matches_oracle(gpu_engine)

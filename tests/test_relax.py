@@ -57,3 +57,50 @@ def test_quickmin_batch_same_as_alone(emu_engine):
             assert [h["time_step"] for h in st.history] == ts
     finally:
         q.close()
+
+
+# ------------------------------------------------------------------ CG2
+# TOTAL ENERGY lines of the reference's CG2 relaxation of this cell
+# (test/optIon/sampleoutput/displaced.out:123-938), eV: every density solve.
+REF_CG2_TRACE_EV = [-231.1425327622, -231.2770513588, -231.6147260670, -231.6471183146, -231.6860136007,
+                    -231.6996685913, -231.7083720964, -231.7111562797, -231.7116104934, -231.7118205898,
+                    -231.7118261145, -231.7118465883, -231.7118498940]
+
+
+def test_oracle_cg2_reproduces_the_reference_trace():
+    """The oracle's CG2 takes the reference's 13 density solves; their energies
+    agree to 1e-4 eV (each solve converges to dE < 1e-6 Ha)."""
+    import cases
+    from oracle import cg2 as ocg2
+    from oracle.consts import HARTREE_TO_EV
+    cell, f, _, _ = cases.golden_case("wt_al4_displaced")
+    _, trace, _ = ocg2.cg2(cell, f.n, ntn.NtnOptions())
+    assert len(trace) == len(REF_CG2_TRACE_EV)
+    assert np.abs(np.array(trace) * HARTREE_TO_EV - REF_CG2_TRACE_EV).max() < 1e-4
+
+
+def check_cg2_matches_oracle(eng):
+    import cases
+    from oracle import cg2 as ocg2
+    cell, f, _, _ = cases.golden_case("wt_al4_displaced")
+    from profess_b200 import recpot
+    z = np.load(cases.GOLDEN + "/al_hc_recpot.npz")
+    sp = recpot.species_from_table(float(z["max_g"]), z["values"], "Al")
+    c = wl.Cell(name="displaced", lattice=cell.lattice, frac=cell.frac, species_of_ion=cell.species_of_ion,
+                species=[sp], grid=tuple(f.n))
+    run = relax.CG2(eng, [c])
+    try:
+        run.run()
+        frac, trace, forces = ocg2.cg2(cell, f.n, ntn.NtnOptions())
+        assert len(run.traces[0]) == len(trace)
+        assert np.abs(np.array(run.traces[0]) - trace).max() < 1e-9
+        d = run.states[0].cell.frac - frac
+        # the last steps are ~10 bohr per Ha/bohr of force along forces of ~1e-4, so the
+        # positions carry the solves' convergence noise: 3e-8 (fractional) on the emulator
+        assert np.abs(d - np.rint(d)).max() < 2e-7
+    finally:
+        run.close()
+
+
+def test_cg2_matches_oracle(emu_engine):
+    check_cg2_matches_oracle(emu_engine)

@@ -332,6 +332,7 @@ def run_ours(args):
     clocks.start()
     barrier()
     l0, _ = eng.counters()
+    cap0 = eng.capture_stats()
     ev0 = torch.cuda.Event(enable_timing=True)
     ev1 = torch.cuda.Event(enable_timing=True)
     lat = []
@@ -343,6 +344,7 @@ def run_ours(args):
     ev1.record(stream)
     barrier()
     l1, _ = eng.counters()
+    cap1 = eng.capture_stats()
     clk = clocks.stop()
     t_mixed = max_over_ranks(ev0.elapsed_time(ev1) / 1e3)
     value = ws * B * args.steps / t_mixed
@@ -430,6 +432,8 @@ def run_ours(args):
                      if tr else None},
         "cpu_baseline": cpu,
         "clocks": clk,
+        "graph_captures_per_step": {"count": (cap1[0] - cap0[0]) / args.steps,
+                                    "host_ms": (cap1[1] - cap0[1]) / args.steps},
         "gpu_launches": l1 - l0,
     }
     print(json.dumps(out), flush=True)

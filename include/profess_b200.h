@@ -231,6 +231,9 @@ int ofdft_slot_download(ofdft_engine* e, int slot, int which, double* out);
 int ofdft_engine_stream(ofdft_engine* e, void** stream);
 /* Kernel launches and ticks issued so far by this engine. */
 int ofdft_engine_counters(ofdft_engine* e, long long* kernel_launches, long long* ticks);
+/* Graphs captured so far (the task lists changed between runs) and the host
+ * time spent capturing and instantiating them (ms). */
+int ofdft_engine_capture_stats(ofdft_engine* e, long long* captures, double* host_ms);
 /* Mean device time (ms) of one batched potential evaluation over every idle
  * slot with a resident input density, timed with events on the engine stream. */
 int ofdft_engine_time_eval(ofdft_engine* e, int iters, double* ms);

@@ -12,6 +12,7 @@
 // to check the same block functions against the oracle.  The emulation build
 // runs each block with one thread; it is never loaded by the product.
 #include <algorithm>
+#include <chrono>
 #include <cmath>
 #include <cstdio>
 #include <cstdlib>
@@ -1326,7 +1327,16 @@ struct Engine {
 
   // Capture `nticks` ticks into one CUDA graph (re-captured when the set of
   // running slots changes).
+  long long n_captures = 0;
+  double capture_ms = 0.0;  // host time spent capturing and instantiating graphs
   int capture(int nticks) {
+    const auto t0 = std::chrono::steady_clock::now();
+    const int rc0 = capture_graph(nticks);
+    capture_ms += std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+    ++n_captures;
+    return rc0;
+  }
+  int capture_graph(int nticks) {
     if (graph_exec) {
       cudaGraphExecDestroy(graph_exec);
       graph_exec = nullptr;
@@ -1544,6 +1554,18 @@ int ofdft_engine_counters(ofdft_engine* e, long long* kernel_launches, long long
   if (!e) return fail(OFDFT_EINVAL, "null engine");
   if (kernel_launches) *kernel_launches = e->eng.n_launches;
   if (ticks) *ticks = e->eng.n_ticks;
+  return OFDFT_OK;
+}
+
+int ofdft_engine_capture_stats(ofdft_engine* e, long long* captures, double* host_ms) {
+  if (!e) return fail(OFDFT_EINVAL, "null engine");
+#if defined(OFDFT_EMU)
+  if (captures) *captures = 0;
+  if (host_ms) *host_ms = 0.0;
+#else
+  if (captures) *captures = e->eng.n_captures;
+  if (host_ms) *host_ms = e->eng.capture_ms;
+#endif
   return OFDFT_OK;
 }
 

@@ -75,6 +75,7 @@ SIGNATURES = {
     "ofdft_slot_set_ion_potential": [_vp, ctypes.c_int, _dp],
     "ofdft_slot_set_ion_ion_energy": [_vp, ctypes.c_int, ctypes.c_double],
     "ofdft_slot_hold_density": [_vp, ctypes.c_int],
+    "ofdft_engine_capture_stats": [_vp, ctypes.POINTER(ctypes.c_longlong), _dp],
     "ofdft_slot_ewald": [_vp, ctypes.c_int, _dp, _dp],
     "ofdft_slot_build_wt_kernel": [_vp, ctypes.c_int],
     "ofdft_slot_build_wgc_kernel": [_vp, ctypes.c_int, ctypes.c_int, _dp, _dp, _dp, _dp],
@@ -341,6 +342,13 @@ class Engine:
         a, b = ctypes.c_longlong(), ctypes.c_longlong()
         self._check(self.lib.ofdft_engine_counters(self.h, ctypes.byref(a), ctypes.byref(b)))
         return a.value, b.value
+
+    def capture_stats(self):
+        """(graphs captured, host ms spent capturing them)."""
+        n = ctypes.c_longlong()
+        ms = np.zeros(1)
+        self._check(self.lib.ofdft_engine_capture_stats(self.h, ctypes.byref(n), _ptr(ms)))
+        return n.value, float(ms[0])
 
     def time_eval(self, iters=10) -> float:
         ms = np.zeros(1)

@@ -30,18 +30,20 @@ def wgc_tables(lib, alpha: float, beta: float, gamma: float):
 
 
 def setup_slot(eng: native.Engine, cell: Cell, precision=native.FP64, ion_ion=None) -> int:
-    """Create a slot for ``cell`` and build its kernel and ion potential on the device."""
+    """Create a slot for ``cell`` and build its kernel and ion potential on the
+    device; the Ewald energy is summed on the device unless ``ion_ion`` gives it."""
     rho_avg = cell.num_electrons / cell.vol
-    if ion_ion is None:
-        ion_ion = ion_ion_energy(eng.lib, cell)
     s = eng.slot_create(cell.grid, cell.lattice, kinetic=cell.kinetic, alpha=cell.alpha, beta=cell.beta,
-                        gamma=cell.gamma, rho0=rho_avg, rho_s=rho_avg, ion_ion=ion_ion, precision=precision)
+                        gamma=cell.gamma, rho0=rho_avg, rho_s=rho_avg, ion_ion=0.0 if ion_ion is None else ion_ion,
+                        precision=precision)
     try:
         if cell.kinetic == native.KEDF_WT:
             eng.build_wt_kernel(s)
         else:
             eng.build_wgc_kernel(s, wgc_tables(eng.lib, cell.alpha, cell.beta, cell.gamma))
         eng.build_ion_potential(s, cell.frac, cell.species_of_ion, cell.species)
+        if ion_ion is None:
+            eng.ewald(s, cell.nion, want_forces=False)
     except Exception:
         eng.slot_destroy(s)
         raise

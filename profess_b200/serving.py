@@ -4,9 +4,10 @@ Requests (a cell plus solve options) arrive over time; the server admits a
 waiting request when its device footprint fits the HBM budget and engine
 slots are free, builds its tables on the device, and starts its solve in the
 engine, where it shares every kernel launch with the solves already running.
-The host-side inputs of a request (its Ewald energy and initial density) are
-prepared by a small thread pool as soon as it arrives, so the engine keeps
-running the admitted solves meanwhile.
+The host-side input of a request (its initial density) is prepared by a
+small thread pool as soon as it arrives, so the engine keeps running the
+admitted solves meanwhile; its Ewald energy is summed on the device at
+admission.
 A mixed-precision request runs an FP32 slot until the FP32 line-search floor
 (or the FP32 tolerance), then FP64 refinement iterations in an FP64 slot
 started from the FP32 density on the device; a plain request runs FP64
@@ -26,7 +27,7 @@ import time
 import numpy as np
 
 from . import native
-from .cell import setup_slot, ion_ion_energy
+from .cell import setup_slot
 from .workloads import Cell, initial_density
 
 MODE_MIXED = "mixed"
@@ -101,7 +102,7 @@ class Server:
     # ------------------------------------------------------------ admission
     @staticmethod
     def _prepare(lib, req: Request):
-        return ion_ion_energy(lib, req.cell), initial_density(req.cell, seed=req.seed)
+        return initial_density(req.cell, seed=req.seed)
 
     def _arrivals(self):
         t = self.now()
@@ -123,17 +124,18 @@ class Server:
                 return  # its inputs are still being prepared; keep serving the others
             self.waiting.pop(0)
             t_adm = self.now()
-            e_ii, rho0 = fut.result()
+            rho0 = fut.result()
             del self.prep[req.rid]
             st = {"req": req, "need": need, "admitted": t_adm, "phase": None, "s32": None, "s64": None}
             if req.mode == MODE_FP64:
-                st["s64"] = setup_slot(self.eng, req.cell, native.FP64, ion_ion=e_ii)
+                st["s64"] = setup_slot(self.eng, req.cell, native.FP64)  # Ewald summed on the device
                 self.eng.start_solve(st["s64"], rho0, native.ntn_options(
                     conv_check=native.CONV_POT, pot_tol=req.pot_tol, max_iter=300))
                 st["phase"] = "fp64"
             else:
+                st["s64"] = setup_slot(self.eng, req.cell, native.FP64)  # Ewald summed on the device
+                e_ii, _ = self.eng.ewald(st["s64"], req.cell.nion, want_forces=False)
                 st["s32"] = setup_slot(self.eng, req.cell, native.FP32, ion_ion=e_ii)
-                st["s64"] = setup_slot(self.eng, req.cell, native.FP64, ion_ion=e_ii)
                 self.eng.start_solve(st["s32"], rho0, native.ntn_options(
                     conv_check=native.CONV_POT, pot_tol=req.fp32_tol, max_iter=300, stall_line=6))
                 st["phase"] = "fp32"

@@ -215,3 +215,22 @@ def test_cancel_and_tick_budget_on_gpu(gpu_engine):
 def test_device_ewald_on_gpu(gpu_engine):
     from test_emu_engine import check_device_ewald
     check_device_ewald(gpu_engine)
+
+
+def test_repeated_ion_builds_hold_device_memory(gpu_engine):
+    """A geometry loop's ion-potential rebuilds reuse the slot's table buffer:
+    the device's free memory does not shrink over 40 rebuilds."""
+    import torch
+    c = wl.fcc_al((2, 2, 2), sigma_ang=0.05, grid=(48, 48, 48), seed=3)
+    s = pcell.setup_slot(gpu_engine, c)
+    try:
+        gpu_engine.build_ion_potential(s, c.frac, c.species_of_ion, c.species)
+        free0, _ = torch.cuda.mem_get_info()
+        rng = np.random.default_rng(0)
+        for _ in range(40):
+            fr = np.mod(c.frac + rng.normal(0, 1e-3, c.frac.shape), 1.0)
+            gpu_engine.build_ion_potential(s, fr, c.species_of_ion, c.species)
+        free1, _ = torch.cuda.mem_get_info()
+        assert free0 - free1 < 2 << 20
+    finally:
+        gpu_engine.slot_destroy(s)

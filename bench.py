@@ -529,8 +529,8 @@ def run_md(args, ws, rank, local, dist):
 
 
 def run_relax(args, ws, rank, local, dist):
-    """QuickMin relaxation rounds of B cfg2 cells (FP64 solves to potNorm < 1e-6,
-    warm-started); cell-steps/s over the wall clock of the timed rounds."""
+    """QuickMin relaxation of B cfg2 cells in lockstep (FP64 solves to potNorm < 1e-6,
+    warm-started); cell-steps/s over the wall clock of the timed batched steps."""
     import torch
     from profess_b200 import native, relax, workloads as wl
     eng = native.Engine()
@@ -539,12 +539,12 @@ def run_relax(args, ws, rank, local, dist):
     qm = relax.QuickMin(eng, cells, max_steps=args.warmup + args.steps + 1)
     try:
         for _ in range(args.warmup):
-            qm.round()
+            qm.step()
         torch.cuda.synchronize()
         if dist is not None:
             dist.barrier()
         t0 = time.perf_counter()
-        moved = sum(qm.round() for _ in range(args.steps))
+        moved = sum(qm.step() for _ in range(args.steps))
         torch.cuda.synchronize()
         wall = time.perf_counter() - t0
         if dist is not None:

@@ -2,7 +2,7 @@
 
 This is the reference's QuickMin ion optimiser, QuickMinOptimization
 (Source/IonOptQui.f90:33-368), run for a batch of cells in lockstep: every
-round, each cell that is still relaxing takes its own QuickMin move, its ion
+batched step, each cell that is still relaxing takes its own QuickMin move, its ion
 terms are refreshed on the device (B-spline ion potential, Ewald sum), and
 the densities of all moved cells are re-solved together, warm-started from
 each cell's resident density.  Forces then decide, per cell, whether the move
@@ -102,7 +102,7 @@ class QuickMin:
             st.forces = self.eng.forces(st.slot, st.cell.nion, include_ewald=False) + st.f_ewald
             st.num_solves += 1
 
-    def round(self) -> int:
+    def step(self) -> int:
         """One QuickMin step of every cell still relaxing; returns how many moved."""
         moved = []
         for st in self.states:
@@ -162,7 +162,7 @@ class QuickMin:
         return len(moved)
 
     def run(self):
-        while self.round():
+        while self.step():
             pass
         return self.states
 
@@ -322,7 +322,7 @@ def cg2_moves(lattice, frac, energy, forces, force_cutoff=FORCE_CUTOFF, max_step
 
 class CG2:
     """Relax ``cells`` (each gets one FP64 slot) with the CG2 optimiser; every
-    round solves the densities of all cells that asked for one together."""
+    batched step solves the densities of all cells that asked for one together."""
 
     def __init__(self, eng: native.Engine, cells, max_steps: int = 200, force_cutoff: float = FORCE_CUTOFF,
                  opts=None, nn_dist: float = 2.0):
@@ -379,7 +379,7 @@ class CG2:
         _, st.f_ewald = self.eng.ewald(st.slot, st.cell.nion)
         self.eng.start_solve(st.slot, None, self.opts)
 
-    def round(self) -> int:
+    def step(self) -> int:
         """Solve every pending geometry together and advance each optimiser."""
         pending = [k for k, st in enumerate(self.states) if not st.done]
         if not pending:
@@ -392,6 +392,6 @@ class CG2:
         return len(pending)
 
     def run(self):
-        while self.round():
+        while self.step():
             pass
         return self.states

@@ -63,6 +63,19 @@ def _trajectory(lines, rel):
     return rows
 
 
+def _stress_au(lines, rel):
+    """The first STRESS (a.u.) block: rows 'ST_AU  i  s_i1 s_i2 s_i3' (Ha/bohr^3)."""
+    rows, src = [], []
+    for i, ln in enumerate(lines):
+        m = re.match(r"\s*ST_AU\s+(\d)\s+(\S+)\s+(\S+)\s+(\S+)", ln)
+        if m:
+            rows.append([float(m.group(k).replace("D", "E")) for k in (2, 3, 4)])
+            src.append(i + 1)
+            if len(rows) == 3:
+                break
+    return {"value": rows, "source": "%s:%d-%d" % (rel, src[0], src[-1])}
+
+
 def _final_terms(lines, rel, nonlocal_label):
     labels = {"tf": r"Thomas-Fermi Kin\. Energy =\s+(\S+) eV",
               "vw": r"Von-Weizsacker Kin\. Ener =\s+(\S+) eV",
@@ -125,6 +138,7 @@ def main():
         "trajectory": _trajectory(lines, rel),
         "final": {"total": dict(zip(("value_ev", "source"),
                                     _find(lines, r"TOTAL ENERGY =\s+(\S+) eV", rel)))},
+        "stress_au": _stress_au(lines, rel),
     }
     for c in cases.values():
         c["dv"] = dict(zip(("value", "source"), c["dv"])) if "dv" in c else None

@@ -1,0 +1,46 @@
+"""The oracle's stress tensor (oracle/stress.py, CalculateStress restated)
+pinned to the reference's own output for the optCell cell, and checked
+against the finite-difference strain derivative of the converged energy."""
+import dataclasses
+
+import numpy as np
+
+import cases
+from oracle import md as omd
+from oracle import ntn
+from oracle import stress as ost
+
+
+def test_stress_matches_the_reference_output():
+    """test/optCell/sampleoutput/displaced.out:138-140 (ST_AU, Ha/bohr^3), first
+    geometry.  The density is converged as the reference's run converged it
+    (dE < 1e-6 Ha); stress is first order in the density error, and the
+    converged per-term energies of the two runs differ by up to 1e-3 eV, hence
+    1e-7 Ha/bohr^3 (0.08 % of the largest component)."""
+    cell, f, rho_u, c = cases.golden_case("wt_al4_cell")
+    r = ntn.NtnSolver(f).solve(rho_u)
+    s = ost.stress(cell, f, r.rho)
+    ref = np.array(c["stress_au"]["value"])
+    assert np.abs(s - ref).max() < 1e-7
+    assert np.allclose(s, s.T, rtol=0, atol=0)
+
+
+def test_stress_is_the_strain_derivative_of_the_energy():
+    """sigma_ab = (1/V) dE/d(eps_ab) of the variationally converged energy
+    (central differences, eps = 1e-4, ions fixed in fractional coordinates)."""
+    cell, f, rho_u, _ = cases.golden_case("wt_al4_cell")
+    opts = ntn.NtnOptions(conv_check="POT", pot_tol=1e-9, max_iter=500)
+    r = ntn.NtnSolver(f, opts).solve(rho_u)
+    s = ost.stress(cell, f, r.rho)
+
+    def energy(eps):
+        c2 = dataclasses.replace(cell, lattice=(np.eye(3) + eps) @ cell.lattice)
+        f2 = omd.functional_for(c2, f.n, f.alpha, f.beta)
+        return ntn.NtnSolver(f2, opts).solve(r.rho * cell.vol / c2.vol).energy[0]
+
+    h = 1e-4
+    for a, b in [(0, 0), (0, 1), (2, 2)]:
+        e = np.zeros((3, 3))
+        e[a, b] = e[b, a] = h if a == b else h / 2
+        fd = (energy(e) - energy(-e)) / (2 * h) / cell.vol
+        assert abs(fd - s[a, b]) < 1e-8, (a, b, fd, s[a, b])

@@ -283,3 +283,34 @@ def check_device_ewald(eng):
 
 def test_device_ewald(emu_engine):
     check_device_ewald(emu_engine)
+
+
+def test_geometry_loop_calls_check_their_state(emu_engine):
+    """The geometry-loop entry points refuse a slot in the wrong state."""
+    cell, f, rho_u, _ = cases.golden_case("wt_al4_displaced")
+    s = cases.engine_slot(emu_engine, f, cell)  # tables set from the host: no ions known to the slot
+    try:
+        with pytest.raises(native.OfdftError) as ei:
+            emu_engine.ewald(s, 4)
+        assert ei.value.code == 1
+        with pytest.raises(native.OfdftError) as ei:
+            emu_engine.start_solve(s, None)  # no resident input yet
+        assert ei.value.code == 1
+        emu_engine.start_solve(s, rho_u)
+        for call in (lambda: emu_engine.hold_density(s), lambda: emu_engine.ewald(s, 4),
+                     lambda: emu_engine.set_input(s, rho_u)):
+            with pytest.raises(native.OfdftError) as ei:
+                call()
+            assert ei.value.code == 4  # OFDFT_EBUSY while the solve runs
+        emu_engine.cancel(s)
+        emu_engine.hold_density(s)  # idle again: accepted
+    finally:
+        emu_engine.slot_destroy(s)
+
+
+@pytest.mark.parametrize("n", [(1, 16, 16), (16, 16, 1024), (16, 13, 16)])
+def test_grid_limits(emu_engine, n):
+    cell, _, _, _ = cases.golden_case("wt_al4_displaced")
+    with pytest.raises(native.OfdftError) as ei:
+        emu_engine.slot_create(n, cell.lattice)
+    assert ei.value.code == 1

@@ -1,6 +1,7 @@
 """Test infrastructure (the oracle): a CPU restatement of the reference's NVE
-molecular dynamics, RunNVE (Source/MolecularDynamicsNVE.f90:33-323), on the
-oracle's functional, NTN solver and forces.  Only tests import it.
+molecular dynamics, RunNVE (Source/MolecularDynamicsNVE.f90:33-323), and of
+its Nose-Hoover NVT variant, RunNVT (Source/MolecularDynamicsNVT.f90:29-463),
+on the oracle's functional, NTN solver and forces.  Only tests import it.
 
 Per step: RemoveMovementOfCenterOfMass (MolecularDynamics.f90:682-743),
 AdjustCenterOfMass with the shift (MolecularDynamics.f90:1130-1191), half
@@ -90,4 +91,71 @@ def run_nve(cell: cs.Cell, n, vel0: np.ndarray, dt: float, nsteps: int, opts: nt
         vel = vel + forces / m[:, None] * (0.5 * dt)
         out.append(NveState(cell.frac.copy(), cart.copy(), vel.copy(), rho, forces, float(r.energy[0]),
                             ke(vel) + float(r.energy[0])))
+    return out
+
+
+def _yoshida(n):
+    if n == 1:
+        return np.ones(1)
+    if n == 3:
+        w = np.full(3, 1.0 / (2.0 - 2.0 ** (1.0 / 3.0)))
+        w[1] = 1.0 - 2.0 * w[1]
+        return w
+    w = np.full(5, 1.0 / (4.0 - 4.0 ** (1.0 / 3.0)))
+    w[2] = 1.0 - 4.0 * w[2]
+    return w
+
+
+def run_nvt(cell: cs.Cell, n, vel0: np.ndarray, dt: float, nsteps: int, opts: ntn.NtnOptions, q_mass: float,
+            temperature_ha: float, n_resn: int = 3, n_yosh: int = 3, alpha: float = 5.0 / 6.0,
+            beta: float = 5.0 / 6.0):
+    """Nose-Hoover NVT, RunNVT and NHIntegrator (Source/MolecularDynamicsNVT.f90:29-463, 322-399).
+    Returns the list of (frac, vel, energy, conserved) after each step."""
+    cell = dataclasses.replace(cell, frac=np.array(cell.frac, dtype=float))
+    m = np.array([atomic_mass(cell.species[s].name) for s in cell.species_of_ion])
+    linv = np.linalg.inv(cell.lattice)
+    g = 3.0 * len(m)
+    w = _yoshida(n_yosh)
+    rho = cs.uniform_density(cell, *n)
+    r = ntn.NtnSolver(functional_for(cell, n, alpha, beta), opts).solve(rho)
+    rho = r.rho
+    energy = float(r.energy[0])
+    forces, _, _ = ofo.total_forces(cell, rho)
+    vel = np.array(vel0, dtype=float)
+    cart = cell.frac @ cell.lattice.T
+    st = {"x": 0.0, "v": 0.0, "k2": float((m[:, None] * vel * vel).sum())}
+
+    def thermostat(vel):
+        scaling = 1.0
+        gl = (st["k2"] - g * temperature_ha) / q_mass
+        for _ in range(n_resn):
+            for wi in w:
+                wdt2 = wi * dt / (2.0 * n_resn)
+                wdt4 = wi * dt / (4.0 * n_resn)
+                st["v"] += gl * wdt4
+                scaling *= np.exp(-wdt2 * st["v"])
+                gl = (scaling ** 2 * st["k2"] - g * temperature_ha) / q_mass
+                st["x"] += st["v"] * wdt2
+                st["v"] += gl * wdt4
+        st["k2"] *= scaling ** 2
+        return vel * scaling
+
+    out = []
+    for _ in range(nsteps):
+        vel = vel - (m[:, None] * vel).sum(axis=0) / m.sum()
+        cart = cart - (m[:, None] * cart).sum(axis=0) / m.sum()
+        cell.frac = np.mod(cart @ linv.T, 1.0)
+        vel = thermostat(vel)
+        vel = vel + forces / m[:, None] * (0.5 * dt)
+        cart = cart + vel * dt
+        cell.frac = np.mod(cell.frac + (vel * dt) @ linv.T, 1.0)
+        r = ntn.NtnSolver(functional_for(cell, n, alpha, beta), opts).solve(rho)
+        rho = r.rho
+        energy = float(r.energy[0])
+        forces, _, _ = ofo.total_forces(cell, rho)
+        vel = vel + forces / m[:, None] * (0.5 * dt)
+        st["k2"] = float((m[:, None] * vel * vel).sum())
+        vel = thermostat(vel)
+        h = 0.5 * st["k2"] + energy + 0.5 * st["v"] ** 2 * q_mass + g * temperature_ha * st["x"]
+        out.append((cell.frac.copy(), vel.copy(), energy, h))
     return out

@@ -1,4 +1,5 @@
-"""NVE molecular dynamics of many independent cells (replicas) on one engine.
+"""NVE and Nose-Hoover NVT molecular dynamics of many independent cells
+(replicas) on one engine.
 
 This is the reference's velocity-Verlet NVE driver, RunNVE
 (Source/MolecularDynamicsNVE.f90:33-323), run for a batch of replicas in
@@ -171,3 +172,87 @@ class NVE:
     def run(self, nsteps: int):
         for _ in range(nsteps):
             self.step()
+
+
+# ---------------------------------------------------------------------------- NVT
+def yoshida_coefficients(n_yosh: int) -> np.ndarray:
+    """Suzuki-Yoshida weights (MakeIntCoeff, MolecularDynamics.f90:506-540)."""
+    if n_yosh == 1:
+        return np.ones(1)
+    if n_yosh == 3:
+        w = np.full(3, 1.0 / (2.0 - 2.0 ** (1.0 / 3.0)))
+        w[1] = 1.0 - 2.0 * w[1]
+        return w
+    if n_yosh == 5:
+        w = np.full(5, 1.0 / (4.0 - 4.0 ** (1.0 / 3.0)))
+        w[2] = 1.0 - 4.0 * w[2]
+        return w
+    raise ValueError("n_yosh must be 1, 3 or 5")
+
+
+class NVT(NVE):
+    """Lockstep Nose-Hoover NVT dynamics (RunNVT, Source/MolecularDynamicsNVT.f90:29-463):
+    the NVE step with the thermostat integrated over a half step before the
+    first kick and after the second (NHIntegrator: n_resn x n_yosh
+    Suzuki-Yoshida substeps, thermostat mass ``q_mass``, target temperature
+    ``temperature_k``).  The conserved quantity is KE + E + Q v_s^2 / 2 + g T x_s
+    with g = 3 N degrees of freedom."""
+
+    def __init__(self, eng, cells, dt: float, q_mass: float, temperature_k: float, velocities=None, seed: int = 0,
+                 opts=None, rho0=None, n_resn: int = 3, n_yosh: int = 3):
+        super().__init__(eng, cells, dt, velocities=velocities, temperature_k=temperature_k, seed=seed, opts=opts,
+                         rho0=rho0)
+        self.q_mass = float(q_mass)
+        self.t_ha = float(temperature_k) * BOLTZMANN
+        self.n_resn = int(n_resn)
+        self.w = yoshida_coefficients(int(n_yosh))
+        for r in self.reps:
+            r.xlogs = 0.0
+            r.vlogs = 0.0
+            r.twice_ke = 2.0 * r.kinetic_energy()
+
+    def _thermostat(self, r):
+        """NHIntegrator (MolecularDynamicsNVT.f90:322-399)."""
+        g = 3.0 * r.cell.nion
+        scaling = 1.0
+        glogs = (r.twice_ke - g * self.t_ha) / self.q_mass
+        for _ in range(self.n_resn):
+            for w in self.w:
+                wdt2 = w * self.dt / (2.0 * self.n_resn)
+                wdt4 = w * self.dt / (4.0 * self.n_resn)
+                r.vlogs += glogs * wdt4
+                scaling *= np.exp(-wdt2 * r.vlogs)
+                glogs = (scaling * scaling * r.twice_ke - g * self.t_ha) / self.q_mass
+                r.xlogs += r.vlogs * wdt2
+                r.vlogs += glogs * wdt4
+        r.vel *= scaling
+        r.twice_ke *= scaling * scaling
+
+    def conserved_nh(self, r) -> float:
+        g = 3.0 * r.cell.nion
+        return 0.5 * r.twice_ke + float(r.energy[0]) + 0.5 * r.vlogs ** 2 * self.q_mass + g * self.t_ha * r.xlogs
+
+    def step(self):
+        """One NVT step of every replica (MolecularDynamicsNVT.f90:201-300)."""
+        dt = self.dt
+        for r in self.reps:
+            c, m = r.cell, r.mass
+            r.vel -= (m[:, None] * r.vel).sum(axis=0) / m.sum()
+            linv = np.linalg.inv(c.lattice)
+            r.cart -= (m[:, None] * r.cart).sum(axis=0) / m.sum()
+            c.frac = np.mod(r.cart @ linv.T, 1.0)
+            self._thermostat(r)   # with the kinetic energy of the end of the last step, as the reference
+            r.vel += r.forces / m[:, None] * (0.5 * dt)
+            r.cart += r.vel * dt
+            c.frac = np.mod(c.frac + (r.vel * dt) @ linv.T, 1.0)
+            self.eng.hold_density(r.slot)
+            self.eng.build_ion_potential(r.slot, c.frac, c.species_of_ion, c.species)
+            self._refresh_ewald(r)
+            self.eng.start_solve(r.slot, None, self.opts)
+        self._finish_solves()
+        for r in self.reps:
+            r.vel += r.forces / r.mass[:, None] * (0.5 * dt)
+            r.twice_ke = 2.0 * r.kinetic_energy()
+            self._thermostat(r)
+            r.history.append({"energy": float(r.energy[0]), "conserved": self.conserved_nh(r),
+                              "temperature": r.temperature(), "num_evals": r.stats["num_evals"]})

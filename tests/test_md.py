@@ -80,3 +80,31 @@ def test_nve_replicas_batched_as_alone(emu_engine):
             assert np.array_equal(rep.cell.frac, fr) and np.array_equal(rep.vel, v) and float(rep.energy[0]) == e
     finally:
         both.close()
+
+
+def test_nvt_matches_oracle(emu_engine):
+    """Nose-Hoover NVT (RunNVT) on the engine against the oracle's restatement."""
+    c, ocell = _cells()
+    v0 = md.initial_velocities(c, 300.0, seed=7)
+    opts = native.ntn_options(conv_check=native.CONV_POT, pot_tol=1.0e-6)
+    q = 2000.0
+    run = md.NVT(emu_engine, [c], DT, q_mass=q, temperature_k=900.0, velocities=[v0], opts=opts)
+    try:
+        run.run(3)
+        rep = run.reps[0]
+        ref = omd.run_nvt(ocell, c.grid, v0, DT, 3, ntn.NtnOptions(conv_check="POT", pot_tol=1.0e-6), q,
+                          900.0 * md.BOLTZMANN)
+        fr, vel, energy, h = ref[-1]
+        assert np.abs(_wrap(rep.cell.frac - fr)).max() < 1e-10
+        assert np.abs(rep.vel - vel).max() < 1e-10 * np.abs(vel).max()
+        assert abs(float(rep.energy[0]) - energy) < 1e-8
+        assert all(abs(hh["conserved"] - r[3]) < 1e-8 for hh, r in zip(rep.history, ref))
+        # the thermostat heats the 300 K start towards 900 K
+        assert rep.history[-1]["temperature"] > 300.0
+    finally:
+        run.close()
+
+
+def test_yoshida_weights_sum_to_one():
+    for n in (1, 3, 5):
+        assert abs(md.yoshida_coefficients(n).sum() - 1.0) < 1e-15

@@ -83,12 +83,16 @@ def test_nve_replicas_batched_as_alone(emu_engine):
 
 
 def test_nvt_matches_oracle(emu_engine):
+    check_nvt_matches_oracle(emu_engine)
+
+
+def check_nvt_matches_oracle(eng):
     """Nose-Hoover NVT (RunNVT) on the engine against the oracle's restatement."""
     c, ocell = _cells()
     v0 = md.initial_velocities(c, 300.0, seed=7)
     opts = native.ntn_options(conv_check=native.CONV_POT, pot_tol=1.0e-6)
     q = 2000.0
-    run = md.NVT(emu_engine, [c], DT, q_mass=q, temperature_k=900.0, velocities=[v0], opts=opts)
+    run = md.NVT(eng, [c], DT, q_mass=q, temperature_k=900.0, velocities=[v0], opts=opts)
     try:
         run.run(3)
         rep = run.reps[0]

@@ -8,9 +8,7 @@ import pytest
 
 import cases
 from oracle import densityfile as odf
-from oracle import functional as fn
 from profess_b200 import densityfile as df
-from profess_b200 import native
 
 
 def _rho(shape, seed=0):

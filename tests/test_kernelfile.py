@@ -5,7 +5,6 @@ import numpy as np
 
 import cases
 from oracle import cellsetup as cs
-from oracle import functional as fn
 from oracle import kedf_kernels as kk
 from oracle import kernelfile as okf
 from oracle.consts import PI

@@ -2,7 +2,6 @@
 the oracle's restatement of RunNVE (oracle/md.py), on the host-emulation
 build (CPU); test_gpu_md.py repeats them on the CUDA build."""
 import numpy as np
-import pytest
 
 from oracle import cellsetup as cs
 from oracle import md as omd

@@ -63,3 +63,14 @@ def test_solve_resumes_from_a_written_density(emu_engine, tmp_path):
         assert st2["num_evals"] <= st["num_evals"] // 2 and abs(e2[0] - e[0]) < 1e-7
     finally:
         emu_engine.slot_destroy(s)
+
+
+def test_two_spin_file_is_refused(tmp_path):
+    rho = _rho((3, 3, 2))
+    p = str(tmp_path / "s.den")
+    df.write_density(p, rho)
+    raw = bytearray(open(p, "rb").read())
+    raw[27 * 3:27 * 4] = b"# of spins:              2\n"
+    open(p, "wb").write(bytes(raw) + bytes(raw[27 * 4:]))
+    with pytest.raises(ValueError):
+        df.read_density(p, (3, 3, 2), 12, 100.0)

@@ -58,3 +58,12 @@ def test_evaluation_with_a_kernel_file(emu_engine, tmp_path):
         assert abs(e_file[8] - e_built[8]) < 1e-6 * abs(e_built[8])
     finally:
         emu_engine.slot_destroy(s)
+
+
+def test_table_too_short_is_refused(tmp_path):
+    import pytest
+    eta, w = _table(101, eta_max=1.5)
+    p = str(tmp_path / "short.ker")
+    kf.write_wt_kernel_file(p, 1.0, 0.03, eta, w)
+    with pytest.raises(ValueError):
+        kf.wt_kernel_from_file(p, np.array([[[0.5, 4.0]]]), 1.0, 1.0)  # eta = 2 > 1.5

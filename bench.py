@@ -134,7 +134,7 @@ def oracle_functional(cell):
     sys.path.insert(0, os.path.join(ROOT, "tests"))
     from oracle import cellsetup as cs, ewald as ew, functional as fn, kedf_kernels as kk
     from profess_b200 import workloads as wl
-    mx, vals = wl.gha_table(float(cell.species[0].charge), 1.15 if cell.species[0].charge == 3 else 1.3, 0.1)
+    mx, vals = wl.heine_abarenkov_table(float(cell.species[0].charge), 1.15 if cell.species[0].charge == 3 else 1.3, 0.1)
     osp = cs.species_from_table(mx, vals, cell.species[0].name)
     ocell = cs.Cell(lattice=cell.lattice, frac=cell.frac, species_of_ion=cell.species_of_ion, species=[osp])
     n = cell.grid
@@ -179,7 +179,7 @@ def run_reference(args):
            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * tot / args.steps,
            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
            "data": "synthetic (seeded)",
-           "config": {"workload": "FCC Al 4x4x4 (256 atoms), 96^3, WT+TF+vW+LDA, Heine-Abarenkov psp, NTN to potNorm<1e-6",
+           "config": {"workload": "FCC Al 4x4x4 (256 atoms), 96^3, WT+TF+vW+LDA, bare Heine-Abarenkov psp (no GNH smoothing), NTN to potNorm<1e-6",
                       "batch_per_step": 1, "parallelism": "cpu"},
            "cpu_baseline": {"value": v, "unit": UNIT, "cores": cores, "kind": "port",
                             "sample": "%d full FP64 NTN solve(s) of the workload by the oracle "
@@ -194,8 +194,8 @@ def run_reference(args):
 
 # --------------------------------------------------------------------------- GPU arm
 WORKLOADS = {
-    "cfg2": "FCC Al 4x4x4 (256 atoms), a=4.05 A, sigma=0.05 A, 96^3, WT(alpha=beta=5/6)+TF+vW+LDA, Heine-Abarenkov psp",
-    "cfg1": "FCC Al conventional cell (4 atoms), sigma=0.02 A, 32^3, WT+TF+vW+LDA, Heine-Abarenkov psp",
+    "cfg2": "FCC Al 4x4x4 (256 atoms), a=4.05 A, sigma=0.05 A, 96^3, WT(alpha=beta=5/6)+TF+vW+LDA, bare Heine-Abarenkov psp (no GNH smoothing)",
+    "cfg1": "FCC Al conventional cell (4 atoms), sigma=0.02 A, 32^3, WT+TF+vW+LDA, bare Heine-Abarenkov psp (no GNH smoothing)",
     "cfg3": "64 FCC Al cells n^3 (n~U{2..5}, 32-500 atoms), a=4.05 A (1+-2%), 48^3-120^3, WT, one batch",
     "cfg4": "hcp Mg 8x8x9 (1152 atoms), a=3.21 A, c/a=1.624, sigma=0.05 A, 160x160x256, WGC 2nd order",
 }

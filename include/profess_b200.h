@@ -179,9 +179,12 @@ int ofdft_proj_norm_rho_minimization(ofdft_engine* e, int slot, double* rho, dou
  * requests return OFDFT_EINVAL.  rho, kernel (keKernel plane, (n1/2+1,n2,n3)),
  * ion_pot and potential are DEVICE pointers (x-fastest, FP64); etable (9
  * doubles, may be NULL) is host memory; stream is a cudaStream_t or NULL.
- * The first call on a device looks up the array's address (make it before
- * any stream capture).  Calls share the array, so calls whose work overlaps
- * on the GPU race; the call returns after its stream has finished. */
+ * The first call on a device looks up the array's address on that device:
+ * make that first call before any stream capture on the device.  Calls on
+ * one GPU share its array, so calls whose work overlaps on that GPU race;
+ * the host-side staging of a call belongs to the calling thread, so calls
+ * from different host threads on different GPUs do not interfere.  The call
+ * returns after its stream has finished. */
 int ofdft_calculate_potential_plus_noalloc(const ofdft_cell_desc* desc, const double* rho, const double* kernel,
                                            const double* ion_pot, int opt_sqrt, double* potential, double* etable,
                                            void* stream);

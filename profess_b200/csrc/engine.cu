@@ -18,6 +18,7 @@
 #include <cstdlib>
 #include <cstring>
 #include <map>
+#include <mutex>
 #include <string>
 #include <vector>
 
@@ -77,6 +78,37 @@ static int dsync() { return cuda_check(cudaDeviceSynchronize(), "synchronize"); 
 // change costs 2 %: the x passes there are bound by issue, not by banks.)
 static int odd_columns(int nf, int rp, size_t csz) {
   return (csz == 16 && (nf & 1) && !(rp & 1) && rp > 1) ? rp - 1 : rp;
+}
+
+// Launch shape of a slot's passes: row pairs per x-forward task (*rp1) and
+// per x-inverse task (s.rp), and the kx tile widths of the y and z passes
+// (*ty, *tz; s.tx = *ty).  The x-forward tasks carry every field (or ion
+// species) of their row pairs in about 72 KB; the y/z tiles take as many kx
+// columns as fit the two shared buffers of a block (one field of n2 values
+// per column in the y pass, a group of gmax fields of n3 values in the z
+// pass) in about 56 KB, four blocks per SM, and at least 4 columns (rows of
+// 32 or 64 bytes) up to 112 KB per block; two-step lengths take at most
+// 256 / R2 columns, so that the first step's work items (columns x R2) fit
+// the 256 threads of a block in one round.  s needs n1..n3, k1, nf and
+// kinetic; csz is the size of one complex value.
+static void launch_shape(SlotDev& s, size_t csz, int nfx, int* rp1, int* ty, int* tz) {
+  *rp1 = std::max(1, std::min(32, 1024 / s.n1));
+  while (*rp1 > 1 && 2 * (size_t)nfx * *rp1 * s.n1 * csz > 72 * 1024) (*rp1)--;
+  s.rp = std::max(1, std::min(32, 1024 / s.n1));
+  while (s.rp > 1 && 2 * (size_t)s.nf * s.rp * s.n1 * csz > 72 * 1024) s.rp--;
+  *rp1 = odd_columns(s.nf, *rp1, csz);
+  s.rp = odd_columns(s.nf, s.rp, csz);
+  const int gmax = s.kinetic == KIN_WGC ? 3 : 1;
+  auto width = [&](size_t per_col) {
+    size_t w = std::min<size_t>((size_t)s.k1, (56 * 1024) / per_col);
+    if (w < 4) w = std::min<size_t>((size_t)s.k1, std::max<size_t>(1, std::min<size_t>(4, (112 * 1024) / per_col)));
+    return (int)std::max<size_t>(1, w);
+  };
+  *ty = width(2 * (size_t)s.n2 * csz);
+  *tz = width(2 * (size_t)gmax * s.n3 * csz);
+  if (fft2_r2(s.n2) > 0) *ty = std::max(1, std::min(*ty, 256 / fft2_r2(s.n2)));
+  if (fft2_r2(s.n3) > 0) *tz = std::max(1, std::min(*tz, 256 / (gmax * fft2_r2(s.n3))));
+  s.tx = *ty;
 }
 
 // ------------------------------------------------------------ FFT plans
@@ -520,32 +552,7 @@ struct Engine {
     const long long nrows = (long long)s.n2 * s.n3;
     h.nrowpairs = (int)((nrows + 1) / 2);
     const size_t csz = 2 * elem_size(h.prec);
-    // tile sizes: about 1-2 K complex points per block, at most ~100 KB of shared memory
-    // x-forward tasks: every field (or species) of rp1 row pairs, in about 72 KB
-    const int nfx = std::max(s.nf, MAX_SPECIES);
-    h.rp1 = std::max(1, std::min(32, 1024 / s.n1));
-    while (h.rp1 > 1 && 2 * (size_t)nfx * h.rp1 * s.n1 * csz > 72 * 1024) h.rp1--;
-    s.rp = std::max(1, std::min(32, 1024 / s.n1));
-    while (s.rp > 1 && 2 * (size_t)s.nf * s.rp * s.n1 * csz > 72 * 1024) s.rp--;
-    h.rp1 = odd_columns(s.nf, h.rp1, csz);
-    s.rp = odd_columns(s.nf, s.rp, csz);
-    // y/z tiles: as many kx columns as fit the two shared buffers of a block
-    // (one field of n2 values per column in the y pass, a group of gmax
-    // fields of n3 values in the z pass) in about 56 KB, four blocks per SM;
-    // at least 4 columns (rows of 32 or 64 bytes) up to 112 KB per block.
-    const int gmax = s.kinetic == KIN_WGC ? 3 : 1;
-    auto width = [&](size_t per_col) {
-      size_t w = std::min<size_t>((size_t)s.k1, (56 * 1024) / per_col);
-      if (w < 4) w = std::min<size_t>((size_t)s.k1, std::max<size_t>(1, std::min<size_t>(4, (112 * 1024) / per_col)));
-      return (int)std::max<size_t>(1, w);
-    };
-    h.ty = width(2 * (size_t)s.n2 * csz);
-    h.tz = width(2 * (size_t)gmax * s.n3 * csz);
-    // two-step lengths: at most 256 / R2 columns, so that the first step's
-    // work items (columns x R2) fit the 256 threads of a block in one round
-    if (fft2_r2(s.n2) > 0) h.ty = std::max(1, std::min(h.ty, 256 / fft2_r2(s.n2)));
-    if (fft2_r2(s.n3) > 0) h.tz = std::max(1, std::min(h.tz, 256 / (gmax * fft2_r2(s.n3))));
-    s.tx = h.ty;
+    launch_shape(s, csz, std::max(s.nf, MAX_SPECIES), &h.rp1, &h.ty, &h.tz);
     s.ntask[K_VEC] = (int)((s.N + VCHUNK - 1) / VCHUNK);
     s.ntask[K_X5] = (h.nrowpairs + s.rp - 1) / s.rp;
     // buffers
@@ -1785,23 +1792,40 @@ int ofdft_wgc_radial_tables(double alpha, double beta, double gamma, int max, do
 // twiddles, spectra, reduction partials and task lists) lives in the
 // file-scope device array below.  Every GPU that loads this library holds
 // the array until the process exits.  Calls share it, so two calls whose
-// work overlaps on the GPU race; each call rewrites everything it reads.
+// work overlaps on the same GPU race; each call rewrites everything it reads.
+// The host-side staging (task lists, twiddles, controller record) belongs to
+// the calling thread, so calls from different host threads on different
+// GPUs are independent.
 #if !defined(OFDFT_EMU)
 namespace noalloc {
 constexpr size_t SCRATCH_BYTES = size_t(12) << 20;  // 12 MiB
 constexpr long long MAX_POINTS = 262144;             // 64^3 grid points
 constexpr int MAX_DIM = 128;
 constexpr int MAX_TASKS = 12288;
+constexpr int MAX_DEVICES = 128;
 static __device__ __align__(256) unsigned char g_scratch[SCRATCH_BYTES];
-static void* g_addr[128];                  // device address of g_scratch per device ordinal
-static Task g_tasks[MAX_TASKS];            // host staging of the task lists
-static cx<double> g_tw[4 * MAX_DIM];       // host staging of the twiddles
-static Ctl g_ctl;
+static void* g_addr[MAX_DEVICES];  // device address of g_scratch per device ordinal
+static std::mutex g_addr_mu;       // guards the first look-up on each device
+static thread_local Task t_tasks[MAX_TASKS];  // this thread's staging of the task lists
+
+// The device address of g_scratch on the current device (looked up once per
+// device, with that device current).
+static int scratch_address(int dev, char** base) {
+  std::lock_guard<std::mutex> lock(g_addr_mu);
+  if (!g_addr[dev]) {
+    void* a = nullptr;
+    const int rc = cuda_check(cudaGetSymbolAddress(&a, g_scratch), "cudaGetSymbolAddress");
+    if (rc) return rc;
+    g_addr[dev] = a;
+  }
+  *base = (char*)g_addr[dev];
+  return OFDFT_OK;
+}
 
 static size_t up256(size_t x) { return (x + 255) & ~size_t(255); }
 
-// Plan of length n with twiddles appended to g_tw at offset *off (no heap use).
-static void make_plan(int n, FftPlan& p, int* off) {
+// Plan of length n with twiddles appended to tw at offset *off (no heap use).
+static void make_plan(int n, FftPlan& p, cx<double>* tw, int* off) {
   memset(&p, 0, sizeof(p));
   p.n = n;
   p.root = -1;
@@ -1825,7 +1849,7 @@ static void make_plan(int n, FftPlan& p, int* off) {
       for (int j = 1; j < R; ++j) {
         const long double a = -2.0L * 3.141592653589793238462643383279502884L * (long double)(j * k) /
                               (long double)(ns * R);
-        g_tw[*off + o++] = mk<double>((double)cosl(a), (double)sinl(a));
+        tw[*off + o++] = mk<double>((double)cosl(a), (double)sinl(a));
       }
     ns *= R;
   }
@@ -1852,18 +1876,8 @@ extern "C" int ofdft_calculate_potential_plus_noalloc(const ofdft_cell_desc* d, 
   const long long N = (long long)d->n1 * d->n2 * d->n3;
   if (N > MAX_POINTS)
     return fail(OFDFT_EINVAL, "grid too large for the allocation-free evaluation (at most 262144 points)");
-  cudaStream_t st = (cudaStream_t)stream_ptr;
-  int dev = 0;
-  int rc = cuda_check(cudaGetDevice(&dev), "cudaGetDevice");
-  if (rc) return rc;
-  if (dev < 0 || dev >= 128) return fail(OFDFT_EINVAL, "device ordinal out of range");
-  if (!g_addr[dev]) {  // once per device, with that device current
-    void* a = nullptr;
-    if ((rc = cuda_check(cudaGetSymbolAddress(&a, g_scratch), "cudaGetSymbolAddress"))) return rc;
-    g_addr[dev] = a;
-  }
-  char* base = (char*)g_addr[dev];
-
+  // Host planning first (descriptor, plans, task lists, scratch layout): a
+  // grid the fixed scratch cannot hold is refused before any CUDA call.
   // slot descriptor (as ofdft_slot_create fills it) pointing at the caller's buffers
   SlotDev s;
   memset(&s, 0, sizeof(s));
@@ -1871,10 +1885,11 @@ extern "C" int ofdft_calculate_potential_plus_noalloc(const ofdft_cell_desc* d, 
   s.k1 = d->n1 / 2 + 1;
   s.N = N;
   s.Nc = (long long)s.k1 * d->n2 * d->n3;
+  cx<double> tw[4 * MAX_DIM];  // twiddles of the three plans (n - 1 per plan)
   int twoff = 0;
-  make_plan(d->n1, s.px, &twoff);
-  make_plan(d->n2, s.py, &twoff);
-  make_plan(d->n3, s.pz, &twoff);
+  make_plan(d->n1, s.px, tw, &twoff);
+  make_plan(d->n2, s.py, tw, &twoff);
+  make_plan(d->n3, s.pz, tw, &twoff);
   const double* L = d->lattice;
   auto A = [&](int r, int c) { return L[3 * c + r]; };
   const double det = A(0, 0) * (A(1, 1) * A(2, 2) - A(1, 2) * A(2, 1)) - A(0, 1) * (A(1, 0) * A(2, 2) - A(1, 2) * A(2, 0)) +
@@ -1906,14 +1921,8 @@ extern "C" int ofdft_calculate_potential_plus_noalloc(const ofdft_cell_desc* d, 
   for (int g = 0; g < s.ngroups; ++g) { s.group_kind[g] = kinds[g]; s.group_f0[g] = g; s.group_nf[g] = 1; }
   const size_t cs = sizeof(cx<double>);
   const int nrows = s.n2 * s.n3, nrp = (nrows + 1) / 2;
-  int rp1 = std::max(1, std::min(32, 1024 / s.n1));
-  while (rp1 > 1 && 2 * (size_t)s.nf * rp1 * s.n1 * cs > 72 * 1024) rp1--;
-  s.rp = std::max(1, std::min(32, 1024 / s.n1));
-  while (s.rp > 1 && 2 * (size_t)s.nf * s.rp * s.n1 * cs > 72 * 1024) s.rp--;
-  rp1 = odd_columns(s.nf, rp1, cs);
-  s.rp = odd_columns(s.nf, s.rp, cs);
-  s.tx = 16;
-  while (s.tx > 2 && 2 * (size_t)s.tx * std::max(s.n2, s.n3) * cs > 100 * 1024) s.tx /= 2;
+  int rp1 = 1, ty = 1, tz = 1;
+  launch_shape(s, cs, s.nf, &rp1, &ty, &tz);  // the engine's own launch shape
   s.ntask[K_X5] = (nrp + s.rp - 1) / s.rp;
   s.buf[B_PHI] = (void*)rho;         // the input density (read only in EV_RHO mode)
   s.buf[B_W0] = (void*)potential;    // the output potential
@@ -1923,7 +1932,7 @@ extern "C" int ofdft_calculate_potential_plus_noalloc(const ofdft_cell_desc* d, 
   int nt[6] = {0, 0, 0, 0, 0, 0}, ntot = 0;
   auto push = [&](int pass, Task t) -> bool {
     if (ntot >= MAX_TASKS) return false;
-    g_tasks[ntot++] = t;
+    t_tasks[ntot++] = t;
     nt[pass]++;
     return true;
   };
@@ -1931,10 +1940,10 @@ extern "C" int ofdft_calculate_potential_plus_noalloc(const ofdft_cell_desc* d, 
   for (int r = 0; r < nrp && ok; r += rp1) ok = push(0, {0, 0, r, std::min(rp1, nrp - r)});
   for (int f = 0; f < s.nf && ok; ++f)
     for (int z = 0; z < s.n3 && ok; ++z)
-      for (int t = 0; t < tile_count(s.k1, s.tx) && ok; ++t) ok = push(1, {0, f, z, tile_code(s.k1, s.tx, t)});
+      for (int t = 0; t < tile_count(s.k1, ty) && ok; ++t) ok = push(1, {0, f, z, tile_code(s.k1, ty, t)});
   for (int g = 0; g < s.ngroups && ok; ++g)
     for (int ky = 0; ky < s.n2 && ok; ++ky)
-      for (int t = 0; t < tile_count(s.k1, s.tx) && ok; ++t) ok = push(2, {0, g, ky, tile_code(s.k1, s.tx, t)});
+      for (int t = 0; t < tile_count(s.k1, tz) && ok; ++t) ok = push(2, {0, g, ky, tile_code(s.k1, tz, t)});
   int ord = 0;
   for (int r = 0; r < nrp && ok; r += s.rp) ok = push(3, {0, r, std::min(s.rp, nrp - r), ord++});
   if (ok) ok = push(4, {0, 0, 0, 0});
@@ -1948,22 +1957,30 @@ extern "C" int ofdft_calculate_potential_plus_noalloc(const ofdft_cell_desc* d, 
   const size_t o_task = o; o = up256(o + sizeof(Task) * (size_t)ntot);
   const size_t o_spec = o; o = up256(o + cs * (size_t)s.nf * (size_t)s.Nc);
   if (o > SCRATCH_BYTES) return fail(OFDFT_EINVAL, "grid needs more scratch than the allocation-free evaluation holds");
+  cudaStream_t st = (cudaStream_t)stream_ptr;
+  int dev = 0;
+  int rc = cuda_check(cudaGetDevice(&dev), "cudaGetDevice");
+  if (rc) return rc;
+  if (dev < 0 || dev >= MAX_DEVICES) return fail(OFDFT_EINVAL, "device ordinal out of range");
+  char* base = nullptr;
+  if ((rc = scratch_address(dev, &base))) return rc;
   s.partials = (double*)(base + o_part);
   s.spec = (void*)(base + o_spec);
-  memset(&g_ctl, 0, sizeof(g_ctl));
-  g_ctl.status = ST_RUNNING;
-  g_ctl.iphi = B_PHI; g_ctl.itrial = B_TRIAL; g_ctl.iw0 = B_W0; g_ctl.iw1 = B_W1; g_ctl.evb = B_P;
-  g_ctl.ev = EV_RHO;
-  g_ctl.opt_sqrt = opt_sqrt ? 1 : 0;
-  g_ctl.want_energy = etable ? 1 : 0;
-  g_ctl.dscale = 1.0;
+  Ctl ctl;
+  memset(&ctl, 0, sizeof(ctl));
+  ctl.status = ST_RUNNING;
+  ctl.iphi = B_PHI; ctl.itrial = B_TRIAL; ctl.iw0 = B_W0; ctl.iw1 = B_W1; ctl.evb = B_P;
+  ctl.ev = EV_RHO;
+  ctl.opt_sqrt = opt_sqrt ? 1 : 0;
+  ctl.want_energy = etable ? 1 : 0;
+  ctl.dscale = 1.0;
   if ((rc = cuda_check(cudaMemcpyAsync(base + o_slot, &s, sizeof(SlotDev), cudaMemcpyHostToDevice, st), "H2D")))
     return rc;
-  if ((rc = cuda_check(cudaMemcpyAsync(base + o_ctl, &g_ctl, sizeof(Ctl), cudaMemcpyHostToDevice, st), "H2D")))
+  if ((rc = cuda_check(cudaMemcpyAsync(base + o_ctl, &ctl, sizeof(Ctl), cudaMemcpyHostToDevice, st), "H2D")))
     return rc;
-  if ((rc = cuda_check(cudaMemcpyAsync(base + o_tw, g_tw, cs * (size_t)twoff, cudaMemcpyHostToDevice, st), "H2D")))
+  if ((rc = cuda_check(cudaMemcpyAsync(base + o_tw, tw, cs * (size_t)twoff, cudaMemcpyHostToDevice, st), "H2D")))
     return rc;
-  if ((rc = cuda_check(cudaMemcpyAsync(base + o_task, g_tasks, sizeof(Task) * (size_t)ntot, cudaMemcpyHostToDevice,
+  if ((rc = cuda_check(cudaMemcpyAsync(base + o_task, t_tasks, sizeof(Task) * (size_t)ntot, cudaMemcpyHostToDevice,
                                        st), "H2D")))
     return rc;
   // launches: passes 1-5 and the controller kernel, as one engine tick does
@@ -1973,8 +1990,8 @@ extern "C" int ofdft_calculate_potential_plus_noalloc(const ofdft_cell_desc* d, 
   a.tw = (const cx<double>*)(base + o_tw);
   a.vchunk = VCHUNK;
   const size_t sm1 = 2 * (size_t)s.nf * rp1 * s.n1 * cs;
-  const size_t sm2 = 2 * (size_t)s.tx * s.n2 * cs;
-  const size_t sm3 = 2 * (size_t)s.tx * s.n3 * cs;
+  const size_t sm2 = 2 * (size_t)ty * s.n2 * cs;
+  const size_t sm3 = 2 * (size_t)tz * s.n3 * cs;
   const size_t sm5 = 2 * (size_t)s.nf * s.rp * s.n1 * cs + NCH * 33 * sizeof(double) + 16;
   auto attr = [&](auto kern, size_t sm) -> int {
     if (sm <= 48 * 1024) return OFDFT_OK;
@@ -1998,12 +2015,12 @@ extern "C" int ofdft_calculate_potential_plus_noalloc(const ofdft_cell_desc* d, 
   a.tasks = tb + nt[0] + nt[1] + nt[2] + nt[3];
   k_ctl<double><<<1, 64, 0, st>>>(a, (int)K_X5);
   if ((rc = cuda_check(cudaGetLastError(), "kernel launch"))) return rc;
-  if ((rc = cuda_check(cudaMemcpyAsync(&g_ctl, base + o_ctl, sizeof(Ctl), cudaMemcpyDeviceToHost, st), "D2H")))
+  if ((rc = cuda_check(cudaMemcpyAsync(&ctl, base + o_ctl, sizeof(Ctl), cudaMemcpyDeviceToHost, st), "D2H")))
     return rc;
   if ((rc = cuda_check(cudaStreamSynchronize(st), "stream synchronize"))) return rc;
-  if ((rc = status_code(g_ctl))) return rc;
+  if ((rc = status_code(ctl))) return rc;
   if (etable)
-    for (int k = 0; k < 9; ++k) etable[k] = g_ctl.energy[k];
+    for (int k = 0; k < 9; ++k) etable[k] = ctl.energy[k];
   return OFDFT_OK;
 #endif
 }

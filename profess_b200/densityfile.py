@@ -24,14 +24,27 @@ RECL = 27
 _LABELS = ("x-dimension:", "y-dimension:", "z-dimension:", "# of spins: ")
 
 
+# Smallest magnitude the two-digit exponent of E26.20 holds (.1E-98); smaller
+# values are written as zero so that every record keeps RECL characters.
+_E26_MIN = 1.0e-99
+
+
 def _e26_20(x: float) -> str:
-    """x in Fortran E26.20 form: sign, '.', 20 digits, 'E', sign, 2 digits (no leading 0)."""
-    if x == 0.0:
+    """x in Fortran E26.20 form: sign, '.', 20 digits, 'E', sign, 2 digits (no leading 0).
+
+    Values below 1e-99 in magnitude (a vacuum region's density) are written as
+    zero; a non-finite value or one of 1e99 or more raises ValueError, since
+    either would break the fixed record length."""
+    if not math.isfinite(x):
+        raise ValueError("non-finite density value %r cannot be written in E26.20" % x)
+    if abs(x) < _E26_MIN:
         return " .00000000000000000000E+00"
     s = "%.19e" % abs(x)                  # d.dddddddddddddddddddde[+-]XX
     mant, ex = s.split("e")
     digits = mant.replace(".", "")
     e = int(ex) + 1
+    if abs(e) > 99:
+        raise ValueError("density value %r is outside the E26.20 exponent range" % x)
     body = ".%sE%s%02d" % (digits, "-" if e < 0 else "+", abs(e))
     return ("-" if x < 0 else " ") + body
 

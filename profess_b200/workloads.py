@@ -2,18 +2,19 @@
 
 All inputs are generated, none are read from a dataset:
 
-* ``gha_species``: the Heine-Abarenkov model potential (V. Heine and
-  I. Abarenkov, Phil. Mag. 9, 451 (1964)) that the Goodwin-Heine-Abarenkov
-  local pseudopotential is built on: a constant well of depth A inside the
-  model radius r_c and the bare Coulomb tail -Z/r outside it.  Its transform
-  is analytic, v(q) = -(4 pi / q^2) [Z cos(q r_c) + (A/q)(sin(q r_c) -
-  q r_c cos(q r_c))], with the finite q -> 0 part 2 pi Z r_c^2 -
+* ``heine_abarenkov_species``: the bare Heine-Abarenkov model potential (V.
+  Heine and I. Abarenkov, Phil. Mag. 9, 451 (1964)): a constant well of depth
+  A inside the model radius r_c and the bare Coulomb tail -Z/r outside it.
+  The benchmark configurations name a Goodwin-Heine-Abarenkov potential;
+  these cells use the bare model potential that it is built on, without the
+  Goodwin-Needs-Heine smoothing, with the configurations' Z, r_c and A.  Its
+  transform is analytic, v(q) = -(4 pi / q^2) [Z cos(q r_c) + (A/q)(sin(q r_c)
+  - q r_c cos(q r_c))], with the finite q -> 0 part 2 pi Z r_c^2 -
   4 pi A r_c^3 / 3 stored at q = 0.  It is tabulated as a recpot table (q
   spacing 0.002 bohr^-1 up to 30 bohr^-1, as in al_HC.lda.recpot), so the
   recpot reader's charge inference recovers Z from the -4 pi Z / q^2 tail.
-  (The smoothing that Goodwin, Needs and Heine add on top was not available
-  offline; the shallow well already keeps the valence density smooth at the
-  cores, which the second-order WGC expansion needs.)
+  The shallow well keeps the valence density smooth at the cores, which the
+  second-order WGC expansion needs.
 * ``fcc_al``: FCC aluminium supercells of the 4-atom conventional cell.
 * ``hcp_mg``: hexagonal magnesium supercells of the 2-atom primitive cell.
 * ``Cell``: lattice (bohr, columns = lattice vectors), fractional positions,
@@ -58,14 +59,14 @@ class Cell:
         return np.array([self.species[s].charge for s in self.species_of_ion], dtype=float)
 
 
-_GHA_CACHE = {}
+_HA_CACHE = {}
 
 
-def gha_table(z: float, rc: float, a_well: float, dq: float = 0.002, npts: int = 15003):
+def heine_abarenkov_table(z: float, rc: float, a_well: float, dq: float = 0.002, npts: int = 15003):
     """(max_g in 1/A, values in eV*A^3) of the Heine-Abarenkov model potential."""
     key = (z, rc, a_well, dq, npts)
-    if key in _GHA_CACHE:
-        return _GHA_CACHE[key]
+    if key in _HA_CACHE:
+        return _HA_CACHE[key]
     q = np.arange(npts, dtype=float) * dq
     vals = np.empty(npts)
     vals[0] = 2.0 * math.pi * z * rc ** 2 - 4.0 * math.pi * a_well * rc ** 3 / 3.0
@@ -74,23 +75,23 @@ def gha_table(z: float, rc: float, a_well: float, dq: float = 0.002, npts: int =
     vals[1:] = -(4.0 * math.pi / qq ** 2) * (z * np.cos(x) + (a_well / qq) * (np.sin(x) - x * np.cos(x)))
     max_g_ang = (npts - 1) * dq / BOHR
     out = (max_g_ang, vals * BOHR ** 3 * HARTREE_TO_EV)
-    _GHA_CACHE[key] = out
+    _HA_CACHE[key] = out
     return out
 
 
-def gha_species(name: str, z: int, rc: float, a_well: float = 0.1) -> Species:
-    max_g, vals = gha_table(float(z), rc, a_well)
+def heine_abarenkov_species(name: str, z: int, rc: float, a_well: float = 0.1) -> Species:
+    max_g, vals = heine_abarenkov_table(float(z), rc, a_well)
     return species_from_table(max_g, vals, name)
 
 
 def al_species() -> Species:
     """Al: Z = 3, r_c = 1.15 bohr, A = 0.1 Ha."""
-    return gha_species("Al", 3, 1.15, 0.1)
+    return heine_abarenkov_species("Al", 3, 1.15, 0.1)
 
 
 def mg_species() -> Species:
     """Mg: Z = 2, r_c = 1.3 bohr, A = 0.1 Ha."""
-    return gha_species("Mg", 2, 1.3, 0.1)
+    return heine_abarenkov_species("Mg", 2, 1.3, 0.1)
 
 
 def smooth_size(m: float) -> int:

@@ -89,3 +89,21 @@ def engine_slot(eng, f, cell, precision=0):
     eng.set_kernel(s, f.kernel)
     eng.set_ion_potential(s, f.ion_pot)
     return s
+
+
+def oracle_cell(c):
+    """Oracle cell of a synthetic workload cell (profess_b200.workloads.Cell):
+    the same lattice, ions and Heine-Abarenkov tables."""
+    from profess_b200 import workloads as wl
+    sp = c.species[0]
+    rc = 1.15 if sp.charge == 3 else 1.3
+    mx, vals = wl.heine_abarenkov_table(float(sp.charge), rc, 0.1)
+    return cs.Cell(lattice=c.lattice, frac=c.frac, species_of_ion=c.species_of_ion,
+                   species=[cs.species_from_table(mx, vals, sp.name)])
+
+
+def workload_functional(c):
+    """(oracle cell, oracle functional) of a synthetic workload cell, with the
+    product set-up's reference densities (rho0 = rho* = N_e / V)."""
+    oc = oracle_cell(c)
+    return oc, functional_for(oc, c.grid, c.kinetic, c.alpha, c.beta, gamma=c.gamma)

@@ -1,25 +1,27 @@
 """Generate the golden fixtures from the reference's own test runs.
 
 Reads the input geometries, the Al pseudopotential table and the printed
-energy/trajectory tables of the reference's shipped sample outputs under
-``/root/reference/test`` and writes them as small fixtures next to this file:
+energy/trajectory tables of the reference's shipped sample outputs (its
+``test`` directory) and writes them as small fixtures next to this file:
 
   ref_cases.json     geometries, KEDF parameters and golden numbers (with the
                      source file:line of every number)
   al_hc_recpot.npz   the al_HC.lda.recpot table (maxG in 1/A, values in eV*A^3)
 
 The fixtures are committed so that tests never need the reference tree.
-Run:  python tests/golden/make_fixtures.py
+Run:  python tests/golden/make_fixtures.py REFERENCE_ROOT
+(or set PROFESS_REFERENCE to the root of the reference's source tree).
 """
 from __future__ import annotations
 
 import json
 import os
 import re
+import sys
 
 import numpy as np
 
-REF = "/root/reference/test"
+REF = None  # the reference's test directory, set by main()
 HERE = os.path.dirname(os.path.abspath(__file__))
 
 
@@ -92,7 +94,12 @@ def _final_terms(lines, rel, nonlocal_label):
     return out
 
 
-def main():
+def main(root=None):
+    global REF
+    root = root or os.environ.get("PROFESS_REFERENCE")
+    if not root:
+        raise SystemExit("usage: make_fixtures.py REFERENCE_ROOT (or set PROFESS_REFERENCE)")
+    REF = os.path.join(root, "test")
     cases = {}
     # WT: displaced Al4 (first density solve of the ion relaxation)
     rel = "test/optIon/sampleoutput/displaced.out"
@@ -163,4 +170,4 @@ def main():
 
 
 if __name__ == "__main__":
-    main()
+    main(sys.argv[1] if len(sys.argv) > 1 else None)

@@ -37,6 +37,28 @@ def test_e26_20_matches_fortran_form():
     assert float(df._e26_20(1.0 / 3.0)) == 1.0 / 3.0
 
 
+def test_records_keep_their_length_at_the_exponent_limits(tmp_path):
+    """A vacuum value below 1e-99 is written as zero (a three-digit exponent
+    would lengthen the record); values that E26.20 cannot hold are refused."""
+    assert df._e26_20(1e-120) == " .00000000000000000000E+00"
+    assert df._e26_20(-3e-100) == " .00000000000000000000E+00"
+    assert df._e26_20(1e-99).endswith("E-98") and float(df._e26_20(1e-99)) == 1e-99
+    rho = _rho((3, 2, 2), seed=2)
+    rho[1, 0, 0] = 1e-130
+    p = str(tmp_path / "v.den")
+    df.write_density(p, rho)
+    assert len(open(p, "rb").read()) == df.RECL * (4 + rho.size)
+    back = df.read_density_file(p)[..., 0]
+    assert back[1, 0, 0] == 0.0 and np.array_equal(np.delete(back.ravel(order="F"), 1),
+                                                    np.delete(rho.ravel(order="F"), 1))
+    for bad in (np.nan, np.inf, -np.inf, 2e99):
+        with pytest.raises(ValueError):
+            df._e26_20(bad)
+        rho[0, 1, 0] = bad
+        with pytest.raises(ValueError):
+            df.write_density(str(tmp_path / "bad.den"), rho)
+
+
 @pytest.mark.parametrize("grid,repeat", [((5, 4, 3), (1, 1, 1)), ((10, 4, 6), (2, 1, 2)),
                                          ((8, 7, 6), (1, 1, 1)), ((9, 4, 5), (2, 1, 1))])
 def test_read_matches_oracle(tmp_path, grid, repeat):

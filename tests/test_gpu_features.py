@@ -60,7 +60,7 @@ def test_large_and_odd_plans(gpu_engine, n):
 def test_wgc_hcp_cell(gpu_engine):
     """WGC on a non-orthogonal (120 degree) hcp Mg cell."""
     c = wl.hcp_mg((2, 2, 2), sigma_ang=0.05, grid=(24, 24, 40), seed=3)
-    mx, vals = wl.gha_table(2.0, 1.3, 0.1)
+    mx, vals = wl.heine_abarenkov_table(2.0, 1.3, 0.1)
     ocell = cs.Cell(lattice=c.lattice, frac=c.frac, species_of_ion=c.species_of_ion,
                     species=[cs.species_from_table(mx, vals, "Mg")])
     f = cases.functional_for(ocell, c.grid, fn.KEDF_WGC, c.alpha, c.beta)
@@ -81,7 +81,7 @@ def test_workload_cfg1_solve(gpu_engine):
     the ion structure factor with atomic adds, so its ion potential differs from
     the oracle's in the last bits and the energies agree to 1e-8 Ha, not 1e-10."""
     c = wl.config_cell(1)
-    mx, vals = wl.gha_table(3.0, 1.15, 0.1)
+    mx, vals = wl.heine_abarenkov_table(3.0, 1.15, 0.1)
     ocell = cs.Cell(lattice=c.lattice, frac=c.frac, species_of_ion=c.species_of_ion,
                     species=[cs.species_from_table(mx, vals, "Al")])
     f = cases.functional_for(ocell, c.grid, fn.KEDF_WT, 5 / 6, 5 / 6)

@@ -1,5 +1,5 @@
 """Host-side set-up logic against the oracle (CPU): grid sizing, recpot
-reading, the GHA workload tables, Ewald, the WGC kernel ODE, footprints."""
+reading, the Heine-Abarenkov workload tables, Ewald, the WGC kernel ODE, footprints."""
 import numpy as np
 import pytest
 
@@ -39,8 +39,8 @@ def test_recpot_reader_matches_oracle():
 
 
 def test_recpot_text_round_trip():
-    mx, vals = wl.gha_table(2.0, 1.3, 0.1)
-    text = recpot.format_recpot(mx, vals, "GHA Mg")
+    mx, vals = wl.heine_abarenkov_table(2.0, 1.3, 0.1)
+    text = recpot.format_recpot(mx, vals, "HA Mg")
     sp = recpot.parse_recpot(text, "Mg")
     ref = recpot.species_from_table(mx, vals, "Mg")
     assert sp.charge == 2 and np.allclose(sp.pot_values, ref.pot_values, rtol=1e-15, atol=0)
@@ -48,9 +48,9 @@ def test_recpot_text_round_trip():
     assert osp.charge == 2 and np.allclose(osp.vqs, sp.vqs, rtol=1e-15, atol=0)
 
 
-def test_gha_tables_have_the_coulomb_tail():
+def test_heine_abarenkov_tables_have_the_coulomb_tail():
     for z, rc in [(3, 1.15), (2, 1.3)]:
-        mx, vals = wl.gha_table(float(z), rc, 0.1)
+        mx, vals = wl.heine_abarenkov_table(float(z), rc, 0.1)
         sp = recpot.species_from_table(mx, vals)
         assert sp.charge == z
         # v(q) q^2 -> -4 pi Z as q -> 0 (the tail ReadPseudo infers Z from)
@@ -59,11 +59,11 @@ def test_gha_tables_have_the_coulomb_tail():
         assert np.all(np.abs(tail / (-4 * np.pi * z) - 1.0) < 1e-4)
 
 
-def test_gha_table_is_the_transform_of_the_model_potential():
+def test_heine_abarenkov_table_is_the_transform_of_the_model_potential():
     """v(q) + 4 pi Z / q^2 = 4 pi int_0^rc r^2 (-A + Z/r) j0(qr) dr (quadrature)."""
     from profess_b200.recpot import BOHR, HARTREE_TO_EV
     z, rc, a = 2.0, 1.3, 0.1
-    mx, vals = wl.gha_table(z, rc, a)
+    mx, vals = wl.heine_abarenkov_table(z, rc, a)
     v = vals / (BOHR ** 3 * HARTREE_TO_EV)
     x, w = np.polynomial.legendre.leggauss(64)
     r, wr = 0.5 * rc * (x + 1.0), 0.5 * rc * w

@@ -13,7 +13,7 @@ DT = 40.0  # a.u. of time (~0.97 fs)
 
 def _cells():
     c = wl.fcc_al((1, 1, 1), sigma_ang=0.05, grid=(20, 20, 20), seed=3)
-    mx, vals = wl.gha_table(3.0, 1.15, 0.1)
+    mx, vals = wl.heine_abarenkov_table(3.0, 1.15, 0.1)
     ocell = cs.Cell(lattice=c.lattice, frac=c.frac, species_of_ion=c.species_of_ion,
                     species=[cs.species_from_table(mx, vals, "Al")])
     return c, ocell

@@ -11,7 +11,7 @@ from profess_b200 import native, relax, workloads as wl
 
 def _cell(seed=3, grid=(16, 16, 16)):
     c = wl.fcc_al((1, 1, 1), sigma_ang=0.1, grid=grid, seed=seed)
-    mx, vals = wl.gha_table(3.0, 1.15, 0.1)
+    mx, vals = wl.heine_abarenkov_table(3.0, 1.15, 0.1)
     ocell = cs.Cell(lattice=c.lattice, frac=c.frac, species_of_ion=c.species_of_ion,
                     species=[cs.species_from_table(mx, vals, "Al")])
     return c, ocell

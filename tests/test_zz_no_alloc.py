@@ -6,13 +6,17 @@ under a memory budget fixed before the solve): its scratch is a static array
 inside the library.  This test gives it device buffers that the test itself
 allocates and checks two calls in a row (two different densities) against
 ofdft_calculate_potential_plus at the tolerances of the other GPU parity
-tests (potential 1e-11 relative, energy terms 1e-10 Ha)."""
+tests (potential 1e-11 relative, energy terms 1e-10 Ha), and the second call
+against the oracle as well.  The grids reach the documented limits: 64^3
+(262144 points), a 128-point axis (128 x 128 x 16), and alpha != beta (four
+spectra in the scratch instead of three)."""
 import ctypes
 
 import numpy as np
 import pytest
 
 import cases
+from oracle import functional as ofn
 from profess_b200 import native
 
 pytestmark = pytest.mark.gpu
@@ -23,13 +27,15 @@ def _dev(a):
     return torch.tensor(np.asfortranarray(a).ravel(order="F"), dtype=torch.float64, device="cuda")
 
 
-@pytest.mark.parametrize("name,n", [("wt_al4_displaced", None), ("wt_al4_displaced", (32, 30, 27))])
-def test_noalloc_matches_engine(name, n):
+@pytest.mark.parametrize("n,alpha,beta", [(None, 5 / 6, 5 / 6), ((32, 30, 27), 5 / 6, 5 / 6),
+                                          ((64, 64, 64), 5 / 6, 5 / 6), ((128, 128, 16), 5 / 6, 5 / 6),
+                                          ((40, 36, 30), 1.2, 0.45)])
+def test_noalloc_matches_engine(n, alpha, beta):
     import torch
     torch.cuda.set_device(0)
-    cell, f, _, _ = cases.golden_case(name)
-    if n is not None:
-        f = cases.functional_for(cell, n, 4, 5 / 6, 5 / 6)
+    cell, f, _, _ = cases.golden_case("wt_al4_displaced")
+    if n is not None or alpha != beta:
+        f = cases.functional_for(cell, n or f.n, 4, alpha, beta)
     lib = native.load_library()
     fn = lib.ofdft_calculate_potential_plus_noalloc
     fn.argtypes = [ctypes.POINTER(native.CellDesc), ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
@@ -56,6 +62,10 @@ def test_noalloc_matches_engine(name, n):
             pot_e, et_e = eng.calculate_potential_plus(slot, rho)
             assert np.abs(pot - pot_e).max() / np.abs(pot_e).max() < 1e-11, "call %d" % call
             assert np.abs(et - et_e).max() < 1e-10, "call %d" % call
+            if call == 1:
+                pot_o, et_o = ofn.calculate_potential_plus(f, rho)
+                assert np.abs(pot - pot_o).max() / np.abs(pot_o).max() < 1e-11
+                assert np.abs(et - et_o).max() < 1e-10
     finally:
         eng.close()
 

@@ -81,35 +81,33 @@ static int odd_columns(int nf, int rp, size_t csz) {
 }
 
 // Launch shape of a slot's passes: row pairs per x-forward task (*rp1) and
-// per x-inverse task (s.rp), and the kx tile widths of the y and z passes
-// (*ty, *tz; s.tx = *ty).  The x-forward tasks carry every field (or ion
-// species) of their row pairs in about 72 KB; the y/z tiles take as many kx
-// columns as fit the two shared buffers of a block (one field of n2 values
-// per column in the y pass, a group of gmax fields of n3 values in the z
-// pass) in about 56 KB, four blocks per SM, and at least 4 columns (rows of
-// 32 or 64 bytes) up to 112 KB per block; two-step lengths take at most
-// 256 / R2 columns, so that the first step's work items (columns x R2) fit
-// the 256 threads of a block in one round.  s needs n1..n3, k1, nf and
-// kinetic; csz is the size of one complex value.
+// per x-inverse task (s.rp), carrying every field (or ion species) of their
+// row pairs in about 36 KB of shared memory; and the tiles of the split y/z
+// path: z columns per y-pass task (*ty: columns of n2 values at an odd row
+// pitch) and y columns per z-pass task (*tz: a group of gmax fields of n3
+// values each), each in about 48 KB, at least 32 columns when n allows.
+// s needs n1..n3, k1, nf and kinetic; csz is the size of one complex value.
 static void launch_shape(SlotDev& s, size_t csz, int nfx, int* rp1, int* ty, int* tz) {
   *rp1 = std::max(1, std::min(32, 1024 / s.n1));
-  while (*rp1 > 1 && 2 * (size_t)nfx * *rp1 * s.n1 * csz > 72 * 1024) (*rp1)--;
+  while (*rp1 > 1 && (size_t)nfx * *rp1 * s.n1 * csz > 36 * 1024) (*rp1)--;
   s.rp = std::max(1, std::min(32, 1024 / s.n1));
-  while (s.rp > 1 && 2 * (size_t)s.nf * s.rp * s.n1 * csz > 72 * 1024) s.rp--;
+  while (s.rp > 1 && (size_t)s.nf * s.rp * s.n1 * csz > 36 * 1024) s.rp--;
   *rp1 = odd_columns(s.nf, *rp1, csz);
   s.rp = odd_columns(s.nf, s.rp, csz);
   const int gmax = s.kinetic == KIN_WGC ? 3 : 1;
-  auto width = [&](size_t per_col) {
-    size_t w = std::min<size_t>((size_t)s.k1, (56 * 1024) / per_col);
-    if (w < 4) w = std::min<size_t>((size_t)s.k1, std::max<size_t>(1, std::min<size_t>(4, (112 * 1024) / per_col)));
-    return (int)std::max<size_t>(1, w);
-  };
-  *ty = width(2 * (size_t)s.n2 * csz);
-  *tz = width(2 * (size_t)gmax * s.n3 * csz);
-  if (fft2_r2(s.n2) > 0) *ty = std::max(1, std::min(*ty, 256 / fft2_r2(s.n2)));
-  if (fft2_r2(s.n3) > 0) *tz = std::max(1, std::min(*tz, 256 / (gmax * fft2_r2(s.n3))));
-  s.tx = *ty;
+  const size_t ycol = (size_t)(s.n2 | 1) * csz, zcol = (size_t)gmax * s.n3 * csz;
+  *ty = (int)std::max<size_t>(1, std::min<size_t>(s.n3, std::max<size_t>(48 * 1024 / ycol, 32)));
+  *tz = (int)std::max<size_t>(1, std::min<size_t>(s.n2, std::max<size_t>(48 * 1024 / zcol, 32)));
+  while (*ty > 1 && *ty * ycol > 160 * 1024) (*ty)--;
+  while (*tz > 1 && *tz * zcol > 160 * 1024) (*tz)--;
 }
+
+// Shared memory of the fused y-z pass of one plane (rows of odd pitch), and
+// the largest plane it takes; bigger planes run the split y/z path.
+static size_t yz_smem(const SlotDev& s, size_t csz) { return (size_t)s.n3 * (s.n2 | 1) * csz; }
+constexpr size_t YZ_SMEM_MAX = 200 * 1024;
+// Planes up to this size run 256-thread blocks (three per SM), larger ones 512.
+constexpr size_t YZ_SMEM_SMALL = 75 * 1024;
 
 // ------------------------------------------------------------ FFT plans
 static bool seven_smooth(int n) {
@@ -119,109 +117,43 @@ static bool seven_smooth(int n) {
   return n == 1;
 }
 
-// Radix sequence of n: the fewest stages with radices from {2, ..., rmax}
-// (7-smooth), then the smallest largest radix; the largest radix goes first
-// (the first Stockham stage has no twiddles).
-static std::vector<int> radices(int n, int rmax) {
-  static const int kR[] = {16, 15, 14, 12, 10, 9, 8, 7, 6, 5, 4, 3, 2};
-  // best[m] = (stages, largest radix, first radix) for m | n, by increasing m
-  std::map<int, std::pair<int, int>> cost;  // m -> (stages, largest radix)
-  std::map<int, int> first;
-  cost[1] = {0, 0};
-  std::vector<int> divs;
-  for (int m = 2; m <= n; ++m)
-    if (n % m == 0) divs.push_back(m);
-  for (int m : divs) {
-    std::pair<int, int> best = {1 << 20, 1 << 20};
-    int bf = 0;
-    for (int R : kR) {
-      if (R > rmax || m % R || !cost.count(m / R)) continue;
-      const std::pair<int, int> c = {cost[m / R].first + 1, std::max(R, cost[m / R].second)};
-      if (c < best) { best = c; bf = R; }
-    }
-    cost[m] = best;
-    first[m] = bf;
-  }
-  std::vector<int> r;
-  for (int m = n; m > 1; m /= first[m]) r.push_back(first[m]);
-  std::sort(r.begin(), r.end(), [](int a, int b) { return a > b; });
-  return r;
-}
-
 constexpr int MAX_N = 512;
-
-// Largest radix of the FP32 and FP64 plans (OFDFT_RMAX_* in fft.cuh) and the
-// minimum resident 256-thread blocks per SM of the FFT pass kernels, per
-// precision (it caps their registers at 65536 / (256 * minb)).  The passes
-// are latency- and issue-bound: on 16 cells of 96^3, Stockham radices <= 8
-// with 4 blocks per SM (64 registers) beat radix <= 16 with 2 blocks per SM;
-// FP64 runs best with 3 blocks per SM (85 registers, no spills in the
-// two-step transforms).
-#ifndef OFDFT_MINB_FP32
-#define OFDFT_MINB_FP32 4
-#endif
-#ifndef OFDFT_MINB_FP64
-#define OFDFT_MINB_FP64 3
-#endif
-constexpr int RMAX_FP32 = OFDFT_RMAX_FP32;
-constexpr int RMAX_FP64 = OFDFT_RMAX_FP64;
-template <typename T> struct PassMinBlocks { static constexpr int value = OFDFT_MINB_FP32; };
-template <> struct PassMinBlocks<double> { static constexpr int value = OFDFT_MINB_FP64; };
-// The FP32 y pass runs five blocks per SM (48 registers, a few spills): 1.7 %
-// less FP32 evaluation time at 96^3 than four.  Other passes lose with more
-// blocks, and every FP64 pass loses with four.
-template <typename T> struct YPassMinBlocks { static constexpr int value = PassMinBlocks<T>::value + 1; };
-template <> struct YPassMinBlocks<double> { static constexpr int value = OFDFT_MINB_FP64; };
-static_assert(OFDFT_RMAX_FP64 >= 8, "the allocation-free evaluation plans radix-8 stages in FP64");
 
 struct PlanTable {
   std::map<int, FftPlan> plans[2];  // [0] FP64 (OFDFT_FP64), [1] FP32
-  std::vector<long double> re, im;
-  void* d_tw64 = nullptr;
+  void* d_tw64 = nullptr;           // exp(-2 pi i e / n), e < n, for every 7-smooth n <= MAX_N
   void* d_tw32 = nullptr;
+  int* d_idx = nullptr;             // perm and iperm of every plan
 
   int build() {
-    for (int pi = 0; pi < 2; ++pi)
-      for (int n = 1; n <= MAX_N; ++n) {
-        if (!seven_smooth(n)) continue;
-        FftPlan p;
-        memset(&p, 0, sizeof(p));
-        p.n = n;
-        p.tw_base = (int)re.size();
-        std::vector<int> rs = radices(n, pi == 0 ? RMAX_FP64 : RMAX_FP32);
-        p.nst = (int)rs.size();
-        int ns = 1, off = 0;
-        for (int s = 0; s < p.nst; ++s) {
-          const int R = rs[s];
-          p.R[s] = R;
-          p.Ns[s] = ns;
-          p.tw[s] = off;
-          for (int k = 0; k < ns; ++k)
-            for (int m = 1; m < R; ++m) {
-              const long double ang = -2.0L * 3.141592653589793238462643383279502884L * (long double)(m * k) /
-                                      (long double)(ns * R);
-              re.push_back(cosl(ang));
-              im.push_back(sinl(ang));
-            }
-          p.ns_magic[s] = (unsigned)(((1u << 20) + (unsigned)ns - 1) / (unsigned)ns);
-          off += ns * (R - 1);
-          ns *= R;
-        }
-        p.root = -1;
-        plans[pi][n] = p;
-      }
-    // exp(-2 pi i e / n), e = 0..n-1, for the two-step transforms
+    std::vector<long double> re, im;
+    std::map<int, int> root_off;
     for (int n = 1; n <= MAX_N; ++n) {
       if (!seven_smooth(n)) continue;
-      const int off = (int)re.size();
+      root_off[n] = (int)re.size();
       for (int e = 0; e < n; ++e) {
         const long double ang = -2.0L * 3.141592653589793238462643383279502884L * (long double)e / (long double)n;
         re.push_back(cosl(ang));
         im.push_back(sinl(ang));
       }
-      plans[0][n].root = off;
-      plans[1][n].root = off;
     }
+    std::vector<int> idx;
+    for (int pi = 0; pi < 2; ++pi)
+      for (int n = 1; n <= MAX_N; ++n) {
+        if (!seven_smooth(n)) continue;
+        int rad[FFT_MAX_STAGES];
+        const int nst = fft_radices(n, pi == 0 ? FftMaxRadix<double>::value : FftMaxRadix<float>::value, rad);
+        FftPlan p;
+        memset(&p, 0, sizeof(p));
+        std::vector<int> perm(n), iperm(n);
+        fft_plan_fill(p, n, rad, nst, perm.data(), iperm.data());
+        p.root = root_off[n];
+        p.perm = (int)idx.size();
+        idx.insert(idx.end(), perm.begin(), perm.end());
+        p.iperm = (int)idx.size();
+        idx.insert(idx.end(), iperm.begin(), iperm.end());
+        plans[pi][n] = p;
+      }
     const size_t nt = re.size();
     std::vector<cx<double>> t64(nt);
     std::vector<cx<float>> t32(nt);
@@ -230,28 +162,43 @@ struct PlanTable {
       t32[i] = mk<float>((float)re[i], (float)im[i]);
     }
     int rc = dmalloc(&d_tw64, nt * sizeof(cx<double>));
-    if (rc) return rc;
-    rc = dmalloc(&d_tw32, nt * sizeof(cx<float>));
-    if (rc) return rc;
-    rc = h2d(d_tw64, t64.data(), nt * sizeof(cx<double>));
-    if (rc) return rc;
-    return h2d(d_tw32, t32.data(), nt * sizeof(cx<float>));
+    if (!rc) rc = dmalloc(&d_tw32, nt * sizeof(cx<float>));
+    if (!rc) rc = dmalloc((void**)&d_idx, idx.size() * sizeof(int));
+    if (!rc) rc = h2d(d_tw64, t64.data(), nt * sizeof(cx<double>));
+    if (!rc) rc = h2d(d_tw32, t32.data(), nt * sizeof(cx<float>));
+    if (!rc) rc = h2d(d_idx, idx.data(), idx.size() * sizeof(int));
+    return rc;
   }
   void release() {
     dfree(d_tw64);
     dfree(d_tw32);
+    dfree(d_idx);
     d_tw64 = d_tw32 = nullptr;
+    d_idx = nullptr;
   }
 };
 
 // ------------------------------------------------------------ kernels
 // Launch lists of one tick.  Passes 1, 3 and 5 have one list for the WT slots
 // (P_X1, P_Z3, P_X5) and one for the WGC slots (P_X1G, P_Z3G, P_X5G), each
-// launched with the kernel instantiated for that functional.
+// launched with the kernel instantiated for that functional.  A slot takes
+// either the fused y-z pass (P_YZ, or P_YZB for planes above YZ_SMEM_SMALL)
+// or the split path (P_Y2, P_Z3/P_Z3G, P_Y4).
 enum Pass : int { P_VEC = 0, P_X1 = 1, P_Y2 = 2, P_Z3 = 3, P_Y4 = 4, P_X5 = 5, P_CTL = 6,
-                  P_X1G = 7, P_Z3G = 8, P_X5G = 9, NPASS = 10 };
+                  P_X1G = 7, P_Z3G = 8, P_X5G = 9, P_YZ = 10, P_YZB = 11, NPASS = 12 };
 constexpr int VEC_PER_TICK = 2;
 constexpr int VCHUNK = 4096;
+
+// Minimum resident 256-thread blocks per SM of the x and split y/z pass
+// kernels per precision (it caps their registers at 65536 / (256 * minb)).
+#ifndef OFDFT_MINB_FP32
+#define OFDFT_MINB_FP32 4
+#endif
+#ifndef OFDFT_MINB_FP64
+#define OFDFT_MINB_FP64 3
+#endif
+template <typename T> struct PassMinBlocks { static constexpr int value = OFDFT_MINB_FP32; };
+template <> struct PassMinBlocks<double> { static constexpr int value = OFDFT_MINB_FP64; };
 
 #if !defined(OFDFT_EMU)
 template <typename T> __global__ void __launch_bounds__(256) k_vec(Args<T> a) {
@@ -262,7 +209,7 @@ template <typename T, int KS> __global__ void __launch_bounds__(256, PassMinBloc
   extern __shared__ __align__(16) char sm[];
   xfwd_block<T, KS>(a, blockIdx.x, threadIdx.x, blockDim.x, sm);
 }
-template <typename T> __global__ void __launch_bounds__(256, YPassMinBlocks<T>::value) k_ypass(Args<T> a, int dir) {
+template <typename T> __global__ void __launch_bounds__(256, PassMinBlocks<T>::value) k_ypass(Args<T> a, int dir) {
   extern __shared__ __align__(16) char sm[];
   ypass_block<T>(a, blockIdx.x, threadIdx.x, blockDim.x, sm, dir);
 }
@@ -270,14 +217,31 @@ template <typename T, int KS> __global__ void __launch_bounds__(256, PassMinBloc
   extern __shared__ __align__(16) char sm[];
   zpass_block<T, KS>(a, blockIdx.x, threadIdx.x, blockDim.x, sm);
 }
+// Fused y-z pass: 256-thread blocks, three per SM, for planes up to
+// YZ_SMEM_SMALL; 512-thread blocks, one per SM, for larger planes.
+template <typename T, int NT> __global__ void __launch_bounds__(NT, NT == 256 ? 3 : 1) k_yzpass(Args<T> a) {
+  extern __shared__ __align__(16) char sm[];
+  yzpass_block<T>(a, blockIdx.x, threadIdx.x, blockDim.x, sm);
+}
 template <typename T, int KS> __global__ void __launch_bounds__(256, PassMinBlocks<T>::value) k_xinv(Args<T> a) {
   extern __shared__ __align__(16) char sm[];
   xinv_block<T, KS>(a, blockIdx.x, threadIdx.x, blockDim.x, sm);
 }
-template <typename T> __global__ void __launch_bounds__(256) k_fill_kernel(const SlotDev* sd, KernArgs ka, int kind) {
+// keKernel planes from the reference layout (k1, n2, n3), x fastest, into
+// the engine's kx-major digit-reversed layout.
+template <typename T> __global__ void __launch_bounds__(256) k_permute_kernel(const SlotDev* sd, const int* idx,
+                                                                             const double* src, int nplanes) {
+  const SlotDev& s = *sd;
+  const long long total = s.Nc * nplanes;
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < total;
+       i += (long long)gridDim.x * blockDim.x)
+    ((T*)s.kern)[i] = (T)src[kernel_source_index(s, idx, i)];
+}
+template <typename T> __global__ void __launch_bounds__(256) k_fill_kernel(const SlotDev* sd, const int* idx,
+                                                                          KernArgs ka, int kind) {
   const SlotDev& s = *sd;
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < (int)s.Nc; i += gridDim.x * blockDim.x)
-    fill_kernel_point<T>(s, ka, kind, i);
+    fill_kernel_point<T>(s, idx, ka, kind, i);
 }
 template <typename T> __global__ void __launch_bounds__(256) k_spread(const SlotDev* sd, const IonStencil* st) {
   for (int w = threadIdx.x; w < SPLINE_ORDER * SPLINE_ORDER * SPLINE_ORDER; w += blockDim.x)
@@ -330,7 +294,8 @@ struct HostSlot {
   SlotDev sd;
   std::vector<void*> allocs;
   int nrowpairs = 0, rp1 = 1;
-  int ty = 1, tz = 1;           // kx tile widths of the y and z passes
+  int ty = 1, tz = 1;           // z columns per y-pass task and y columns per z-pass task (split path)
+  bool setup_pass = false;      // running an ion-potential or force pass (split path)
   int nplanes = 0;
   int nion = 0;                 // ions of the last ion-potential build
   IonStencil* d_stencil = nullptr;
@@ -589,14 +554,14 @@ struct Engine {
     HostSlot& h = slots[i];
 #if defined(OFDFT_EMU)
     for (int idx = 0; idx < (int)h.sd.Nc; ++idx) {
-      if (h.prec == OFDFT_FP32) fill_kernel_point<float>(h.sd, ka, kind, idx);
-      else fill_kernel_point<double>(h.sd, ka, kind, idx);
+      if (h.prec == OFDFT_FP32) fill_kernel_point<float>(h.sd, plans.d_idx, ka, kind, idx);
+      else fill_kernel_point<double>(h.sd, plans.d_idx, ka, kind, idx);
     }
     return OFDFT_OK;
 #else
     const int blocks = (int)std::min<long long>(4096, (h.sd.Nc + 255) / 256);
-    if (h.prec == OFDFT_FP32) k_fill_kernel<float><<<blocks, 256, 0, stream>>>(d_slots + i, ka, kind);
-    else k_fill_kernel<double><<<blocks, 256, 0, stream>>>(d_slots + i, ka, kind);
+    if (h.prec == OFDFT_FP32) k_fill_kernel<float><<<blocks, 256, 0, stream>>>(d_slots + i, plans.d_idx, ka, kind);
+    else k_fill_kernel<double><<<blocks, 256, 0, stream>>>(d_slots + i, plans.d_idx, ka, kind);
     int rc = cuda_check(cudaGetLastError(), "fill kernel launch");
     return rc ? rc : sync_stream();
 #endif
@@ -773,12 +738,16 @@ struct Engine {
     return OFDFT_OK;
   }
 
-  // Run a slot that needs a single evaluation tick.
+  // Run a slot that needs a single evaluation tick (the ion-potential and
+  // force set-up passes, which take the split y/z path).
   int run_one(int i) {
     slots[i].running = true;
+    slots[i].setup_pass = true;
     dirty = true;
     int running = 0;
     int rc = run(4, &running, 1);
+    slots[i].setup_pass = false;
+    dirty = true;
     if (rc) return rc;
     if (slots[i].running) return fail(OFDFT_ETIMEOUT, "set-up pass did not finish");
     Ctl c;
@@ -906,6 +875,34 @@ struct Engine {
     return d2h(dst, io, bytes);
   }
 #endif
+
+  // keKernel(k1G, k2G, k3G, nplanes) from the host (reference layout, FP64)
+  // into the slot's kernel planes (kx-major, digit-reversed, slot precision).
+  int set_kernel(int i, const double* kernel) {
+    HostSlot& h = slots[i];
+    const long long n = h.sd.Nc * h.nplanes;
+#if defined(OFDFT_EMU)
+    for (long long k = 0; k < n; ++k) {
+      const double v = kernel[kernel_source_index(h.sd, plans.d_idx, k)];
+      if (h.prec == OFDFT_FP32) ((float*)h.sd.kern)[k] = (float)v;
+      else ((double*)h.sd.kern)[k] = v;
+    }
+    return OFDFT_OK;
+#else
+    void* io = nullptr;
+    int rc = io_scratch(sizeof(double) * (size_t)n, &io);
+    if (rc) return rc;
+    if ((rc = cuda_check(cudaMemcpyAsync(io, kernel, sizeof(double) * (size_t)n, cudaMemcpyHostToDevice, stream),
+                         "H2D async")))
+      return rc;
+    if (h.prec == OFDFT_FP32)
+      k_permute_kernel<float><<<io_blocks(n), 256, 0, stream>>>(d_slots + i, plans.d_idx, (const double*)io, h.nplanes);
+    else
+      k_permute_kernel<double><<<io_blocks(n), 256, 0, stream>>>(d_slots + i, plans.d_idx, (const double*)io, h.nplanes);
+    if ((rc = cuda_check(cudaGetLastError(), "kernel permute launch"))) return rc;
+    return sync_stream();
+#endif
+  }
 
   int get_ctl(int i, Ctl& c) { return d2h(&c, d_ctl + i, sizeof(Ctl)); }
   int put_ctl(int i, const Ctl& c) { return h2d(d_ctl + i, &c, sizeof(Ctl)); }
@@ -1173,6 +1170,12 @@ struct Engine {
   }
 
   // ---------------------------------------------------------- task lists
+  // Whether a running slot takes the fused y-z pass: WT slots whose (y, z)
+  // plane fits shared memory, outside the set-up passes.
+  bool uses_yz(const HostSlot& h) const {
+    return h.sd.kinetic == KIN_WT && !h.setup_pass && yz_smem(h.sd, 2 * elem_size(h.prec)) <= YZ_SMEM_MAX;
+  }
+
   int build_lists() {
     for (int p = 0; p < 2; ++p)
       for (int k = 0; k < NPASS; ++k) {
@@ -1193,27 +1196,38 @@ struct Engine {
       for (int r = 0; r < h.nrowpairs; r += h.rp1)
         L[px1].h.push_back({i, 0, r, std::min(h.rp1, h.nrowpairs - r)});
       L[px1].nthr = 256;
-      L[px1].smem = std::max(L[px1].smem, 2 * (size_t)std::max(s.nf, s.ion.nspec) * h.rp1 * s.n1 * cs);
-      for (int pass : {P_Y2, P_Y4}) {
-        for (int f = 0; f < s.nf; ++f)
-          for (int z = 0; z < s.n3; ++z)
-            for (int t = 0; t < tile_count(s.k1, h.ty); ++t) L[pass].h.push_back({i, f, z, tile_code(s.k1, h.ty, t)});
-        L[pass].nthr = 256;
-        L[pass].smem = std::max(L[pass].smem, 2 * (size_t)h.ty * s.n2 * cs);
+      L[px1].smem = std::max(L[px1].smem, (size_t)std::max(s.nf, s.ion.nspec) * h.rp1 * s.n1 * cs);
+      if (uses_yz(h)) {  // fused y-z pass: one task per (field, kx)
+        const size_t sm = yz_smem(s, cs);
+        const int pyz = sm <= YZ_SMEM_SMALL ? P_YZ : P_YZB;
+        for (int g = 0; g < s.ngroups; ++g)
+          for (int kx = 0; kx < s.k1; ++kx) L[pyz].h.push_back({i, g, kx, 0});
+        L[pyz].nthr = pyz == P_YZ ? 256 : 512;
+        L[pyz].smem = std::max(L[pyz].smem, sm);
+      } else {  // split path: y forward, z with the operator, y inverse
+        for (int pass : {P_Y2, P_Y4}) {
+          for (int f = 0; f < s.nf; ++f)
+            for (int kx = 0; kx < s.k1; ++kx)
+              for (int t = 0; t < tile_count(s.n3, h.ty); ++t)
+                L[pass].h.push_back({i, f, kx, tile_code(s.n3, h.ty, t)});
+          L[pass].nthr = 256;
+          L[pass].smem = std::max(L[pass].smem, (size_t)h.ty * (s.n2 | 1) * cs);
+        }
+        const int gmax = s.kinetic == KIN_WGC ? 3 : 1;
+        for (int g = 0; g < s.ngroups; ++g)
+          for (int kx = 0; kx < s.k1; ++kx)
+            for (int t = 0; t < tile_count(s.n2, h.tz); ++t)
+              L[pz3].h.push_back({i, g, kx, tile_code(s.n2, h.tz, t)});
+        L[pz3].nthr = 256;
+        L[pz3].smem = std::max(L[pz3].smem, (size_t)std::max(gmax, s.ion.nspec) * h.tz * s.n3 * cs);
       }
-      const int gmax = s.kinetic == KIN_WGC ? 3 : 1;
-      for (int g = 0; g < s.ngroups; ++g)
-        for (int ky = 0; ky < s.n2; ++ky)
-          for (int t = 0; t < tile_count(s.k1, h.tz); ++t) L[pz3].h.push_back({i, g, ky, tile_code(s.k1, h.tz, t)});
-      L[pz3].nthr = 256;
-      L[pz3].smem = std::max(L[pz3].smem, 2 * (size_t)std::max(gmax, s.ion.nspec) * h.tz * s.n3 * cs);
       int ord = 0;
       for (int r = 0; r < h.nrowpairs; r += s.rp) L[px5].h.push_back({i, r, std::min(s.rp, h.nrowpairs - r), ord++});
       L[P_CTL].h.push_back({i, 0, 0, 0});
       L[P_CTL].nthr = 64;
       L[P_CTL].smem = 0;
       L[px5].nthr = 256;
-      L[px5].smem = std::max(L[px5].smem, 2 * (size_t)std::max(s.nf, s.ion.nspec) * s.rp * s.n1 * cs +
+      L[px5].smem = std::max(L[px5].smem, (size_t)std::max(s.nf, s.ion.nspec) * s.rp * s.n1 * cs +
                                               NCH * 33 * sizeof(double) + 16);
     }
 #if defined(OFDFT_EMU)
@@ -1247,6 +1261,7 @@ struct Engine {
     a.ctl = d_ctl;
     a.tasks = lists[prec][pass].d;
     a.tw = (const cx<T>*)(prec == OFDFT_FP32 ? plans.d_tw32 : plans.d_tw64);
+    a.idx = plans.d_idx;
     a.vchunk = VCHUNK;
     return a;
   }
@@ -1272,6 +1287,8 @@ struct Engine {
     run(P_Z3, [](Args<T>& a, int b, char* sm) { zpass_block<T, KS_WT>(a, b, 0, 1, sm); });
     run(P_Z3G, [](Args<T>& a, int b, char* sm) { zpass_block<T, KS_WGC>(a, b, 0, 1, sm); });
     run(P_Y4, [](Args<T>& a, int b, char* sm) { ypass_block<T>(a, b, 0, 1, sm, 1); });
+    run(P_YZ, [](Args<T>& a, int b, char* sm) { yzpass_block<T>(a, b, 0, 1, sm); });
+    run(P_YZB, [](Args<T>& a, int b, char* sm) { yzpass_block<T>(a, b, 0, 1, sm); });
     run(P_X5, [](Args<T>& a, int b, char* sm) { xinv_block<T, KS_WT>(a, b, 0, 1, sm); });
     run(P_X5G, [](Args<T>& a, int b, char* sm) { xinv_block<T, KS_WGC>(a, b, 0, 1, sm); });
     run(P_CTL, [](Args<T>& a, int b, char*) { ctl_block(a.slots, a.ctl, a.tasks, K_X5, b, 0, 1, (char*)ctl_sm); });
@@ -1294,6 +1311,8 @@ struct Engine {
     }
     if ((rc = launch_one<T>(prec, P_X1, k_xfwd<T, KS_WT>))) return rc;
     if ((rc = launch_one<T>(prec, P_X1G, k_xfwd<T, KS_WGC>))) return rc;
+    if ((rc = launch_one<T>(prec, P_YZ, k_yzpass<T, 256>))) return rc;
+    if ((rc = launch_one<T>(prec, P_YZB, k_yzpass<T, 512>))) return rc;
     if ((rc = launch_one<T>(prec, P_Y2, k_ypass<T>, -1))) return rc;
     if ((rc = launch_one<T>(prec, P_Z3, k_zpass<T, KS_WT>))) return rc;
     if ((rc = launch_one<T>(prec, P_Z3G, k_zpass<T, KS_WGC>))) return rc;
@@ -1328,6 +1347,8 @@ struct Engine {
     if ((rc = attr(k_zpass<T, KS_WGC>, P_Z3G))) return rc;
     if ((rc = attr(k_xinv<T, KS_WGC>, P_X5G))) return rc;
     if ((rc = attr(k_ypass<T>, lists[prec][P_Y2].smem >= lists[prec][P_Y4].smem ? P_Y2 : P_Y4))) return rc;
+    if ((rc = attr(k_yzpass<T, 256>, P_YZ))) return rc;
+    if ((rc = attr(k_yzpass<T, 512>, P_YZB))) return rc;
     if ((rc = attr(k_zpass<T, KS_WT>, P_Z3))) return rc;
     return attr(k_xinv<T, KS_WT>, P_X5);
   }
@@ -1490,7 +1511,7 @@ int ofdft_slot_set_kernel(ofdft_engine* e, int slot, const double* kernel, int n
   if (rc) return rc;
   HostSlot& h = e->eng.slots[slot];
   if (nplanes != h.nplanes) return fail(OFDFT_EINVAL, "kernel plane count does not match the functional");
-  return e->eng.upload_real(h.prec, h.sd.kern, kernel, h.sd.Nc * nplanes);
+  return e->eng.set_kernel(slot, kernel);
 }
 
 int ofdft_slot_set_ion_potential(ofdft_engine* e, int slot, const double* v) {
@@ -1824,36 +1845,23 @@ static int scratch_address(int dev, char** base) {
 
 static size_t up256(size_t x) { return (x + 255) & ~size_t(255); }
 
-// Plan of length n with twiddles appended to tw at offset *off (no heap use).
-static void make_plan(int n, FftPlan& p, cx<double>* tw, int* off) {
+// Plan of length n (the engine's FP64 radix rule) with its roots of unity
+// appended to tw at *toff and its digit-reversal tables to idx at *ioff (no
+// heap use).
+static void make_plan(int n, FftPlan& p, cx<double>* tw, int* toff, int* idx, int* ioff) {
   memset(&p, 0, sizeof(p));
-  p.n = n;
-  p.root = -1;
-  p.tw_base = *off;
-  int r[FFT_MAX_STAGES], nr = 0, m = n, e2 = 0;
-  while (m % 2 == 0) { m /= 2; ++e2; }
-  while (e2 >= 3) { r[nr++] = 8; e2 -= 3; }
-  if (e2 == 2) r[nr++] = 4;
-  if (e2 == 1) r[nr++] = 2;
-  for (int q : {3, 5, 7})
-    while (m % q == 0) { r[nr++] = q; m /= q; }
-  p.nst = nr;
-  int ns = 1, o = 0;
-  for (int s = 0; s < nr; ++s) {
-    const int R = r[s];
-    p.R[s] = R;
-    p.Ns[s] = ns;
-    p.tw[s] = o;
-    p.ns_magic[s] = (unsigned)(((1u << 20) + (unsigned)ns - 1) / (unsigned)ns);
-    for (int k = 0; k < ns; ++k)
-      for (int j = 1; j < R; ++j) {
-        const long double a = -2.0L * 3.141592653589793238462643383279502884L * (long double)(j * k) /
-                              (long double)(ns * R);
-        tw[*off + o++] = mk<double>((double)cosl(a), (double)sinl(a));
-      }
-    ns *= R;
+  int rad[FFT_MAX_STAGES];
+  const int nst = fft_radices(n, FftMaxRadix<double>::value, rad);
+  fft_plan_fill(p, n, rad, nst, idx + *ioff, idx + *ioff + n);
+  p.root = *toff;
+  p.perm = *ioff;
+  p.iperm = *ioff + n;
+  for (int e = 0; e < n; ++e) {
+    const long double a = -2.0L * 3.141592653589793238462643383279502884L * (long double)e / (long double)n;
+    tw[*toff + e] = mk<double>((double)cosl(a), (double)sinl(a));
   }
-  *off += o;
+  *toff += n;
+  *ioff += 2 * n;
 }
 }  // namespace noalloc
 #endif
@@ -1885,11 +1893,12 @@ extern "C" int ofdft_calculate_potential_plus_noalloc(const ofdft_cell_desc* d, 
   s.k1 = d->n1 / 2 + 1;
   s.N = N;
   s.Nc = (long long)s.k1 * d->n2 * d->n3;
-  cx<double> tw[4 * MAX_DIM];  // twiddles of the three plans (n - 1 per plan)
-  int twoff = 0;
-  make_plan(d->n1, s.px, tw, &twoff);
-  make_plan(d->n2, s.py, tw, &twoff);
-  make_plan(d->n3, s.pz, tw, &twoff);
+  cx<double> tw[3 * MAX_DIM];  // roots of unity of the three plans
+  int ptab[6 * MAX_DIM];        // their digit-reversal tables
+  int twoff = 0, poff = 0;
+  make_plan(d->n1, s.px, tw, &twoff, ptab, &poff);
+  make_plan(d->n2, s.py, tw, &twoff, ptab, &poff);
+  make_plan(d->n3, s.pz, tw, &twoff, ptab, &poff);
   const double* L = d->lattice;
   auto A = [&](int r, int c) { return L[3 * c + r]; };
   const double det = A(0, 0) * (A(1, 1) * A(2, 2) - A(1, 2) * A(2, 1)) - A(0, 1) * (A(1, 0) * A(2, 2) - A(1, 2) * A(2, 0)) +
@@ -1927,8 +1936,12 @@ extern "C" int ofdft_calculate_potential_plus_noalloc(const ofdft_cell_desc* d, 
   s.buf[B_PHI] = (void*)rho;         // the input density (read only in EV_RHO mode)
   s.buf[B_W0] = (void*)potential;    // the output potential
   s.vion = (void*)ion_pot;
-  s.kern = (void*)kernel;
-  // task lists, packed one pass after the other
+  // the engine's passes: the fused y-z pass when the plane fits, else the split path
+  const size_t yzsm = yz_smem(s, cs);
+  const bool fused = yzsm <= YZ_SMEM_MAX;
+  const int yzthr = yzsm <= YZ_SMEM_SMALL ? 256 : 512;
+  // task lists, packed one pass after the other: x forward, y forward (or
+  // y-z), z, y inverse, x inverse, controller
   int nt[6] = {0, 0, 0, 0, 0, 0}, ntot = 0;
   auto push = [&](int pass, Task t) -> bool {
     if (ntot >= MAX_TASKS) return false;
@@ -1938,12 +1951,17 @@ extern "C" int ofdft_calculate_potential_plus_noalloc(const ofdft_cell_desc* d, 
   };
   bool ok = true;
   for (int r = 0; r < nrp && ok; r += rp1) ok = push(0, {0, 0, r, std::min(rp1, nrp - r)});
-  for (int f = 0; f < s.nf && ok; ++f)
-    for (int z = 0; z < s.n3 && ok; ++z)
-      for (int t = 0; t < tile_count(s.k1, ty) && ok; ++t) ok = push(1, {0, f, z, tile_code(s.k1, ty, t)});
-  for (int g = 0; g < s.ngroups && ok; ++g)
-    for (int ky = 0; ky < s.n2 && ok; ++ky)
-      for (int t = 0; t < tile_count(s.k1, tz) && ok; ++t) ok = push(2, {0, g, ky, tile_code(s.k1, tz, t)});
+  if (fused) {
+    for (int g = 0; g < s.ngroups && ok; ++g)
+      for (int kx = 0; kx < s.k1 && ok; ++kx) ok = push(1, {0, g, kx, 0});
+  } else {
+    for (int f = 0; f < s.nf && ok; ++f)
+      for (int kx = 0; kx < s.k1 && ok; ++kx)
+        for (int t = 0; t < tile_count(s.n3, ty) && ok; ++t) ok = push(1, {0, f, kx, tile_code(s.n3, ty, t)});
+    for (int g = 0; g < s.ngroups && ok; ++g)
+      for (int kx = 0; kx < s.k1 && ok; ++kx)
+        for (int t = 0; t < tile_count(s.n2, tz) && ok; ++t) ok = push(2, {0, g, kx, tile_code(s.n2, tz, t)});
+  }
   int ord = 0;
   for (int r = 0; r < nrp && ok; r += s.rp) ok = push(3, {0, r, std::min(s.rp, nrp - r), ord++});
   if (ok) ok = push(4, {0, 0, 0, 0});
@@ -1953,8 +1971,10 @@ extern "C" int ofdft_calculate_potential_plus_noalloc(const ofdft_cell_desc* d, 
   const size_t o_slot = o; o = up256(o + sizeof(SlotDev));
   const size_t o_ctl = o; o = up256(o + sizeof(Ctl));
   const size_t o_tw = o; o = up256(o + cs * (size_t)twoff);
+  const size_t o_idx = o; o = up256(o + sizeof(int) * (size_t)poff);
   const size_t o_part = o; o = up256(o + sizeof(double) * NCH * (size_t)s.ntask[K_X5]);
   const size_t o_task = o; o = up256(o + sizeof(Task) * (size_t)ntot);
+  const size_t o_kern = o; o = up256(o + sizeof(double) * (size_t)s.Nc);
   const size_t o_spec = o; o = up256(o + cs * (size_t)s.nf * (size_t)s.Nc);
   if (o > SCRATCH_BYTES) return fail(OFDFT_EINVAL, "grid needs more scratch than the allocation-free evaluation holds");
   cudaStream_t st = (cudaStream_t)stream_ptr;
@@ -1966,6 +1986,7 @@ extern "C" int ofdft_calculate_potential_plus_noalloc(const ofdft_cell_desc* d, 
   if ((rc = scratch_address(dev, &base))) return rc;
   s.partials = (double*)(base + o_part);
   s.spec = (void*)(base + o_spec);
+  s.kern = (void*)(base + o_kern);  // the caller's keKernel, permuted into the engine's layout below
   Ctl ctl;
   memset(&ctl, 0, sizeof(ctl));
   ctl.status = ST_RUNNING;
@@ -1980,36 +2001,51 @@ extern "C" int ofdft_calculate_potential_plus_noalloc(const ofdft_cell_desc* d, 
     return rc;
   if ((rc = cuda_check(cudaMemcpyAsync(base + o_tw, tw, cs * (size_t)twoff, cudaMemcpyHostToDevice, st), "H2D")))
     return rc;
+  if ((rc = cuda_check(cudaMemcpyAsync(base + o_idx, ptab, sizeof(int) * (size_t)poff, cudaMemcpyHostToDevice, st),
+                       "H2D")))
+    return rc;
   if ((rc = cuda_check(cudaMemcpyAsync(base + o_task, t_tasks, sizeof(Task) * (size_t)ntot, cudaMemcpyHostToDevice,
                                        st), "H2D")))
     return rc;
-  // launches: passes 1-5 and the controller kernel, as one engine tick does
+  const int* didx = (const int*)(base + o_idx);
+  k_permute_kernel<double><<<(unsigned)std::min<long long>(4 * 148, (s.Nc + 255) / 256), 256, 0, st>>>(
+      (const SlotDev*)(base + o_slot), didx, kernel, 1);
+  // launches: the passes and the controller kernel, as one engine tick does
   Args<double> a;
   a.slots = (SlotDev*)(base + o_slot);
   a.ctl = (Ctl*)(base + o_ctl);
   a.tw = (const cx<double>*)(base + o_tw);
+  a.idx = didx;
   a.vchunk = VCHUNK;
-  const size_t sm1 = 2 * (size_t)s.nf * rp1 * s.n1 * cs;
-  const size_t sm2 = 2 * (size_t)ty * s.n2 * cs;
-  const size_t sm3 = 2 * (size_t)tz * s.n3 * cs;
-  const size_t sm5 = 2 * (size_t)s.nf * s.rp * s.n1 * cs + NCH * 33 * sizeof(double) + 16;
+  const size_t sm1 = (size_t)s.nf * rp1 * s.n1 * cs;
+  const size_t sm2 = (size_t)ty * (s.n2 | 1) * cs;
+  const size_t sm3 = (size_t)tz * s.n3 * cs;
+  const size_t sm5 = (size_t)s.nf * s.rp * s.n1 * cs + NCH * 33 * sizeof(double) + 16;
   auto attr = [&](auto kern, size_t sm) -> int {
     if (sm <= 48 * 1024) return OFDFT_OK;
     return cuda_check(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm),
                       "cudaFuncSetAttribute");
   };
-  if ((rc = attr(k_xfwd<double, KS_WT>, sm1)) || (rc = attr(k_ypass<double>, sm2)) || (rc = attr(k_zpass<double, KS_WT>, sm3)) ||
-      (rc = attr(k_xinv<double, KS_WT>, sm5)))
+  if ((rc = attr(k_xfwd<double, KS_WT>, sm1)) || (rc = attr(k_xinv<double, KS_WT>, sm5)))
+    return rc;
+  if (fused && (rc = yzthr == 256 ? attr(k_yzpass<double, 256>, yzsm) : attr(k_yzpass<double, 512>, yzsm)))
+    return rc;
+  if (!fused && ((rc = attr(k_ypass<double>, sm2)) || (rc = attr(k_zpass<double, KS_WT>, sm3))))
     return rc;
   const Task* tb = (const Task*)(base + o_task);
   a.tasks = tb;
   k_xfwd<double, KS_WT><<<nt[0], 256, sm1, st>>>(a);
   a.tasks = tb + nt[0];
-  k_ypass<double><<<nt[1], 256, sm2, st>>>(a, -1);
-  a.tasks = tb + nt[0] + nt[1];
-  k_zpass<double, KS_WT><<<nt[2], 256, sm3, st>>>(a);
-  a.tasks = tb + nt[0];
-  k_ypass<double><<<nt[1], 256, sm2, st>>>(a, 1);
+  if (fused) {
+    if (yzthr == 256) k_yzpass<double, 256><<<nt[1], 256, yzsm, st>>>(a);
+    else k_yzpass<double, 512><<<nt[1], 512, yzsm, st>>>(a);
+  } else {
+    k_ypass<double><<<nt[1], 256, sm2, st>>>(a, -1);
+    a.tasks = tb + nt[0] + nt[1];
+    k_zpass<double, KS_WT><<<nt[2], 256, sm3, st>>>(a);
+    a.tasks = tb + nt[0];
+    k_ypass<double><<<nt[1], 256, sm2, st>>>(a, 1);
+  }
   a.tasks = tb + nt[0] + nt[1] + nt[2];
   k_xinv<double, KS_WT><<<nt[3], 256, sm5, st>>>(a);
   a.tasks = tb + nt[0] + nt[1] + nt[2] + nt[3];

@@ -1,24 +1,30 @@
-// Batched mixed-radix Stockham FFT over shared memory.
+// Batched in-place mixed-radix FFT over shared memory.
 //
-// A transform of length n = R_0 * R_1 * ... runs as one Stockham stage per
-// radix.  The radices are 2, 3, 4, 5, 7, 8 and the compound radices 6, 9, 10,
-// 12, 14, 15, 16, whose R-point DFTs run in registers as an A x B
-// Cooley-Tukey split of the small DFTs with compile-time twiddles, so most
-// lengths up to 256 take two stages.  Each stage reads R points at stride n/R,
-// multiplies by the stage twiddles, does the R-point DFT in registers and
-// writes the R outputs in self-sorting order, ping-ponging between two shared
-// buffers; the caller reads the result from whichever buffer fft_batch
-// returns.  Many independent transforms of the same length are done together:
-// element i of transform b lives at buf[b + i*si].  Work items (b, butterfly)
-// are spread over the block's threads with b fastest, so consecutive threads
-// touch consecutive shared-memory words; the index arithmetic uses
-// multiply-high divisions by constants prepared on the host.  The direction
-// (DIR = -1 forward, +1 inverse) is a template parameter.
+// A transform of length n = R_0 * R_1 * ... * R_{S-1} runs as one stage per
+// radix, in place: the forward transform is a decimation in frequency
+// (natural order in, digit-reversed order out), the inverse a decimation in
+// time (digit-reversed order in, natural order out), so a forward transform,
+// a pointwise operator in k-space and the inverse need neither a second
+// buffer nor a reordering pass.  Stage s works on blocks of length
+// L_s = n / (R_0 ... R_{s-1}) with stride m_s = L_s / R_s: the butterfly
+// (block b, offset j0 < m_s) reads the R_s points b L_s + j0 + m_s j1, does
+// the R_s-point DFT in registers and, going forward, multiplies output r by
+// W_{L_s}^{j0 r} (W_M = exp(-2 pi i / M)) and stores it at b L_s + j0 + m_s r;
+// the inverse stage undoes that with the conjugate twiddles first and the
+// inverse DFT second, stages in reverse order.  After the forward transform,
+// position q holds frequency perm[q], with perm built by
+// perm(q) = r + R_0 perm'(q - r m_0), r = q / m_0, over the remaining
+// radices; iperm is its inverse.
 //
-// Twiddles are precomputed on the host in long double and stored per plan:
-// stage s with span Ns (product of the earlier radices) and radix R uses
-// tw[off_s + k*(R-1) + (m-1)] = exp(-2*pi*i*m*k/(Ns*R)), k = 0..Ns-1.
-// The inverse transform uses the conjugates.  No scaling is applied here.
+// The radices are 2, 3, 4, 5, 7, 8 and the compound 6, 9, 10, 12, 14, 15, 16,
+// whose DFTs run in registers as an A x B Cooley-Tukey split with
+// compile-time twiddles.  Many columns of the same length are transformed
+// together: element i of column c lives at buf[c*cs + i*es]; work items
+// (column, butterfly) are spread over the block's threads with the column
+// fastest, so consecutive threads touch consecutive columns (conflict-free
+// shared-memory access when cs = 1, or when cs is odd).  The twiddles are
+// the n-th roots of unity exp(-2 pi i e / n), e < n, computed on the host in
+// long double; W_{L_s}^{e} is root[e n / L_s].  No scaling is applied.
 #pragma once
 #include "cx.cuh"
 
@@ -27,31 +33,22 @@ namespace ofdft {
 constexpr int FFT_MAX_STAGES = 12;
 constexpr int FFT_MAX_RADIX = 16;
 
-// Largest radix of the FP32 and FP64 plans.  An R-point DFT holds R complex
-// values in registers; only the radices up to the limit are compiled into a
-// precision's kernels, so the limit also bounds their register use.
-#ifndef OFDFT_RMAX_FP32
-#define OFDFT_RMAX_FP32 8
-#endif
-#ifndef OFDFT_RMAX_FP64
-#define OFDFT_RMAX_FP64 8
-#endif
-template <typename T> struct FftMaxRadix { static constexpr int value = OFDFT_RMAX_FP32; };
-template <> struct FftMaxRadix<double> { static constexpr int value = OFDFT_RMAX_FP64; };
+// Largest radix of the FP32 and FP64 plans: an R-point DFT holds R complex
+// values in registers, and only the radices up to the limit are compiled
+// into a precision's kernels.
+template <typename T> struct FftMaxRadix { static constexpr int value = 16; };
+template <> struct FftMaxRadix<double> { static constexpr int value = 12; };
 
 struct FftPlan {
   int n;
   int nst;
   int R[FFT_MAX_STAGES];
-  int Ns[FFT_MAX_STAGES];
-  int tw[FFT_MAX_STAGES];  // offset of the stage's twiddles in the plan table
-  unsigned ns_magic[FFT_MAX_STAGES];  // ceil(2^20 / Ns): j / Ns == (j * magic) >> 20 for j < 2048
-  int tw_base;             // offset of this plan in the global twiddle table
-  int root;                // offset of exp(-2 pi i e / n), e = 0..n-1, in that table; -1: none
+  int L[FFT_MAX_STAGES];               // block length of stage s, n / (R_0 ... R_{s-1})
+  unsigned m_magic[FFT_MAX_STAGES];    // magic32(L[s] / R[s])
+  int root;                            // offset of exp(-2 pi i e / n), e < n, in the twiddle table
+  int perm;                            // offset of perm (position -> frequency) in the index table
+  int iperm;                           // offset of iperm (frequency -> position)
 };
-
-// Exact quotient j / d for 0 <= j < 2048 and 1 <= d <= 512 from magic = ceil(2^20 / d).
-HD int magic_div(int j, unsigned magic) { return (int)(((unsigned)j * magic) >> 20); }
 
 // Exact quotient w / d for 0 <= w < 2^24 and 1 <= d <= 4096 from m32 = ceil(2^32 / d)
 // (d = 1 is encoded as m32 = 0).
@@ -297,306 +294,144 @@ HD void dft_ab(cx<T>* v) {
   }
 }
 
-// One Stockham stage of radix R over nb transforms: src -> dst.  Element i of
-// transform b is at [b + i*si] (si >= nb); mnb = magic32(nb).
+// One in-place stage of radix R over ncols columns (mcols = magic32(ncols)):
+// DIR = -1 forward (DFT, then twiddles), +1 inverse (conjugate twiddles,
+// then inverse DFT).  tstep = n / L.
 template <typename T, int R, int DIR>
-HD void fft_stage_r(const cx<T>* __restrict__ src, cx<T>* __restrict__ dst, int nb, unsigned mnb, int si, int n,
-                    int Ns, unsigned magic, const cx<T>* __restrict__ tw, int tid, int nthr) {
-  const int nbf = n / R;  // butterflies per transform
-  const int total = nbf * nb;
+HD void ip_stage_r(cx<T>* __restrict__ buf, int ncols, unsigned mcols, int cs, int es, int n, int L, unsigned mm,
+                   const cx<T>* __restrict__ roots, int tid, int nthr) {
+  const int m = L / R;
+  const int total = (n / R) * ncols;
+  const int tstep = n / L;
+  const int ms = m * es;
   for (int w = tid; w < total; w += nthr) {
-    const int j = magic_div32(w, mnb);
-    const int b = w - j * nb;
-    const int jq = magic_div(j, magic);
-    const int kmod = j - jq * Ns;
+    const int bf = magic_div32(w, mcols), c = w - bf * ncols;
+    const int blk = magic_div32(bf, mm), j0 = bf - blk * m;
+    cx<T>* p = buf + c * cs + (blk * L + j0) * es;
     cx<T> v[R];
-    const cx<T>* s = src + b;
 #pragma unroll
-    for (int m = 0; m < R; ++m) v[m] = s[(j + m * nbf) * si];
-    if (Ns > 1) {
-      const cx<T>* t = tw + kmod * (R - 1);
+    for (int r = 0; r < R; ++r) v[r] = p[r * ms];
+    const int e = j0 * tstep;
+    if (DIR > 0 && m > 1) {
 #pragma unroll
-      for (int m = 1; m < R; ++m) {
-        cx<T> f = t[m - 1];
-        if (DIR > 0) f.y = -f.y;
-        v[m] = cmul(v[m], f);
-      }
+      for (int r = 1; r < R; ++r) v[r] = cmul(v[r], conj(roots[r * e]));
     }
     Dft<T, R, DIR>::run(v);
-    cx<T>* d = dst + b;
-    const int base = jq * Ns * R + kmod;
+    if (DIR < 0 && m > 1) {
 #pragma unroll
-    for (int m = 0; m < R; ++m) d[(base + m * Ns) * si] = v[m];
+      for (int r = 1; r < R; ++r) v[r] = cmul(v[r], roots[r * e]);
+    }
+#pragma unroll
+    for (int r = 0; r < R; ++r) p[r * ms] = v[r];
   }
 }
 
 template <typename T, int DIR>
-HD void fft_stage(const cx<T>* src, cx<T>* dst, int nb, unsigned mnb, int si, int n, int R, int Ns, unsigned magic,
-                  const cx<T>* tw, int tid, int nthr) {
+HD void ip_stage(cx<T>* buf, int ncols, unsigned mcols, int cs, int es, const FftPlan& p, int s, const cx<T>* roots,
+                 int tid, int nthr) {
   constexpr int RM = FftMaxRadix<T>::value;
-#define OFDFT_STAGE_CASE(r)                                                                 \
-  case r:                                                                                   \
-    if constexpr (r <= RM) fft_stage_r<T, r, DIR>(src, dst, nb, mnb, si, n, Ns, magic, tw, tid, nthr); \
+  const int n = p.n, L = p.L[s];
+  const unsigned mm = p.m_magic[s];
+#define OFDFT_IP_CASE(r)                                                                          \
+  case r:                                                                                         \
+    if constexpr (r <= RM) ip_stage_r<T, r, DIR>(buf, ncols, mcols, cs, es, n, L, mm, roots, tid, nthr); \
     break;
-  switch (R) {
-    OFDFT_STAGE_CASE(2)
-    OFDFT_STAGE_CASE(3)
-    OFDFT_STAGE_CASE(4)
-    OFDFT_STAGE_CASE(5)
-    OFDFT_STAGE_CASE(6)
-    OFDFT_STAGE_CASE(7)
-    OFDFT_STAGE_CASE(8)
-    OFDFT_STAGE_CASE(9)
-    OFDFT_STAGE_CASE(10)
-    OFDFT_STAGE_CASE(12)
-    OFDFT_STAGE_CASE(14)
-    OFDFT_STAGE_CASE(15)
-    OFDFT_STAGE_CASE(16)
+  switch (p.R[s]) {
+    OFDFT_IP_CASE(2)
+    OFDFT_IP_CASE(3)
+    OFDFT_IP_CASE(4)
+    OFDFT_IP_CASE(5)
+    OFDFT_IP_CASE(6)
+    OFDFT_IP_CASE(7)
+    OFDFT_IP_CASE(8)
+    OFDFT_IP_CASE(9)
+    OFDFT_IP_CASE(10)
+    OFDFT_IP_CASE(12)
+    OFDFT_IP_CASE(14)
+    OFDFT_IP_CASE(15)
+    OFDFT_IP_CASE(16)
     default: break;
   }
-#undef OFDFT_STAGE_CASE
+#undef OFDFT_IP_CASE
 }
 
-// Full transform of nb sequences held in buf (tmp is scratch of the same
-// layout), element i of sequence b at [b + i*si].  DIR = -1 forward, +1
-// inverse.  Returns the buffer (buf or tmp) holding the result.  Must be
-// called by every thread of the block.
+// Full in-place transform of ncols columns (element i of column c at
+// buf[c*cs + i*es]).  DIR = -1: forward, natural -> digit-reversed; DIR = +1:
+// inverse, digit-reversed -> natural.  Every thread of the block must call
+// it; the data must be complete in shared memory on entry (the caller's
+// barrier), and the block synchronises after every stage, so the result is
+// complete on return.
 template <typename T, int DIR>
-HD cx<T>* fft_batch(cx<T>* buf, cx<T>* tmp, int nb, int si, const FftPlan& p, const cx<T>* twtab, int tid,
-                    int nthr) {
-  cx<T>* a = buf;
-  cx<T>* b = tmp;
-  const unsigned mnb = magic32(nb);
-  const int nst = p.nst, n = p.n;
-  for (int s = 0; s < nst; ++s) {
-    fft_stage<T, DIR>(a, b, nb, mnb, si, n, p.R[s], p.Ns[s], p.ns_magic[s], twtab + p.tw_base + p.tw[s], tid, nthr);
-    BLOCK_SYNC();
-    cx<T>* t = a;
-    a = b;
-    b = t;
-  }
-  return a;
-}
-
-// Runtime direction: dir = -1 forward, +1 inverse.
-template <typename T>
-HD cx<T>* fft_batch(cx<T>* buf, cx<T>* tmp, int nb, int si, const FftPlan& p, const cx<T>* twtab, int dir,
-                    int tid, int nthr) {
-  return dir < 0 ? fft_batch<T, -1>(buf, tmp, nb, si, p, twtab, tid, nthr)
-                 : fft_batch<T, 1>(buf, tmp, nb, si, p, twtab, tid, nthr);
-}
-
-// ------------------------------------------------------------ transforms between accessors
-// Element i of column b of a batch held in shared memory at p[b + i*si].
-template <typename T>
-struct SmemIO {
-  cx<T>* p;
-  int si;
-  HD cx<T> ld(int i, int b) const { return p[b + i * si]; }
-  HD void st(int i, int b, cx<T> v) const { p[b + i * si] = v; }
-};
-
-// One Stockham stage of radix R whose inputs come from src.ld(i, b) and whose
-// outputs go to dst.st(i, b, v) (same work split as fft_stage_r).
-template <typename T, int R, int DIR, class Src, class Dst>
-HD void fft_stage_io(const Src& src, const Dst& dst, int nb, unsigned mnb, int n, int Ns, unsigned magic,
-                     const cx<T>* __restrict__ tw, int tid, int nthr) {
-  const int nbf = n / R;
-  const int total = nbf * nb;
-  for (int w = tid; w < total; w += nthr) {
-    const int j = magic_div32(w, mnb);
-    const int b = w - j * nb;
-    const int jq = magic_div(j, magic);
-    const int kmod = j - jq * Ns;
-    cx<T> v[R];
-#pragma unroll
-    for (int m = 0; m < R; ++m) v[m] = src.ld(j + m * nbf, b);
-    if (Ns > 1) {
-      const cx<T>* t = tw + kmod * (R - 1);
-#pragma unroll
-      for (int m = 1; m < R; ++m) {
-        cx<T> f = t[m - 1];
-        if (DIR > 0) f.y = -f.y;
-        v[m] = cmul(v[m], f);
-      }
-    }
-    Dft<T, R, DIR>::run(v);
-    const int base = jq * Ns * R + kmod;
-#pragma unroll
-    for (int m = 0; m < R; ++m) dst.st(base + m * Ns, b, v[m]);
-  }
-}
-
-template <typename T, int DIR, class Src, class Dst>
-HD void fft_stage_io_any(const Src& src, const Dst& dst, int nb, unsigned mnb, int n, int R, int Ns, unsigned magic,
-                         const cx<T>* tw, int tid, int nthr) {
-  constexpr int RM = FftMaxRadix<T>::value;
-#define OFDFT_IO_CASE(r)                                                                           \
-  case r:                                                                                          \
-    if constexpr (r <= RM) fft_stage_io<T, r, DIR>(src, dst, nb, mnb, n, Ns, magic, tw, tid, nthr); \
-    break;
-  switch (R) {
-    OFDFT_IO_CASE(2)
-    OFDFT_IO_CASE(3)
-    OFDFT_IO_CASE(4)
-    OFDFT_IO_CASE(5)
-    OFDFT_IO_CASE(6)
-    OFDFT_IO_CASE(7)
-    OFDFT_IO_CASE(8)
-    OFDFT_IO_CASE(9)
-    OFDFT_IO_CASE(10)
-    OFDFT_IO_CASE(12)
-    OFDFT_IO_CASE(14)
-    OFDFT_IO_CASE(15)
-    OFDFT_IO_CASE(16)
-    default: break;
-  }
-#undef OFDFT_IO_CASE
-}
-
-// Full transform of nb columns: stage 0 reads src, stage s (0 <= s < nst-1)
-// writes buffer A (s even) or B (s odd), the last stage writes dst.  src may
-// be A's or B's storage only if it is not the buffer stage 0 writes (A).
-// When dst is shared memory it must be fft_out_buffer(nst, A, B), the buffer
-// the last stage does not read.  No barrier after the last stage.
-template <typename T, int DIR, class Src, class Dst>
-HD void fft_run(const Src& src, const Dst& dst, cx<T>* A, cx<T>* B, int nb, const FftPlan& p, const cx<T>* twtab,
-                int tid, int nthr) {
-  const unsigned mnb = magic32(nb);
-  const int nst = p.nst, n = p.n;
-  const cx<T>* tw0 = twtab + p.tw_base;
-  if (nst == 1) {
-    fft_stage_io_any<T, DIR>(src, dst, nb, mnb, n, p.R[0], p.Ns[0], p.ns_magic[0], tw0 + p.tw[0], tid, nthr);
-    return;
-  }
-  const SmemIO<T> a{A, nb}, b{B, nb};
-  fft_stage_io_any<T, DIR>(src, a, nb, mnb, n, p.R[0], p.Ns[0], p.ns_magic[0], tw0 + p.tw[0], tid, nthr);
-  BLOCK_SYNC();
-  for (int s = 1; s < nst - 1; ++s) {
-    if (s & 1) fft_stage_io_any<T, DIR>(a, b, nb, mnb, n, p.R[s], p.Ns[s], p.ns_magic[s], tw0 + p.tw[s], tid, nthr);
-    else fft_stage_io_any<T, DIR>(b, a, nb, mnb, n, p.R[s], p.Ns[s], p.ns_magic[s], tw0 + p.tw[s], tid, nthr);
-    BLOCK_SYNC();
-  }
-  const int sl = nst - 1;
-  if (sl & 1) fft_stage_io_any<T, DIR>(a, dst, nb, mnb, n, p.R[sl], p.Ns[sl], p.ns_magic[sl], tw0 + p.tw[sl], tid, nthr);
-  else fft_stage_io_any<T, DIR>(b, dst, nb, mnb, n, p.R[sl], p.Ns[sl], p.ns_magic[sl], tw0 + p.tw[sl], tid, nthr);
-}
-
-// The buffer of fft_run that the last stage does not read (A or B).
-template <typename T>
-HD cx<T>* fft_out_buffer(int nst, cx<T>* A, cx<T>* B) { return ((nst - 1) & 1) ? B : A; }
-
-// ------------------------------------------------------------ two-step register FFT
-// A transform of length n = R1 * R2 (both compile-time) over NC columns, with
-// one shared-memory exchange: with j = t + R2*j1 and k = k1 + R1*k2,
-//   X[k1 + R1 k2] = sum_t W_R2^{t k2} W_n^{t k1} sum_j1 W_R1^{j1 k1} x[t + R2 j1],
-// W_m = exp(DIR * 2 pi i / m).  Step 1 (one work item per column and t)
-// loads its R1 inputs from src.ld(i, c) straight into registers, does the
-// R1-point DFT and the twiddles W_n^{t k1} = roots[t*k1] (t*k1 < n), and
-// writes the exchange buffer X (NC * n values); step 2 (one work item per
-// column and k1) does the R2-point DFT and writes the outputs with
-// dst.st(k, c, v).  Consecutive threads take consecutive columns.  src may be
-// the same memory as dst: every input is read before the barrier between the
-// steps and every output is written after it.
-template <typename T, int R1, int R2, int DIR, class Src, class Dst>
-HD void fft2_tile(const Src& src, const Dst& dst, cx<T>* __restrict__ X, int NC, const cx<T>* __restrict__ roots,
-                  int tid, int nthr) {
-  const unsigned mnc = magic32(NC);
-  for (int w = tid; w < NC * R2; w += nthr) {
-    const int t = magic_div32(w, mnc), c = w - t * NC;
-    cx<T> v[R1], f[R1];
-#pragma unroll
-    for (int j1 = 0; j1 < R1; ++j1) v[j1] = src.ld(t + R2 * j1, c);
-    // the twiddles are loaded while the data loads are in flight
-#pragma unroll
-    for (int k1 = 1; k1 < R1; ++k1) f[k1] = roots[t * k1];
-    Dft<T, R1, DIR>::run(v);
-#pragma unroll
-    for (int k1 = 1; k1 < R1; ++k1) {
-      if (DIR > 0) f[k1].y = -f[k1].y;
-      v[k1] = cmul(v[k1], f[k1]);
-    }
-    cx<T>* x = X + c + NC * t;
-#pragma unroll
-    for (int k1 = 0; k1 < R1; ++k1) x[NC * R2 * k1] = v[k1];
-  }
-  BLOCK_SYNC();
-  for (int w = tid; w < NC * R1; w += nthr) {
-    const int k1 = magic_div32(w, mnc), c = w - k1 * NC;
-    cx<T> v[R2];
-    const cx<T>* x = X + c + NC * R2 * k1;
-#pragma unroll
-    for (int t = 0; t < R2; ++t) v[t] = x[NC * t];
-    Dft<T, R2, DIR>::run(v);
-#pragma unroll
-    for (int k2 = 0; k2 < R2; ++k2) dst.st(k1 + R1 * k2, c, v[k2]);
-  }
-}
-
-// Largest step-2 radix of the two-step transforms per precision (R2 complex
-// values stay in registers).
-template <typename T> struct Fft2MaxRadix { static constexpr int value = 16; };
-template <> struct Fft2MaxRadix<double> { static constexpr int value = 12; };
-
-// The lengths with a two-step transform and their factors (R1 <= R2).
-#define OFDFT_FFT2_SIZES(X) \
-  X(32, 4, 8)               \
-  X(48, 6, 8)               \
-  X(64, 8, 8)               \
-  X(72, 8, 9)               \
-  X(80, 8, 10)              \
-  X(96, 8, 12)              \
-  X(120, 10, 12)            \
-  X(128, 8, 16)             \
-  X(144, 12, 12)            \
-  X(160, 10, 16)            \
-  X(192, 12, 16)            \
-  X(240, 15, 16)            \
-  X(256, 16, 16)
-
-// Second-step radix R2 of the two-step transform of length n (0: none).
-HD int fft2_r2(int n) {
-  switch (n) {
-#define OFDFT_FFT2_R2(N, A, B) \
-  case N:                      \
-    return B;
-    OFDFT_FFT2_SIZES(OFDFT_FFT2_R2)
-#undef OFDFT_FFT2_R2
-    default:
-      return 0;
-  }
-}
-
-// Whether length n has a two-step transform in precision T.
-template <typename T>
-HD bool fft2_supported(const FftPlan& p) {
-  if (p.root < 0) return false;
-  switch (p.n) {
-#define OFDFT_FFT2_CASE(N, A, B) \
-  case N:                        \
-    return B <= Fft2MaxRadix<T>::value;
-    OFDFT_FFT2_SIZES(OFDFT_FFT2_CASE)
-#undef OFDFT_FFT2_CASE
-    default:
-      return false;
-  }
-}
-
-// Two-step transform of length p.n (fft2_supported must hold).
-template <typename T, int DIR, class Src, class Dst>
-HD void fft2_run(const Src& src, const Dst& dst, cx<T>* X, int NC, const FftPlan& p, const cx<T>* twtab, int tid,
-                 int nthr) {
+HD void fft_inplace(cx<T>* buf, int ncols, int cs, int es, const FftPlan& p, const cx<T>* twtab, int tid, int nthr) {
+  const unsigned mcols = magic32(ncols);
   const cx<T>* roots = twtab + p.root;
-  switch (p.n) {
-#define OFDFT_FFT2_CASE(N, A, B)                                                       \
-  case N:                                                                              \
-    if constexpr (B <= Fft2MaxRadix<T>::value)                                         \
-      fft2_tile<T, A, B, DIR>(src, dst, X, NC, roots, tid, nthr);                      \
-    break;
-    OFDFT_FFT2_SIZES(OFDFT_FFT2_CASE)
-#undef OFDFT_FFT2_CASE
-    default:
-      break;
+  if (DIR < 0) {
+    for (int s = 0; s < p.nst; ++s) {
+      ip_stage<T, -1>(buf, ncols, mcols, cs, es, p, s, roots, tid, nthr);
+      BLOCK_SYNC();
+    }
+  } else {
+    for (int s = p.nst - 1; s >= 0; --s) {
+      ip_stage<T, 1>(buf, ncols, mcols, cs, es, p, s, roots, tid, nthr);
+      BLOCK_SYNC();
+    }
+  }
+}
+
+// ------------------------------------------------------------ host planning
+// Radix sequence of n (7-smooth, n <= 512): the fewest stages with radices
+// up to rmax, then the smallest largest radix; largest radix first.  No heap
+// use (the allocation-free entry point plans with it too).  Returns the
+// number of stages, 0 if n has no such factorisation.
+inline int fft_radices(int n, int rmax, int* out) {
+  static const int kR[] = {16, 15, 14, 12, 10, 9, 8, 7, 6, 5, 4, 3, 2};
+  int st[513], big[513], first[513];
+  for (int m = 0; m <= n; ++m) { st[m] = 1 << 20; big[m] = 1 << 20; first[m] = 0; }
+  st[1] = 0;
+  big[1] = 0;
+  for (int m = 2; m <= n; ++m) {
+    if (n % m) continue;
+    for (int R : kR) {
+      if (R > rmax || m % R || st[m / R] >= (1 << 20)) continue;
+      const int cs = st[m / R] + 1, cb = R > big[m / R] ? R : big[m / R];
+      if (cs < st[m] || (cs == st[m] && cb < big[m])) { st[m] = cs; big[m] = cb; first[m] = R; }
+    }
+  }
+  if (st[n] >= (1 << 20)) return 0;
+  int k = 0;
+  for (int m = n; m > 1; m /= first[m]) out[k++] = first[m];
+  for (int a = 0; a < k; ++a)  // largest first
+    for (int b = a + 1; b < k; ++b)
+      if (out[b] > out[a]) { const int t = out[a]; out[a] = out[b]; out[b] = t; }
+  return k;
+}
+
+// Fill plan p of length n from its radix sequence (stage block lengths and
+// magic numbers; the table offsets are the caller's), and the digit-reversal
+// tables: perm[q] = frequency at position q after the forward transform,
+// iperm[k] = position of frequency k.  No heap use.
+inline void fft_plan_fill(FftPlan& p, int n, const int* radix, int nst, int* perm, int* iperm) {
+  p.n = n;
+  p.nst = nst;
+  int L = n;
+  for (int s = 0; s < nst; ++s) {
+    p.R[s] = radix[s];
+    p.L[s] = L;
+    p.m_magic[s] = magic32(L / radix[s]);
+    L /= radix[s];
+  }
+  for (int q = 0; q < n; ++q) {
+    int k = 0, mult = 1, rem = q, len = n;
+    for (int s = 0; s < nst; ++s) {
+      const int m = len / radix[s];
+      const int r = rem / m;
+      k += mult * r;
+      mult *= radix[s];
+      rem -= r * m;
+      len = m;
+    }
+    perm[q] = k;
+    iperm[k] = q;
   }
 }
 

@@ -1,13 +1,23 @@
-// Block functions of the engine: the vector-op kernel and the five passes of
-// one potential evaluation (CalculatePotentialPlus):
+// Block functions of the engine: the vector-op kernel and the passes of one
+// potential evaluation (CalculatePotentialPlus).
+//
+// Spectrum layout: field f of a slot is a half spectrum of k1 = n1/2 + 1
+// planes, kx-major: element (kx, row j = y + n2 z) at spec[f*Nc + kx*nrows +
+// j], so that every (y, z) plane of one kx is contiguous.  Between the
+// forward and the inverse transforms along y and z the plane is in the
+// digit-reversed order of the in-place FFT (position q holds frequency
+// perm[q]); the kernel planes are stored in that order.
 //
 //   pass 1  X forward : prologue (phi_in, rho and the functional's fields) and
-//                       the x-direction real-to-complex FFT of row pairs
-//   pass 2  Y forward : complex FFT along y on (field, z, kx-tile) tiles
-//   pass 3  Z         : complex FFT along z, the k-space operator of each field
-//                       group (Hartree 4pi/G^2, vW G^2, WT/WGC kernels, with the
-//                       1/N forward scaling), inverse FFT along z
-//   pass 4  Y inverse
+//                       the x-direction real-to-complex FFT of row pairs,
+//                       stored kx-major
+//   pass YZ           : one (y, z) plane of one field in shared memory:
+//                       forward FFT along y and z, the k-space operator
+//                       (Hartree 4pi/G^2, vW G^2, the WT kernel, with the 1/N
+//                       forward scaling), inverse FFT along z and y
+//   (planes that do not fit shared memory, the WGC groups and the set-up
+//    modes run the same work as three passes: Y forward, Z with the
+//    operator, Y inverse)
 //   pass 5  X inverse : complex-to-real FFT of all fields of a row pair and the
 //                       real-space epilogue (potential, chain rule, energies and
 //                       the optimiser's fused sums)
@@ -37,8 +47,9 @@ struct Args {
   SlotDev* slots;
   Ctl* ctl;
   const Task* tasks;
-  const cx<T>* tw;
-  int vchunk;  // points per task of the vector kernel
+  const cx<T>* tw;   // roots of unity of every plan length
+  const int* idx;    // digit-reversal tables (FftPlan::perm, iperm)
+  int vchunk;        // points per task of the vector kernel
 };
 
 // V_loc(|q|) by the index-knot cubic spline (PspRecipCubicSpline, LocalPseudoPot.f90:92-202).
@@ -469,7 +480,6 @@ HD void xfwd_block(const Args<T>& a, int bid, int tid, int nthr, char* smem) {
   const FieldPar<T> fp = field_par<T>(s);
   const FftPlan& px = s.px;
   cx<T>* buf = (cx<T>*)smem;
-  cx<T>* tmp = buf + NB * n1;
   const unsigned mn1 = magic32(n1);
   for (int w = tid; w < nb * n1; w += nthr) {
     const int b = magic_div32(w, mn1), i = w - b * n1;
@@ -500,156 +510,80 @@ HD void xfwd_block(const Args<T>& a, int bid, int tid, int nthr, char* smem) {
       if (f < nfe) d[f * nb] = mk<T>(v0[f], v1[f]);
   }
   BLOCK_SYNC();
-  const cx<T>* res = buf;
-  if (fft2_supported<T>(px)) {  // in place in buf, tmp as the exchange buffer
-    const SmemIO<T> io{buf, NB};
-    fft2_run<T, -1>(io, io, tmp, NB, px, a.tw, tid, nthr);
-    BLOCK_SYNC();
-  } else {
-    res = fft_batch<T, -1>(buf, tmp, NB, NB, px, a.tw, tid, nthr);
-  }
-  const unsigned mk1 = magic32(k1), mnb = magic32(nb);
+  fft_inplace<T, -1>(buf, NB, 1, NB, px, a.tw, tid, nthr);
+  // split the two real rows' spectra: Z = X[k], Zc = conj(X[n1 - k]) (read at
+  // their digit-reversed positions); row j0 gets (Z + Zc) / 2, row j1
+  // (Z - Zc) / 2i, stored kx-major (consecutive threads, consecutive row pairs)
+  const int* __restrict__ ip = a.idx + px.iperm;
+  const unsigned mnb = magic32(nb), mk1 = magic32(k1);
   for (int w = tid; w < NB * k1; w += nthr) {
-    const int col = magic_div32(w, mk1), k = w - col * k1;
-    const int f = magic_div32(col, mnb), b = col - f * nb;
+    const int rest = magic_div32(w, mnb), b = w - rest * nb;
+    const int f = magic_div32(rest, mk1), k = rest - f * k1;
+    const int col = f * nb + b;
     const int j0 = 2 * (rp0 + b), j1 = j0 + 1;
-    const cx<T> z = res[col + k * NB];
-    const cx<T> zc = conj(res[col + (k == 0 ? 0 : n1 - k) * NB]);
+    const cx<T> z = buf[col + ip[k] * NB];
+    const cx<T> zc = conj(buf[col + ip[k == 0 ? 0 : n1 - k] * NB]);
     const cx<T> sum = z + zc, dif = z - zc;
-    cx<T>* __restrict__ out = (cx<T>*)s.spec + (size_t)f * (size_t)Nc;
-    out[j0 * k1 + k] = mk<T>(sum.x * T(0.5), sum.y * T(0.5));
-    if (j1 < nrows) out[j1 * k1 + k] = mk<T>(dif.y * T(0.5), -dif.x * T(0.5));
+    cx<T>* __restrict__ out = (cx<T>*)s.spec + (size_t)f * (size_t)Nc + (size_t)k * nrows;
+    out[j0] = mk<T>(sum.x * T(0.5), sum.y * T(0.5));
+    if (j1 < nrows) out[j1] = mk<T>(dif.y * T(0.5), -dif.x * T(0.5));
   }
 }
 
-// ------------------------------------------------------------ column accessors
-// y pass: element i of column b of a tile at p[i*stride + b].
-template <typename T>
-struct ColIO {
-  cx<T>* p;
-  int stride;
-  HD cx<T> ld(int i, int b) const { return p[(size_t)i * stride + b]; }
-  HD void st(int i, int b, cx<T> v) const { p[(size_t)i * stride + b] = v; }
-};
+// ------------------------------------------------------------ k-space operators
+HD int signed_freq(int k, int n) { return k > n / 2 ? k - n : k; }
 
-// z pass: column q*nb + b is field q of the group at p[q*nc + i*plane + b];
-// fields q >= gin read as zero and fields q >= gout are not stored.
+// Real factor of the single-field operators at the frequency (m1, m2, m3)
+// (signed): Hartree 4 pi / |G|^2 (0 at G = 0) and vW |G|^2, each times the
+// 1/N forward scale; |G|^2 in the slot's precision.
 template <typename T>
-struct GroupIO {
-  cx<T>* p;
-  int nb, plane, gin, gout;
-  unsigned mnb;
-  long long nc;
-  HD cx<T> ld(int i, int col) const {
-    const int q = magic_div32(col, mnb), b = col - q * nb;
-    return q < gin ? p[(size_t)q * nc + (size_t)i * plane + b] : mk<T>(T(0), T(0));
-  }
-  HD void st(int i, int col, cx<T> v) const {
-    const int q = magic_div32(col, mnb), b = col - q * nb;
-    if (q < gout) p[(size_t)q * nc + (size_t)i * plane + b] = v;
-  }
-};
-
-// z pass, forward: the last step stores element (kz = i, column b) of a
-// single-field group in shared memory, res[b + i*NB], already multiplied by
-// the group's real k-space factor (the same factors as zpass_operator):
-// Hartree 4 pi / |G|^2 (0 at G = 0), vW |G|^2, or the WT kernel plane, each
-// times the 1/N forward scale.
-template <typename T>
-struct ZOpStore {
-  cx<T>* res;
-  int NB, kind, kx0, ky, n3, plane;
-  T rt0, rt1, rt2, rt6, rt7, rt8, ty0, ty1, ty2, sc, c4;
-  const T* kern;  // plane at (ky, kx0)
-  HD void st(int i, int b, cx<T> v) const {
-    T m;
-    if (kind == G_KMUL) {
-      m = kern[i * plane + b] * sc;
-    } else {
-      const int m1 = kx0 + b;
-      const int m3 = i > n3 / 2 ? i - n3 : i;
-      const T tx = rt0 * (T)m1 + ty0 + rt6 * (T)m3;
-      const T ty = rt1 * (T)m1 + ty1 + rt7 * (T)m3;
-      const T tz = rt2 * (T)m1 + ty2 + rt8 * (T)m3;
-      const T g2 = tx * tx + ty * ty + tz * tz;
-      m = kind == G_VW ? g2 * sc : ((m1 == 0 && ky == 0 && i == 0) ? T(0) : c4 / g2);
-    }
-    res[b + i * NB] = v * m;
-  }
-};
-
-// ------------------------------------------------------------ passes 2, 4
-template <typename T>
-HD void ypass_block(const Args<T>& a, int bid, int tid, int nthr, char* smem, int dir) {
-  const Task t = a.tasks[bid];
-  const SlotDev& s = a.slots[t.slot];
-  const Ctl& c = a.ctl[t.slot];
-  if (c.status != ST_RUNNING || c.ev == EV_NONE) return;
-  const int f = t.a, z = t.b, kx0 = tile_kx0(t.c), nb = tile_width(t.c);
-  if (c.ev == EV_ION && f >= (dir < 0 ? s.ion.nspec : 1)) return;
-  if (c.ev == EV_FORCE && f >= (dir < 0 ? 1 : s.ion.nspec)) return;
-  const int n2 = s.n2, k1 = s.k1;
-  cx<T>* buf = (cx<T>*)smem;
-  cx<T>* tmp = buf + nb * n2;
-  cx<T>* __restrict__ sp = (cx<T>*)s.spec + (size_t)f * (size_t)s.Nc + (size_t)z * n2 * k1 + kx0;
-  if (fft2_supported<T>(s.py)) {  // in place, straight from and to the spectra
-    const ColIO<T> io{sp, k1};
-    if (dir < 0) fft2_run<T, -1>(io, io, buf, nb, s.py, a.tw, tid, nthr);
-    else fft2_run<T, 1>(io, io, buf, nb, s.py, a.tw, tid, nthr);
-    return;
-  }
-  const unsigned mnb = magic32(nb);
-  for (int w = tid; w < nb * n2; w += nthr) {
-    const int i = magic_div32(w, mnb), b = w - i * nb;
-    buf[w] = sp[i * k1 + b];
-  }
-  BLOCK_SYNC();
-  const cx<T>* res = fft_batch(buf, tmp, nb, nb, s.py, a.tw, dir, tid, nthr);
-  for (int w = tid; w < nb * n2; w += nthr) {
-    const int i = magic_div32(w, mnb), b = w - i * nb;
-    sp[i * k1 + b] = res[w];
-  }
-}
-
-// ------------------------------------------------------------ pass 3
-// The k-space operator of one z-pass tile: res holds the forward z
-// transforms of the group's gn fields, [kz][q*nb + b] (NB = gn*nb), for kx =
-// kx0 + b and ky; the results replace them in place.
-template <typename T, int KS>
-HD void zpass_operator(const SlotDev& s, int kind, int gn, bool setup_mode, cx<T>* res, int NB, int nb, int kx0,
-                       int ky, int tid, int nthr) {
-  const int n2 = s.n2, n3 = s.n3, k1 = s.k1, plane = n2 * k1, Nc = (int)s.Nc;
-  const int m2 = ky > n2 / 2 ? ky - n2 : ky;
-  const unsigned mnb = magic32(nb);
-  const T* __restrict__ kern = (const T*)s.kern + ky * k1 + kx0;
-  const T sc = (T)s.inv_n;
-  // |G|^2 of the Hartree and vW operators in the slot's precision; the
-  // set-up modes (ion potential, forces) evaluate |G| in FP64.
+struct GFactor {
   T rt[9];
+  T sc, c4;
+  HD void init(const SlotDev& s) {
 #pragma unroll
-  for (int q = 0; q < 9; ++q) rt[q] = (T)s.recip[q];
-  const T ty0 = rt[3] * (T)m2, ty1 = rt[4] * (T)m2, ty2 = rt[5] * (T)m2;
-  const T c4 = (T)(4.0 * PI_D * s.inv_n);
+    for (int q = 0; q < 9; ++q) rt[q] = (T)s.recip[q];
+    sc = (T)s.inv_n;
+    c4 = (T)(4.0 * PI_D * s.inv_n);
+  }
+  HD T operator()(int kind, int m1, int m2, int m3) const {
+    const T tx = rt[0] * (T)m1 + rt[3] * (T)m2 + rt[6] * (T)m3;
+    const T ty = rt[1] * (T)m1 + rt[4] * (T)m2 + rt[7] * (T)m3;
+    const T tz = rt[2] * (T)m1 + rt[5] * (T)m2 + rt[8] * (T)m3;
+    const T g2 = tx * tx + ty * ty + tz * tz;
+    if (kind == G_VW) return g2 * sc;
+    return (m1 == 0 && m2 == 0 && m3 == 0) ? T(0) : c4 / g2;
+  }
+};
+
+// The operator of one z-pass tile: res[i*NB + q*nb + b] holds field q of
+// the group at z position i (frequency kz = permz[i]) and y position y0 + b
+// (ky = permy[y0 + b]), for kx; the results replace the inputs.
+template <typename T, int KS>
+HD void zpass_operator(const SlotDev& s, int kind, int gn, bool setup_mode, cx<T>* res, int NB, int nb, int kx,
+                       int y0, const int* __restrict__ permy, const int* __restrict__ permz, int tid, int nthr) {
+  const int n2 = s.n2, n3 = s.n3, nrows = n2 * n3;
+  const long long Nc = s.Nc;
+  const unsigned mnb = magic32(nb);
+  const T* __restrict__ kern = (const T*)s.kern + (size_t)kx * nrows + y0;
+  const T sc = (T)s.inv_n;
+  GFactor<T> gf;
+  gf.init(s);
   for (int w = tid; w < nb * n3; w += nthr) {
     const int i = magic_div32(w, mnb), b = w - i * nb;
-    const int m1 = kx0 + b;
-    const int m3 = i > n3 / 2 ? i - n3 : i;
-    const int kidx = i * plane + b;
+    const int ky = permy[y0 + b], kz = permz[i];
+    const int m2 = signed_freq(ky, n2), m3 = signed_freq(kz, n3);
+    const int kidx = i * n2 + b;
     cx<T>* e = res + i * NB + b;
     if (kind == G_HARTREE || kind == G_VW) {
-      const T tx = rt[0] * (T)m1 + ty0 + rt[6] * (T)m3;
-      const T ty = rt[1] * (T)m1 + ty1 + rt[7] * (T)m3;
-      const T tz = rt[2] * (T)m1 + ty2 + rt[8] * (T)m3;
-      const T g2 = tx * tx + ty * ty + tz * tz;
-      const T m = kind == G_VW ? g2 * sc : ((m1 == 0 && ky == 0 && i == 0) ? T(0) : c4 / g2);
-      e[0] = e[0] * m;
+      e[0] = e[0] * gf(kind, kx, m2, m3);
       continue;
     }
     double q = 0.0;
     if (setup_mode) {
-      const double gx = s.recip[0] * m1 + s.recip[3] * m2 + s.recip[6] * m3;
-      const double gy = s.recip[1] * m1 + s.recip[4] * m2 + s.recip[7] * m3;
-      const double gz = s.recip[2] * m1 + s.recip[5] * m2 + s.recip[8] * m3;
+      const double gx = s.recip[0] * kx + s.recip[3] * m2 + s.recip[6] * m3;
+      const double gy = s.recip[1] * kx + s.recip[4] * m2 + s.recip[7] * m3;
+      const double gz = s.recip[2] * kx + s.recip[5] * m2 + s.recip[8] * m3;
       q = sqrt(gx * gx + gy * gy + gz * gz);
     }
     switch (kind) {
@@ -668,7 +602,7 @@ HD void zpass_operator(const SlotDev& s, int kind, int gn, bool setup_mode, cx<T
       }
       case G_ION: {  // conj(sum_s V_s(|G|) b1 b2 b3 S_s) N / vol, times the 1/N forward scale
         // (IonElectronPotRecipSpline, IonElectronSpline.f90:180-203)
-        const cx<double> bb = cmul(cmul(s.ion.b1[m1], s.ion.b2[ky]), s.ion.b3[i]);
+        const cx<double> bb = cmul(cmul(s.ion.b1[kx], s.ion.b2[ky]), s.ion.b3[kz]);
         double yr = 0.0, yi = 0.0;
         for (int sp = 0; sp < gn; ++sp) {
           const double v = psp_value(s.ion, sp, q);
@@ -682,9 +616,9 @@ HD void zpass_operator(const SlotDev& s, int kind, int gn, bool setup_mode, cx<T
       }
       default: {  // G_FORCE: rho(G) V_s(|G|) b1 b2 b3 per species, G = 0 excluded
         // (IonElectronForcesSpline, IonElectronSpline.f90:300-330)
-        const cx<double> bb = cmul(cmul(s.ion.b1[m1], s.ion.b2[ky]), s.ion.b3[i]);
+        const cx<double> bb = cmul(cmul(s.ion.b1[kx], s.ion.b2[ky]), s.ion.b3[kz]);
         const cx<T> F = e[0];
-        const bool g0 = m1 == 0 && ky == 0 && i == 0;
+        const bool g0 = kx == 0 && ky == 0 && kz == 0;
         for (int sp = gn - 1; sp >= 0; --sp) {
           const double v = g0 ? 0.0 : psp_value(s.ion, sp, q) * s.inv_n;
           const double fr = (double)F.x * v, fi = (double)F.y * v;
@@ -696,79 +630,133 @@ HD void zpass_operator(const SlotDev& s, int kind, int gn, bool setup_mode, cx<T
   }
 }
 
-// All gn fields of a group are transformed as one batch of gn*nb sequences
-// laid out [kz][q*nb + b].
+// Odd row pitch of a plane or tile held in shared memory with y fastest:
+// transforms along y then take columns at an odd stride (conflict-free).
+HD int odd_pitch(int n) { return n | 1; }
+
+// ------------------------------------------------------------ Y passes (split path)
+// Task (field f, kx, z tile): nz columns of n2 contiguous values (one per
+// z), transformed along y in place: forward (dir < 0) natural -> digit
+// reversed, inverse (dir > 0) back.
+template <typename T>
+HD void ypass_block(const Args<T>& a, int bid, int tid, int nthr, char* smem, int dir) {
+  const Task t = a.tasks[bid];
+  const SlotDev& s = a.slots[t.slot];
+  const Ctl& c = a.ctl[t.slot];
+  if (c.status != ST_RUNNING || c.ev == EV_NONE) return;
+  const int f = t.a, kx = t.b, z0 = tile_first(t.c), nz = tile_width(t.c);
+  if (c.ev == EV_ION && f >= (dir < 0 ? s.ion.nspec : 1)) return;
+  if (c.ev == EV_FORCE && f >= (dir < 0 ? 1 : s.ion.nspec)) return;
+  const int n2 = s.n2, P = odd_pitch(n2);
+  cx<T>* buf = (cx<T>*)smem;
+  cx<T>* __restrict__ sp =
+      (cx<T>*)s.spec + (size_t)f * (size_t)s.Nc + (size_t)kx * (n2 * s.n3) + (size_t)z0 * n2;
+  const unsigned mn2 = magic32(n2);
+  for (int w = tid; w < nz * n2; w += nthr) {
+    const int zc = magic_div32(w, mn2), y = w - zc * n2;
+    buf[zc * P + y] = sp[w];
+  }
+  BLOCK_SYNC();
+  if (dir < 0) fft_inplace<T, -1>(buf, nz, P, 1, s.py, a.tw, tid, nthr);
+  else fft_inplace<T, 1>(buf, nz, P, 1, s.py, a.tw, tid, nthr);
+  for (int w = tid; w < nz * n2; w += nthr) {
+    const int zc = magic_div32(w, mn2), y = w - zc * n2;
+    sp[w] = buf[zc * P + y];
+  }
+}
+
+// ------------------------------------------------------------ Z pass (split path)
+// Task (group g, kx, y tile): the group's gn fields at ny consecutive y
+// positions, all n3 z values, as gn*ny columns [z][q*ny + b]: forward FFT
+// along z, the group's operator, inverse FFT along z.
 template <typename T, int KS>
 HD void zpass_block(const Args<T>& a, int bid, int tid, int nthr, char* smem) {
   const Task t = a.tasks[bid];
   const SlotDev& s = a.slots[t.slot];
   const Ctl& c = a.ctl[t.slot];
   if (c.status != ST_RUNNING || c.ev == EV_NONE) return;
-  const int g = t.a, ky = t.b, kx0 = tile_kx0(t.c), nb = tile_width(t.c);
+  const int g = t.a, kx = t.b, y0 = tile_first(t.c), nb = tile_width(t.c);
   const int ev = c.ev;
   const bool setup_mode = ev == EV_ION || ev == EV_FORCE;
   if (setup_mode && g != 0) return;
-  const int n2 = s.n2, n3 = s.n3, k1 = s.k1;
+  const int n2 = s.n2, n3 = s.n3, nrows = n2 * n3;
   const int kind = ev == EV_ION ? G_ION : ev == EV_FORCE ? G_FORCE : s.group_kind[g];
   const int gn = setup_mode ? s.ion.nspec : s.group_nf[g];
   const int gin = ev == EV_FORCE ? 1 : gn;  // fields loaded
   const int gout = ev == EV_ION ? 1 : gn;   // fields stored
   const int NB = gn * nb;
-  const int plane = n2 * k1;
-  const int Nc = (int)s.Nc;
+  const long long Nc = s.Nc;
   cx<T>* __restrict__ spec =
-      (cx<T>*)s.spec + (size_t)(setup_mode ? 0 : s.group_f0[g]) * (size_t)Nc + ky * k1 + kx0;
+      (cx<T>*)s.spec + (size_t)(setup_mode ? 0 : s.group_f0[g]) * (size_t)Nc + (size_t)kx * nrows + y0;
   cx<T>* buf = (cx<T>*)smem;
-  cx<T>* tmp = buf + NB * n3;
   const unsigned mNB = magic32(NB), mnb = magic32(nb);
-  if (fft2_supported<T>(s.pz)) {  // forward into tmp, operator, inverse back to the spectra
-    const GroupIO<T> gio{spec, nb, plane, gin, gout, mnb, (long long)Nc};
-    const SmemIO<T> o{tmp, NB};
-    if (!setup_mode && gn == 1 && (kind == G_HARTREE || kind == G_VW || kind == G_KMUL)) {
-      // single-field groups: the operator is applied as the forward transform stores
-      const int m2 = ky > n2 / 2 ? ky - n2 : ky;
-      ZOpStore<T> zo;
-      zo.res = tmp;
-      zo.NB = NB;
-      zo.kind = kind;
-      zo.kx0 = kx0;
-      zo.ky = ky;
-      zo.n3 = n3;
-      zo.plane = plane;
-      zo.rt0 = (T)s.recip[0]; zo.rt1 = (T)s.recip[1]; zo.rt2 = (T)s.recip[2];
-      zo.rt6 = (T)s.recip[6]; zo.rt7 = (T)s.recip[7]; zo.rt8 = (T)s.recip[8];
-      zo.ty0 = (T)s.recip[3] * (T)m2; zo.ty1 = (T)s.recip[4] * (T)m2; zo.ty2 = (T)s.recip[5] * (T)m2;
-      zo.sc = (T)s.inv_n;
-      zo.c4 = (T)(4.0 * PI_D * s.inv_n);
-      zo.kern = (const T*)s.kern + ky * k1 + kx0;
-      const ColIO<T> col{spec, plane};  // one field: column b at spec[i*plane + b]
-      fft2_run<T, -1>(col, zo, buf, NB, s.pz, a.tw, tid, nthr);
-      BLOCK_SYNC();
-      fft2_run<T, 1>(o, col, buf, NB, s.pz, a.tw, tid, nthr);
-      return;
+  for (int w = tid; w < NB * n3; w += nthr) {
+    const int i = magic_div32(w, mNB), qb = w - i * NB;
+    const int q = magic_div32(qb, mnb), b = qb - q * nb;
+    buf[w] = q < gin ? spec[(size_t)q * Nc + i * n2 + b] : mk<T>(T(0), T(0));
+  }
+  BLOCK_SYNC();
+  fft_inplace<T, -1>(buf, NB, 1, NB, s.pz, a.tw, tid, nthr);
+  zpass_operator<T, KS>(s, kind, gn, setup_mode, buf, NB, nb, kx, y0, a.idx + s.py.perm, a.idx + s.pz.perm, tid,
+                        nthr);
+  BLOCK_SYNC();
+  fft_inplace<T, 1>(buf, NB, 1, NB, s.pz, a.tw, tid, nthr);
+  for (int w = tid; w < NB * n3; w += nthr) {
+    const int i = magic_div32(w, mNB), qb = w - i * NB;
+    const int q = magic_div32(qb, mnb), b = qb - q * nb;
+    if (q < gout) spec[(size_t)q * Nc + i * n2 + b] = buf[w];
+  }
+}
+
+// ------------------------------------------------------------ YZ pass (fused path)
+// Task (group g, kx) of a single-field group: the whole (y, z) plane of the
+// field at kx (n2*n3 contiguous values) in shared memory, rows of odd pitch
+// P: forward FFT along y (columns z) and z (columns y), the operator at the
+// digit-reversed positions, inverse FFT along z and y, one read and one
+// write of the plane.
+template <typename T>
+HD void yzpass_block(const Args<T>& a, int bid, int tid, int nthr, char* smem) {
+  const Task t = a.tasks[bid];
+  const SlotDev& s = a.slots[t.slot];
+  const Ctl& c = a.ctl[t.slot];
+  const int ev = c.ev;
+  if (c.status != ST_RUNNING || ev == EV_NONE || ev == EV_ION || ev == EV_FORCE) return;
+  const int g = t.a, kx = t.b;
+  const int n2 = s.n2, n3 = s.n3, nrows = n2 * n3, P = odd_pitch(n2);
+  const int kind = s.group_kind[g];
+  cx<T>* __restrict__ plane = (cx<T>*)s.spec + (size_t)s.group_f0[g] * (size_t)s.Nc + (size_t)kx * nrows;
+  cx<T>* buf = (cx<T>*)smem;
+  const unsigned mn2 = magic32(n2);
+  for (int w = tid; w < nrows; w += nthr) {
+    const int z = magic_div32(w, mn2), y = w - z * n2;
+    buf[z * P + y] = plane[w];
+  }
+  BLOCK_SYNC();
+  fft_inplace<T, -1>(buf, n3, P, 1, s.py, a.tw, tid, nthr);
+  fft_inplace<T, -1>(buf, n2, 1, P, s.pz, a.tw, tid, nthr);
+  const int* __restrict__ permy = a.idx + s.py.perm;
+  const int* __restrict__ permz = a.idx + s.pz.perm;
+  if (kind == G_KMUL) {
+    const T* __restrict__ kern = (const T*)s.kern + (size_t)kx * nrows;
+    const T sc = (T)s.inv_n;
+    for (int w = tid; w < nrows; w += nthr) {
+      const int z = magic_div32(w, mn2), y = w - z * n2;
+      buf[z * P + y] = buf[z * P + y] * (kern[w] * sc);
     }
-    fft2_run<T, -1>(gio, o, buf, NB, s.pz, a.tw, tid, nthr);
-    BLOCK_SYNC();
-    zpass_operator<T, KS>(s, kind, gn, setup_mode, tmp, NB, nb, kx0, ky, tid, nthr);
-    BLOCK_SYNC();
-    fft2_run<T, 1>(o, gio, buf, NB, s.pz, a.tw, tid, nthr);
-    return;
-  }
-  for (int w = tid; w < NB * n3; w += nthr) {
-    const int i = magic_div32(w, mNB), qb = w - i * NB;
-    const int q = magic_div32(qb, mnb), b = qb - q * nb;
-    buf[w] = q < gin ? spec[(size_t)q * Nc + i * plane + b] : mk<T>(T(0), T(0));
+  } else {
+    GFactor<T> gf;
+    gf.init(s);
+    for (int w = tid; w < nrows; w += nthr) {
+      const int z = magic_div32(w, mn2), y = w - z * n2;
+      buf[z * P + y] = buf[z * P + y] * gf(kind, kx, signed_freq(permy[y], n2), signed_freq(permz[z], n3));
+    }
   }
   BLOCK_SYNC();
-  cx<T>* res = fft_batch<T, -1>(buf, tmp, NB, NB, s.pz, a.tw, tid, nthr);
-  cx<T>* oth = res == buf ? tmp : buf;
-  zpass_operator<T, KS>(s, kind, gn, setup_mode, res, NB, nb, kx0, ky, tid, nthr);
-  BLOCK_SYNC();
-  const cx<T>* out = fft_batch<T, 1>(res, oth, NB, NB, s.pz, a.tw, tid, nthr);
-  for (int w = tid; w < NB * n3; w += nthr) {
-    const int i = magic_div32(w, mNB), qb = w - i * NB;
-    const int q = magic_div32(qb, mnb), b = qb - q * nb;
-    if (q < gout) spec[(size_t)q * Nc + i * plane + b] = out[w];
+  fft_inplace<T, 1>(buf, n2, 1, P, s.pz, a.tw, tid, nthr);
+  fft_inplace<T, 1>(buf, n3, P, 1, s.py, a.tw, tid, nthr);
+  for (int w = tid; w < nrows; w += nthr) {
+    const int z = magic_div32(w, mn2), y = w - z * n2;
+    plane[w] = buf[z * P + y];
   }
 }
 
@@ -961,42 +949,35 @@ HD void xinv_block(const Args<T>& a, int bid, int tid, int nthr, char* smem) {
   const int nf = ev == EV_ION ? 1 : ev == EV_FORCE ? s.ion.nspec : s.nf;
   const int NB = nf * nb;
   const int nrows = s.n2 * s.n3;
-  const int Nc = (int)s.Nc;
+  const long long Nc = s.Nc;
   const cx<T>* __restrict__ spec = (const cx<T>*)s.spec;
   cx<T>* buf = (cx<T>*)smem;
-  cx<T>* tmp = buf + NB * n1;
-  const bool even = (n1 % 2) == 0;
-  const int nyq = even ? n1 / 2 : -1;
-  // gather: consecutive threads read consecutive k of one half-spectrum row
-  const unsigned mn1 = magic32(n1), mnb = magic32(nb);
-  for (int w = tid; w < NB * n1; w += nthr) {
-    const int fb = magic_div32(w, mn1), k = w - fb * n1;
-    const int f = magic_div32(fb, mnb), b = fb - f * nb;
-    const cx<T>* sp = spec + (size_t)f * Nc;
+  const int nyq = (n1 % 2) == 0 ? n1 / 2 : -1;
+  // gather: consecutive threads read the consecutive row pairs of one kx
+  // (kx-major spectra); the packed complex sequence Z = A + i B of the two
+  // rows' spectra goes to the digit-reversed positions the inverse
+  // transform takes, Z[k] from the stored k < k1 and Z[n1 - k] from its
+  // conjugate symmetry
+  const int* __restrict__ ip = a.idx + s.px.iperm;
+  const unsigned mnb = magic32(nb), mk1 = magic32(k1);
+  for (int w = tid; w < NB * k1; w += nthr) {
+    const int rest = magic_div32(w, mnb), b = w - rest * nb;
+    const int f = magic_div32(rest, mk1), k = rest - f * k1;
+    const cx<T>* sp = spec + (size_t)f * Nc + (size_t)k * nrows;
     const int j0 = 2 * (rp0 + b), j1 = j0 + 1;
-    const bool has1 = j1 < nrows;
-    const bool lo = k < k1;
-    const int kk = lo ? k : n1 - k;
-    cx<T> A = sp[j0 * k1 + kk];
-    cx<T> B = has1 ? sp[j1 * k1 + kk] : mk<T>(T(0), T(0));
-    if (!lo) {
-      A.y = -A.y;
-      B.y = -B.y;
-    } else if (k == 0 || k == nyq) {  // c2r ignores these imaginary parts
-      A.y = T(0);
-      B.y = T(0);
+    cx<T> A = sp[j0];
+    cx<T> B = j1 < nrows ? sp[j1] : mk<T>(T(0), T(0));
+    const int col = f * nb + b;
+    if (k == 0 || k == nyq) {  // c2r ignores these imaginary parts
+      buf[ip[k] * NB + col] = mk<T>(A.x, B.x);
+    } else {
+      buf[ip[k] * NB + col] = mk<T>(A.x - B.y, A.y + B.x);
+      buf[ip[n1 - k] * NB + col] = mk<T>(A.x + B.y, B.x - A.y);
     }
-    buf[k * NB + fb] = mk<T>(A.x - B.y, A.y + B.x);
   }
   BLOCK_SYNC();
+  fft_inplace<T, 1>(buf, NB, 1, NB, s.px, a.tw, tid, nthr);
   const cx<T>* res = buf;
-  if (fft2_supported<T>(s.px)) {  // in place in buf, tmp as the exchange buffer
-    const SmemIO<T> io{buf, NB};
-    fft2_run<T, 1>(io, io, tmp, NB, s.px, a.tw, tid, nthr);
-    BLOCK_SYNC();
-  } else {
-    res = fft_batch<T, 1>(buf, tmp, NB, NB, s.px, a.tw, tid, nthr);
-  }
   if (setup_mode) {
     // EV_ION: ionPotReal; EV_FORCE: the per-species Factor arrays in buf[B_B + s]
     const unsigned m2n1s = magic32(2 * n1);
@@ -1014,7 +995,7 @@ HD void xinv_block(const Args<T>& a, int bid, int tid, int nthr, char* smem) {
     double zero[NCH];
 #pragma unroll
     for (int ch = 0; ch < NCH; ++ch) zero[ch] = 0.0;
-    store_partials<0, 0>(s, ordinal, zero, (double*)(tmp + NB * n1), tid, nthr);
+    store_partials<0, 0>(s, ordinal, zero, (double*)(buf + NB * n1), tid, nthr);
     return;
   }
 
@@ -1060,8 +1041,8 @@ HD void xinv_block(const Args<T>& a, int bid, int tid, int nthr, char* smem) {
       else xinv_points<T, KS, EV_RHO, false>(e, acc, tid, nthr);
       break;
   }
-  if (ev == EV_CG) store_partials<CH_M0, CH_M0 + 1>(s, ordinal, acc, (double*)(tmp + NB * n1), tid, nthr);
-  else store_partials(s, ordinal, acc, (double*)(tmp + NB * n1), tid, nthr);
+  if (ev == EV_CG) store_partials<CH_M0, CH_M0 + 1>(s, ordinal, acc, (double*)(buf + NB * n1), tid, nthr);
+  else store_partials(s, ordinal, acc, (double*)(buf + NB * n1), tid, nthr);
 }
 
 }  // namespace ofdft

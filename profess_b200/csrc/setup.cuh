@@ -185,12 +185,31 @@ HD double spline_val(const double* t, const double* y, const double* ypp, int n,
   return y[lo] + dt * (tmp1 + tmp2 + dt * (0.5 * ypp[lo] + dt * (tmp3 / (6.0 * h))));
 }
 
+// Frequencies (kx, ky, kz) of element i of a kernel plane in the engine's
+// layout: kx-major planes of n2*n3 values in the digit-reversed order of
+// the slot's y and z transforms (idx: the plan index table).
+HD void kernel_freq(const SlotDev& s, const int* idx, long long i, int& kx, int& ky, int& kz) {
+  const int nrows = s.n2 * s.n3;
+  kx = (int)(i / nrows);
+  const int rem = (int)(i - (long long)kx * nrows);
+  const int qz = rem / s.n2, qy = rem - qz * s.n2;
+  ky = idx[s.py.perm + qy];
+  kz = idx[s.pz.perm + qz];
+}
+
+// Index in the reference layout keKernel(k1G, k2G, k3G, plane) of element i
+// (of all planes) in the engine's layout.
+HD long long kernel_source_index(const SlotDev& s, const int* idx, long long i) {
+  const long long p = i / s.Nc, e = i - p * s.Nc;
+  int kx, ky, kz;
+  kernel_freq(s, idx, e, kx, ky, kz);
+  return p * s.Nc + kx + (long long)s.k1 * (ky + (long long)s.n2 * kz);
+}
+
 template <typename T>
-HDNI void fill_kernel_point(const SlotDev& s, const KernArgs& ka, int kind, int idx) {
-  const int k1 = s.k1;
-  const int m1 = idx % k1;
-  const int rest = idx / k1;
-  const int ky = rest % s.n2, kz = rest / s.n2;
+HDNI void fill_kernel_point(const SlotDev& s, const int* idxtab, const KernArgs& ka, int kind, int idx) {
+  int m1, ky, kz;
+  kernel_freq(s, idxtab, idx, m1, ky, kz);
   const double q = qnorm_at(s, m1, ky, kz);
   T* kern = (T*)s.kern;
   if (kind == KIN_WT) {

@@ -3,9 +3,9 @@
 // A slot is one cell being evaluated or solved.  Its grid, lattice, functional
 // parameters and device buffers live in a SlotDev record; its optimiser state
 // lives in a Ctl record that the last block of every kernel updates for that
-// slot.  All arrays of a slot are x-fastest (Fortran order, as the reference's
-// rho(n1,n2,n3)); half spectra are (k1 = n1/2+1, n2, n3) complex, also
-// x-fastest.
+// slot.  The real-space arrays of a slot are x-fastest (Fortran order, as the
+// reference's rho(n1,n2,n3)); half spectra (k1 = n1/2+1 planes of n2*n3
+// complex values) are kx-major, each (y, z) plane contiguous with y fastest.
 #pragma once
 #include "cx.cuh"
 #include "dcsrch.cuh"
@@ -91,7 +91,6 @@ struct SlotDev {
   double dv, inv_n, vol;
   int kinetic, nf, ngroups, alpha_eq_beta;
   int pow56;       // alpha == beta == 5/6: rho^(5/6) = sqrt(rho) * cbrt(rho)
-  int tx;          // kx tile width of the Y/Z passes
   int rp;          // row pairs per X-pass task
   int group_kind[MAX_GROUPS];
   int group_f0[MAX_GROUPS];
@@ -142,16 +141,16 @@ struct Task {
   int slot, a, b, c;
 };
 
-// kx tiles of the y and z passes: ceil(k1 / tx) tiles of nearly equal width
-// (a 49-wide half spectrum becomes 13 + 12 + 12 + 12, not 16 + 16 + 16 + 1).
-// A task's c field holds kx0 | (width << 16).
+// Tiles of the split y and z passes: ceil(n / tx) tiles of nearly equal width
+// over n columns (49 columns in tiles of 16 become 13 + 12 + 12 + 12, not
+// 16 + 16 + 16 + 1).  A task's c field holds the first column | (width << 16).
 HD int tile_count(int k1, int tx) { return (k1 + tx - 1) / tx; }
 HD int tile_code(int k1, int tx, int t) {
   const int nt = tile_count(k1, tx), base = k1 / nt, rem = k1 % nt;
   const int kx0 = t * base + (t < rem ? t : rem);
   return kx0 | ((base + (t < rem ? 1 : 0)) << 16);
 }
-HD int tile_kx0(int c) { return c & 0xffff; }
+HD int tile_first(int c) { return c & 0xffff; }
 HD int tile_width(int c) { return c >> 16; }
 
 }  // namespace ofdft

@@ -3,32 +3,49 @@
 
 Workload (the configuration the headline metric is quoted on): FCC Al 4x4x4
 supercell, 256 atoms, a = 4.05 A, seeded Gaussian displacements sigma =
-0.05 A, Heine-Abarenkov model pseudopotential (Z = 3, r_c = 1.15 bohr, well depth A = 0.1 Ha),
-WT + TF + vW + LDA, 96^3 grid.  One "step" is a batch of B such cells (distinct
-seeds) each solved to convergence by the sqrt-density truncated-Newton method:
-FP32 evaluations until the line search reaches the FP32 precision floor (or
-|dL/dphi| < 3e-5), then at most three FP64 Newton iterations to |dL/dphi| <
-1e-6 (mixed precision).  The plain FP64 GPU path (FP64 throughout, to
-|dL/dphi| < 1e-6) is timed on the same cells for comparison, and the mixed
-energies (eV/atom) and forces (eV/A) are checked against it.
+0.05 A, the bare Heine-Abarenkov model pseudopotential (Z = 3, r_c = 1.15
+bohr, well depth A = 0.1 Ha), WT + TF + vW + LDA, 96^3 grid.  One "step" is a
+batch of B such cells (distinct seeds) each solved to convergence by the
+sqrt-density truncated-Newton method: FP32 evaluations until the line search
+reaches the FP32 precision floor (or |dL/dphi| < 3e-5), then at most three
+FP64 Newton iterations to |dL/dphi| < 1e-6 (mixed precision).  The plain
+FP64 GPU path (FP64 throughout, to |dL/dphi| < 1e-6) is timed on the same
+cells for comparison, and the mixed energies (eV/atom) and forces (eV/A) are
+checked against it.
 
 value  : solves/s of the mixed path, initial densities resident in HBM,
          device time (CUDA events on the engine stream), max over ranks.
 e2e    : the same through the public API with host densities (the initial
          densities H2D from pinned host arrays and the result densities and
          energies D2H into pinned host arrays, every step).
-Multi-GPU: independent replicas (each rank its own batch), scaling "weak".
+errors_vs_oracle : the first cell's converged mixed and FP64 GPU solves
+         against the oracle's FP64 solve from the same initial density (every
+         energy term, forces) and the FP32/FP64 potential at the oracle's
+         converged density (RMS), outside the timed regions.
+serving : a short seeded request stream of the serving mix (Al/Mg cells of
+         32-2048 atoms, grids 32^3-256^3, 70 % WT / 30 % WGC) run as mixed
+         and as plain FP64 requests on the same cells: saturated capacity,
+         p50/p99 latency at 80 % of it, and the mixed requests' energy error
+         against the FP64 ones.
+Multi-GPU: independent replicas (each rank its own batch), scaling "weak";
+`--gpus N` without a launcher starts N ranks itself (torch.distributed.run).
 Data: synthetic, seeded.  Between timed steps the working set (B cells x
 ~160 MB) exceeds the 126 MB L2, so no L2 flush is needed.
 
 --impl reference runs the CPU restatement of the reference's path (the
 oracle: FP64 NumPy/SciPy, all host cores) on the same workload.
+
+With no GPU and PROFESS_B200_LIB naming the host-emulation build of the
+engine (a test harness), the GPU arm runs on the host: timings come from the
+host clock and the line is marked "emulated".
 """
 from __future__ import annotations
 
 import argparse
+import hashlib
 import json
 import os
+import socket
 import statistics
 import subprocess
 import sys
@@ -43,6 +60,8 @@ sys.path.insert(0, ROOT)
 METRIC = "OF-DFT density solves/s & p50/p99 latency, mixed vs FP64 GPU at 1e-5 eV/atom"
 UNIT = "solves/s"
 HBM_FALLBACK = 6650.0
+HA_EV = 27.211396132
+BOHR_ANG = 0.529177208607388
 
 
 def _peaks():
@@ -54,33 +73,49 @@ def _peaks():
         return HBM_FALLBACK, "fallback"
 
 
+def source_sha() -> str:
+    """SHA-256 (first 16 hex digits) of the engine's CUDA sources: the build a
+    profile describes."""
+    h = hashlib.sha256()
+    csrc = os.path.join(ROOT, "profess_b200", "csrc")
+    for name in sorted(os.listdir(csrc)):
+        if name.endswith((".cu", ".cuh")):
+            with open(os.path.join(csrc, name), "rb") as fh:
+                h.update(name.encode() + b"\0" + fh.read())
+    return h.hexdigest()[:16]
+
+
 def _traffic_per_eval():
     """DRAM bytes of one 96^3 WT potential evaluation of one FP32 and one FP64
-    slot (passes 1-5, from the committed ncu summary), or None."""
+    slot from the committed ncu summary, or None when the summary was taken on
+    other sources than the ones built now."""
     path = os.path.join(ROOT, "profiles", "eval_traffic.txt")
     vals = {}
     try:
         with open(path) as fh:
             for ln in fh:
-                for key in ("dram_bytes_per_eval_fp32_96:", "dram_bytes_per_eval_fp64_96:"):
+                for key in ("dram_bytes_per_eval_fp32_96:", "dram_bytes_per_eval_fp64_96:", "source_sha:"):
                     if ln.startswith(key):
-                        vals[key[:-1]] = float(ln.split(":")[1])
+                        vals[key[:-1]] = ln.split(":", 1)[1].strip()
     except OSError:
         return None
-    if len(vals) < 2:
+    if vals.get("source_sha") != source_sha() or len(vals) < 3:
         return None
-    return vals["dram_bytes_per_eval_fp32_96"], vals["dram_bytes_per_eval_fp64_96"]
+    return float(vals["dram_bytes_per_eval_fp32_96"]), float(vals["dram_bytes_per_eval_fp64_96"])
 
 
 class ClockSampler:
     """nvidia-smi samples of SM clock and throttle reasons during the timed region."""
 
-    def __init__(self, device=0):
+    def __init__(self, device=0, enabled=True):
         self.device = device
         self.proc = None
         self.lines = []
+        self.enabled = enabled
 
     def start(self):
+        if not self.enabled:
+            return
         cmd = ["nvidia-smi", "-i", str(self.device),
                "--query-gpu=clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.hw_slowdown,"
                "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
@@ -98,7 +133,8 @@ class ClockSampler:
 
     def stop(self):
         if not self.proc:
-            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+            return {"sm_mhz": None, "sm_max_mhz": None,
+                    "reasons": ["nvidia-smi unavailable" if self.enabled else "no GPU (host emulation)"]}
         self.proc.terminate()
         try:
             self.proc.wait(timeout=5)
@@ -129,30 +165,67 @@ def _dist():
     return ws, rank, local
 
 
+def _free_port():
+    s = socket.socket()
+    s.bind(("127.0.0.1", 0))
+    port = s.getsockname()[1]
+    s.close()
+    return port
+
+
+def _emulated():
+    """No GPU, and the engine library named by PROFESS_B200_LIB (the host
+    emulation build): the CPU test harness of this script."""
+    import torch
+    return (not torch.cuda.is_available()) and bool(os.environ.get("PROFESS_B200_LIB"))
+
+
 # --------------------------------------------------------------------------- CPU restatement
 def oracle_functional(cell):
-    sys.path.insert(0, os.path.join(ROOT, "tests"))
+    """(oracle cell, oracle functional) of a synthetic workload cell."""
     from oracle import cellsetup as cs, ewald as ew, functional as fn, kedf_kernels as kk
     from profess_b200 import workloads as wl
-    mx, vals = wl.heine_abarenkov_table(float(cell.species[0].charge), 1.15 if cell.species[0].charge == 3 else 1.3, 0.1)
-    osp = cs.species_from_table(mx, vals, cell.species[0].name)
+    sp = cell.species[0]
+    mx, vals = wl.heine_abarenkov_table(float(sp.charge), 1.15 if sp.charge == 3 else 1.3, 0.1)
+    osp = cs.species_from_table(mx, vals, sp.name)
     ocell = cs.Cell(lattice=cell.lattice, frac=cell.frac, species_of_ion=cell.species_of_ion, species=[osp])
     n = cell.grid
     qt = cs.q_table(ocell.recip, *n)
     rho_avg = ocell.num_electrons / ocell.vol
-    kern = kk.wt_kernel(qt, rho_avg, cell.alpha, cell.beta, 1.0, 1.0)[None]
+    if cell.kinetic == 4:
+        kern = kk.wt_kernel(qt, rho_avg, cell.alpha, cell.beta, 1.0, 1.0)[None]
+    else:
+        kern = kk.wgc_kernels(qt, rho_avg, cell.gamma, kk.wgc_radial_tables(cell.alpha, cell.beta, cell.gamma))
     vion = cs.ion_potential_real(ocell, *n)
     e_ii, _ = ew.ewald(ocell.lattice, ocell.frac, ocell.charges())
-    return fn.Functional(kinetic=4, n=tuple(n), dv=ocell.vol / float(np.prod(n)), qtab=qt, kernel=kern,
-                         ion_pot=vion, ion_ion=e_ii, alpha=cell.alpha, beta=cell.beta, rho_s=rho_avg)
+    f = fn.Functional(kinetic=cell.kinetic, n=tuple(n), dv=ocell.vol / float(np.prod(n)), qtab=qt, kernel=kern,
+                      ion_pot=vion, ion_ion=e_ii, alpha=cell.alpha, beta=cell.beta, rho_s=rho_avg)
+    return ocell, f
 
 
-def cpu_solve_time(cell, rho0):
+def cpu_solve(f, rho0):
+    """One FP64 NTN solve by the oracle on every host core: (seconds, result)."""
     from oracle import ntn
-    f = oracle_functional(cell)
     t0 = time.perf_counter()
     r = ntn.NtnSolver(f, ntn.NtnOptions(conv_check="POT", pot_tol=1.0e-6)).solve(rho0)
     return time.perf_counter() - t0, r
+
+
+def cpu_one_core(f, rho, evals_per_solve, k=3):
+    """Solves/s of the oracle on one core, from k potential evaluations timed on
+    one core and the evaluations per solve of the all-core solve."""
+    from oracle import cellsetup as cs, functional as fn
+    old = cs.FFT_WORKERS
+    cs.FFT_WORKERS = 1
+    try:
+        fn.calculate_potential_plus(f, rho)
+        t0 = time.perf_counter()
+        for _ in range(k):
+            fn.calculate_potential_plus(f, rho)
+        t_eval = (time.perf_counter() - t0) / k
+    finally:
+        cs.FFT_WORKERS = old
+    return 1.0 / (t_eval * evals_per_solve), t_eval
 
 
 def run_reference(args):
@@ -160,18 +233,17 @@ def run_reference(args):
     if rank != 0:
         return 0
     from profess_b200 import workloads as wl
+    from oracle import functional as fn
     cell = wl.config_cell(2, seed=0)
     rho0 = wl.initial_density(cell, seed=0)
-    f = oracle_functional(cell)
-    from oracle import functional as fn, ntn
+    _, f = oracle_functional(cell)
     # warm-up: one potential evaluation per requested warm-up step (imports, FFT plans, page faults)
     for _ in range(max(1, args.warmup)):
         fn.calculate_potential_plus(f, rho0)
     times = []
     for _ in range(args.steps):
-        t0 = time.perf_counter()
-        ntn.NtnSolver(f, ntn.NtnOptions(conv_check="POT", pot_tol=1.0e-6)).solve(rho0)
-        times.append(time.perf_counter() - t0)
+        t, _ = cpu_solve(f, rho0)
+        times.append(t)
     tot = sum(times)
     v = args.steps / tot
     cores = os.cpu_count() or 1
@@ -179,7 +251,8 @@ def run_reference(args):
            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * tot / args.steps,
            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
            "data": "synthetic (seeded)",
-           "config": {"workload": "FCC Al 4x4x4 (256 atoms), 96^3, WT+TF+vW+LDA, bare Heine-Abarenkov psp (no GNH smoothing), NTN to potNorm<1e-6",
+           "config": {"workload": "FCC Al 4x4x4 (256 atoms), 96^3, WT+TF+vW+LDA, bare Heine-Abarenkov psp "
+                                  "(no GNH smoothing), NTN to potNorm<1e-6",
                       "batch_per_step": 1, "parallelism": "cpu"},
            "cpu_baseline": {"value": v, "unit": UNIT, "cores": cores, "kind": "port",
                             "sample": "%d full FP64 NTN solve(s) of the workload by the oracle "
@@ -193,11 +266,12 @@ def run_reference(args):
 
 
 # --------------------------------------------------------------------------- GPU arm
+PSP = "bare Heine-Abarenkov psp (no GNH smoothing)"
 WORKLOADS = {
-    "cfg2": "FCC Al 4x4x4 (256 atoms), a=4.05 A, sigma=0.05 A, 96^3, WT(alpha=beta=5/6)+TF+vW+LDA, bare Heine-Abarenkov psp (no GNH smoothing)",
-    "cfg1": "FCC Al conventional cell (4 atoms), sigma=0.02 A, 32^3, WT+TF+vW+LDA, bare Heine-Abarenkov psp (no GNH smoothing)",
-    "cfg3": "64 FCC Al cells n^3 (n~U{2..5}, 32-500 atoms), a=4.05 A (1+-2%), 48^3-120^3, WT, one batch",
-    "cfg4": "hcp Mg 8x8x9 (1152 atoms), a=3.21 A, c/a=1.624, sigma=0.05 A, 160x160x256, WGC 2nd order",
+    "cfg2": "FCC Al 4x4x4 (256 atoms), a=4.05 A, sigma=0.05 A, 96^3, WT(alpha=beta=5/6)+TF+vW+LDA, " + PSP,
+    "cfg1": "FCC Al conventional cell (4 atoms), sigma=0.02 A, 32^3, WT+TF+vW+LDA, " + PSP,
+    "cfg3": "64 FCC Al cells n^3 (n~U{2..5}, 32-500 atoms), a=4.05 A (1+-2%), 48^3-120^3, WT, one batch, " + PSP,
+    "cfg4": "hcp Mg 8x8x9 (1152 atoms), a=3.21 A, c/a=1.624, sigma=0.05 A, 160x160x256, WGC 2nd order, " + PSP,
 }
 
 
@@ -220,27 +294,124 @@ def eval_bytes(cell, s):
     return s * n * (2 * F + 4 + k / 2.0)
 
 
+class Runtime:
+    """Placement and timing of the GPU arm: one GPU per rank with CUDA events
+    on the engine's stream, or (host emulation, a CPU test harness) the host
+    clock.  Collectives (barriers, max/sum over ranks) go over NCCL, or gloo
+    in the emulation."""
+
+    def __init__(self, args):
+        import torch
+        self.torch = torch
+        self.ws, self.rank, self.local = _dist()
+        self.emulated = _emulated()
+        if not self.emulated:
+            if not torch.cuda.is_available():
+                raise SystemExit("bench.py needs a CUDA GPU")
+            torch.cuda.set_device(self.local)
+        self.dist = None
+        if self.ws > 1:
+            import datetime
+            import torch.distributed as dist
+            dist.init_process_group("gloo" if self.emulated else "nccl", timeout=datetime.timedelta(seconds=900))
+            self.dist = dist
+        self.stream = None
+        self._pinned = []
+
+    def bind(self, eng):
+        if not self.emulated:
+            self.stream = self.torch.cuda.ExternalStream(eng.stream())
+
+    def sync(self):
+        if not self.emulated:
+            self.torch.cuda.synchronize()
+
+    def barrier(self):
+        if self.dist is not None:
+            self.dist.barrier()
+        self.sync()
+
+    def _reduce(self, x, op):
+        if self.dist is None:
+            return x
+        dev = "cpu" if self.emulated else "cuda"
+        t = self.torch.tensor([float(x)], dtype=self.torch.float64, device=dev)
+        self.dist.all_reduce(t, op=op)
+        return float(t.item())
+
+    def max_over_ranks(self, x):
+        return self._reduce(x, None if self.dist is None else self.dist.ReduceOp.MAX)
+
+    def sum_over_ranks(self, x):
+        return self._reduce(x, None if self.dist is None else self.dist.ReduceOp.SUM)
+
+    def timer(self):
+        return _Timer(self)
+
+    def host_array(self, shape, init=None):
+        """An F-ordered float64 array in page-locked host memory (plain host
+        memory in the emulation), reused from step to step as a host code would."""
+        if self.emulated:
+            a = np.zeros(shape, order="F")
+        else:
+            t = self.torch.empty(int(np.prod(shape)), dtype=self.torch.float64, pin_memory=True)
+            self._pinned.append(t)  # the array views the tensor's memory
+            a = t.numpy().reshape(shape, order="F")
+        if init is not None:
+            a[...] = init
+        return a
+
+    def close(self):
+        if self.dist is not None:
+            self.dist.destroy_process_group()
+            self.dist = None
+
+
+class _Timer:
+    """Device time of a region: CUDA events on the engine stream (the host
+    clock in the emulation); seconds() once the region has been synchronised."""
+
+    def __init__(self, rt):
+        self.rt = rt
+        if not rt.emulated:
+            self.e0 = rt.torch.cuda.Event(enable_timing=True)
+            self.e1 = rt.torch.cuda.Event(enable_timing=True)
+
+    def start(self):
+        if self.rt.emulated:
+            self.t0 = time.perf_counter()
+        else:
+            self.e0.record(self.rt.stream)
+
+    def stop(self):
+        if self.rt.emulated:
+            self.t1 = time.perf_counter()
+        else:
+            self.e1.record(self.rt.stream)
+
+    def seconds(self):
+        return (self.t1 - self.t0) if self.rt.emulated else self.e0.elapsed_time(self.e1) / 1e3
+
+
+def _term_errors(e_gpu, e_ref, nion):
+    names = ["total", "kinetic", "ion_electron", "hartree", "xc", "ion_ion", "tf", "vw", "nonlocal"]
+    err = np.abs(np.asarray(e_gpu) - np.asarray(e_ref)) * HA_EV / nion
+    return {k: float(v) for k, v in zip(names, err)}, float(err.max())
+
+
 def run_ours(args):
-    import torch
-    ws, rank, local = _dist()
-    if not torch.cuda.is_available():
-        raise SystemExit("bench.py needs a CUDA GPU")
-    torch.cuda.set_device(local)
-    dist = None
-    if ws > 1:
-        import datetime
-        import torch.distributed as dist
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+    rt = Runtime(args)
+    ws, rank = rt.ws, rt.rank
     from profess_b200 import cell as pcell
     from profess_b200 import native, workloads as wl
-    from profess_b200.recpot import BOHR, HARTREE_TO_EV
     if args.workload == "serving":
-        return run_serving(args, ws, rank, local, dist)
+        return run_serving(args, rt)
     if args.workload == "md":
-        return run_md(args, ws, rank, local, dist)
+        return run_md(args, rt)
     if args.workload == "relax":
-        return run_relax(args, ws, rank, local, dist)
+        return run_relax(args, rt)
     eng = native.Engine()
+    rt.bind(eng)
     cells = make_cells(args, rank)
     B = len(cells)
     rho0 = [wl.initial_density(c, seed=1000 * rank + b) for b, c in enumerate(cells)]
@@ -260,7 +431,6 @@ def run_ours(args):
     # above potNorm 1e-6 with the energy already converged to round-off (the
     # FP64 NTN line search then needs tens of trials per iteration).
     o64 = native.ntn_options(conv_check=native.CONV_POT, pot_tol=1.0e-6, max_iter=300, stall_line=6)
-    stream = torch.cuda.ExternalStream(eng.stream())
 
     def run_all(slots, t0, done_at):
         while True:
@@ -272,21 +442,9 @@ def run_ours(args):
             if left == 0:
                 return
 
-    # The caller's host arrays for the end-to-end run: the initial densities
-    # and the result densities in pinned (page-locked) host memory, reused
-    # from step to step as a host code would.
-    pinned = []
-
-    def pinned_array(shape, init=None):
-        t = torch.empty(int(np.prod(shape)), dtype=torch.float64, pin_memory=True)
-        pinned.append(t)
-        a = t.numpy().reshape(shape, order="F")
-        if init is not None:
-            a[...] = init
-        return a
-
-    rho_in = [pinned_array(c.grid, r) for c, r in zip(cells, rho0)]
-    rho_out = [pinned_array(c.grid) for c in cells]
+    # the caller's host arrays for the end-to-end run
+    rho_in = [rt.host_array(c.grid, r) for c, r in zip(cells, rho0)]
+    rho_out = [rt.host_array(c.grid) for c in cells]
 
     def mixed_step(host=False):
         t0 = time.perf_counter()
@@ -312,100 +470,117 @@ def run_ours(args):
         run_all(s64, t0, done)
         return [eng.result(b, want_rho=False) for b in s64], [done[b] for b in s64]
 
-    def barrier():
-        if dist is not None:
-            dist.barrier()
-        torch.cuda.synchronize()
-
-    def max_over_ranks(x):
-        if dist is None:
-            return x
-        t = torch.tensor([x], dtype=torch.float64, device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        return float(t.item())
-
     # ---------------- mixed path, device-resident inputs
     for _ in range(args.warmup):
         mixed_step()
-    clocks = ClockSampler(local)
+    clocks = ClockSampler(rt.local, enabled=not rt.emulated)
     clocks.start()
-    barrier()
+    rt.barrier()
     l0, _ = eng.counters()
     cap0 = eng.capture_stats()
-    ev0 = torch.cuda.Event(enable_timing=True)
-    ev1 = torch.cuda.Event(enable_timing=True)
+    tm = rt.timer()
     lat = []
     mixed_res = None
-    ev0.record(stream)
+    tm.start()
     for _ in range(args.steps):
         mixed_res, l = mixed_step()
         lat.extend(l)
-    ev1.record(stream)
-    barrier()
+    tm.stop()
+    rt.barrier()
     l1, _ = eng.counters()
     cap1 = eng.capture_stats()
     clk = clocks.stop()
-    t_mixed = max_over_ranks(ev0.elapsed_time(ev1) / 1e3)
+    t_mixed = rt.max_over_ranks(tm.seconds())
     value = ws * B * args.steps / t_mixed
-    # forces on the mixed solution (the FP64 slots hold it), compared below with the plain FP64 solution
+    # forces and the first cell's density of the mixed solution (the FP64 slots hold it)
     f_mixed = [eng.forces(b, c.nion, include_ewald=False) for b, c in zip(s64, cells)]
+    f_mixed0 = eng.forces(s64[0], cells[0].nion, include_ewald=True)
 
     # ---------------- plain FP64 path on the same cells
     for _ in range(min(args.warmup, 1)):
         fp64_step()
-    barrier()
-    ev0.record(stream)
+    rt.barrier()
+    tf = rt.timer()
     fp64_res = None
     lat64 = []
+    tf.start()
     for _ in range(args.steps):
         fp64_res, l = fp64_step()
         lat64.extend(l)
-    ev1.record(stream)
-    barrier()
-    t_fp64 = max_over_ranks(ev0.elapsed_time(ev1) / 1e3)
+    tf.stop()
+    rt.barrier()
+    t_fp64 = rt.max_over_ranks(tf.seconds())
     fp64_value = ws * B * args.steps / t_fp64
-    errs = [abs(m[0][0] - f[1][0]) * HARTREE_TO_EV / c.nion for m, f, c in zip(mixed_res, fp64_res, cells)]
+    errs = [abs(m[0][0] - f[1][0]) * HA_EV / c.nion for m, f, c in zip(mixed_res, fp64_res, cells)]
     f_fp64 = [eng.forces(b, c.nion, include_ewald=False) for b, c in zip(s64, cells)]
-    ferr = max(float(np.abs(a - b).max()) for a, b in zip(f_mixed, f_fp64)) * HARTREE_TO_EV / BOHR
+    ferr = max(float(np.abs(a - b).max()) for a, b in zip(f_mixed, f_fp64)) * HA_EV / BOHR_ANG
+    f_fp640 = eng.forces(s64[0], cells[0].nion, include_ewald=True)
     evals32 = [m[2]["num_evals"] for m in mixed_res]
     evals_ref = [m[1]["num_evals"] for m in mixed_res]
     evals64 = [f[2]["num_evals"] for f in fp64_res]
 
     # ---------------- end to end through the public API with host buffers
     mixed_step(host=True)  # warm-up
-    barrier()
+    rt.barrier()
     t0 = time.perf_counter()
     for _ in range(args.steps):
         mixed_step(host=True)
-    barrier()
-    t_e2e = max_over_ranks(time.perf_counter() - t0)
+    rt.barrier()
+    t_e2e = rt.max_over_ranks(time.perf_counter() - t0)
     h2d = int(sum(np.prod(c.grid) * 8 for c in cells))
     d2h = int(sum(np.prod(c.grid) * 8 + 9 * 8 for c in cells))
 
     # ---------------- roofline probe: batched potential evaluations of every slot
-    ms_eval = eng.time_eval(iters=10)
-    alg_bytes = sum(eval_bytes(c, 4) + eval_bytes(c, 8) for c in cells)
-    achieved = alg_bytes / (ms_eval / 1e3) / 1e9
-    peak, peak_kind = _peaks()
-    tr = _traffic_per_eval() if args.workload == "cfg2" else None
+    roofline = None
+    if not rt.emulated:
+        ms_eval = eng.time_eval(iters=10)
+        alg_bytes = sum(eval_bytes(c, 4) + eval_bytes(c, 8) for c in cells)
+        achieved = alg_bytes / (ms_eval / 1e3) / 1e9
+        peak, peak_kind = _peaks()
+        tr = _traffic_per_eval() if args.workload == "cfg2" else None
+        roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                    "peak_source": peak_kind,
+                    "kernel": "batched potential evaluation (all passes + controller) of every cell in FP32 and "
+                              "FP64 (%d slots)" % (2 * B),
+                    "ms_per_launch": ms_eval,
+                    "traffic": (B * (tr[0] + tr[1])) if tr else None,
+                    "traffic_source": ("profiles/eval_traffic.txt (ncu dram__bytes per slot evaluation x slots, "
+                                       "taken on these sources: %s)" % source_sha()) if tr else
+                                      "none taken on these sources (%s)" % source_sha()}
 
+    # ---------------- the oracle: CPU baseline and errors of the GPU solves
     cpu = None
-    if rank == 0 and ws == 1 and not args.no_cpu_baseline and args.workload == "cfg2":
-        t_cpu, _ = cpu_solve_time(cells[0], rho0[0])
+    oracle_err = None
+    if rank == 0 and args.workload != "cfg4" and not args.no_cpu_baseline:
+        ocell, f = oracle_functional(cells[0])
+        t_cpu, r_o = cpu_solve(f, rho0[0])
+        v1, t_eval1 = cpu_one_core(f, rho0[0], r_o.num_evals)
         cpu = {"value": 1.0 / t_cpu, "unit": UNIT, "cores": os.cpu_count() or 1, "kind": "port",
-               "sample": "one FP64 NTN solve (to potNorm < 1e-6) of one cell of the workload by the "
-                         "oracle, a CPU restatement of the reference's path (NumPy + scipy.fft on all cores)"}
+               "sample": "one FP64 NTN solve (to potNorm < 1e-6, %d evaluations) of the first cell of the "
+                         "workload by the oracle, a CPU restatement of the reference's path (NumPy + "
+                         "scipy.fft on all cores)" % r_o.num_evals,
+               "one_core": {"value": v1, "unit": UNIT, "cores": 1,
+                            "sample": "3 oracle potential evaluations on one core (%.3f s each) x the %d "
+                                      "evaluations of the all-core solve" % (t_eval1, r_o.num_evals)}}
+        oracle_err = oracle_errors(eng, cells[0], s32[0], s64[0], ocell, f, r_o, mixed_res[0][0], f_mixed0,
+                                   fp64_res[0][1], f_fp640)
+
+    serving_line = None
+    if args.workload == "cfg2" and args.serving_requests > 0 and not rt.emulated:
+        for s in s32 + s64:
+            eng.slot_destroy(s)
+        serving_line = serving_compare(args, eng, rt)
     if rank != 0:
-        if dist is not None:
-            dist.destroy_process_group()
+        rt.close()
         return 0
     out = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": 1e3 * t_mixed / args.steps, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f32+f64",
         "data": "synthetic (seeded cells)",
-        "config": {"workload": WORKLOADS[args.workload] + "; NTN: FP32 to potNorm<%g or the FP32 line-search floor, "
-                                                          "then <=%d FP64 iterations" % (args.fp32_tol, args.refine),
+        "config": {"workload": WORKLOADS[args.workload] + "; NTN: FP32 to potNorm<%g or the FP32 line-search "
+                                                          "floor, then <=%d FP64 iterations" % (args.fp32_tol,
+                                                                                                args.refine),
                    "batch_per_step": B, "parallelism": "replicas x%d" % ws,
                    "l2_flush": "not needed: batch working set above the 126 MB L2"},
         "fp64_gpu": {"value": fp64_value, "unit": UNIT, "ms_per_step": 1e3 * t_fp64 / args.steps,
@@ -415,158 +590,217 @@ def run_ours(args):
         "mixed_over_fp64": value / fp64_value,
         "energy_error_ev_per_atom_max": max(errs),
         "force_error_ev_per_ang_max": ferr,
+        "errors_vs_oracle": oracle_err,
         "latency_ms": {"p50": 1e3 * float(np.percentile(lat, 50)), "p99": 1e3 * float(np.percentile(lat, 99))},
         "evals_per_solve_mixed": {"fp32": float(np.mean(evals32)), "fp64_refine": float(np.mean(evals_ref))},
         "final_pot_norm_max": {"mixed": max(m[1]["pot_norm"] for m in mixed_res),
                                "fp64": max(f[2]["pot_norm"] for f in fp64_res)},
         "e2e": {"value": ws * B * args.steps / t_e2e, "unit": UNIT, "h2d_bytes_per_step": h2d,
                 "d2h_bytes_per_step": d2h},
-        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
-                     "frac": achieved / peak, "peak_source": peak_kind,
-                     "kernel": "batched potential evaluation (passes 1-5 + controller) of every cell in FP32 and "
-                               "FP64 (%d slots)" % (2 * B),
-                     "ms_per_launch": ms_eval,
-                     "traffic": (B * (tr[0] + tr[1])) if tr else None,
-                     "traffic_source": "profiles/eval_traffic.txt (ncu dram__bytes per slot evaluation x slots)"
-                     if tr else None},
+        "roofline": roofline,
         "cpu_baseline": cpu,
+        "serving": serving_line,
         "clocks": clk,
         "graph_captures_per_step": {"count": (cap1[0] - cap0[0]) / args.steps,
                                     "host_ms": (cap1[1] - cap0[1]) / args.steps},
         "gpu_launches": l1 - l0,
     }
+    if rt.emulated:
+        out["emulated"] = "no GPU: the engine's kernels ran in the host emulation build (test harness)"
     print(json.dumps(out), flush=True)
-    if dist is not None:
-        dist.destroy_process_group()
+    rt.close()
     return 0
 
 
-def run_serving(args, ws, rank, local, dist):
+def oracle_errors(eng, cell, s32, s64, ocell, f, r_o, e_mixed, f_mixed, e_fp64, f_fp64):
+    """The first cell's GPU solves against the oracle's FP64 solve from the same
+    initial density: every energy term (eV/atom), the largest force component
+    difference (eV/A, forces on each solver's own converged density), and the
+    RMS of the FP32 and FP64 potentials at the oracle's converged density (Ha)."""
+    from oracle import forces as ofo, functional as fn
+    F_o, _, _ = ofo.total_forces(ocell, r_o.rho)
+    pot_o, _ = fn.calculate_potential_plus(f, r_o.rho)
+    pot32, _ = eng.calculate_potential_plus(s32, r_o.rho)
+    pot64, _ = eng.calculate_potential_plus(s64, r_o.rho)
+    mixed_terms, mixed_max = _term_errors(e_mixed, r_o.energy, cell.nion)
+    fp64_terms, fp64_max = _term_errors(e_fp64, r_o.energy, cell.nion)
+    conv = HA_EV / BOHR_ANG
+    return {"cell": "first cell of the batch (%d atoms, grid %s)" % (cell.nion, "x".join(map(str, cell.grid))),
+            "oracle": "FP64 NTN solve to potNorm < 1e-6 from the same initial density (%d evaluations)"
+                      % r_o.num_evals,
+            "mixed": {"energy_terms_ev_per_atom": mixed_terms, "energy_max_ev_per_atom": mixed_max,
+                      "force_max_ev_per_ang": float(np.abs(f_mixed - F_o).max()) * conv},
+            "fp64": {"energy_terms_ev_per_atom": fp64_terms, "energy_max_ev_per_atom": fp64_max,
+                     "force_max_ev_per_ang": float(np.abs(f_fp64 - F_o).max()) * conv},
+            "potential_rms_ha_at_oracle_density": {"fp32_eval": float(np.sqrt(np.mean((pot32 - pot_o) ** 2))),
+                                                   "fp64_eval": float(np.sqrt(np.mean((pot64 - pot_o) ** 2)))}}
+
+
+def _serve(eng, cells, mode, arrivals, budget, args):
+    from profess_b200 import serving
+    srv = serving.Server(eng, budget, max_active=args.max_active)
+    for i, (c, t) in enumerate(zip(cells, arrivals)):
+        srv.submit(serving.Request(rid=i, cell=c, arrival=t, seed=i, mode=mode, fp32_tol=args.fp32_tol,
+                                   refine_iters=args.refine))
+    res = srv.run_until_done(timeout=3600)
+    return {r.rid: r for r in res}, serving.latency_stats(res)
+
+
+def serving_compare(args, eng, rt):
+    """The serving mix as mixed and as plain FP64 requests on the same cells:
+    saturated capacity, then a Poisson stream at 80 % of each mode's capacity."""
+    from profess_b200 import serving, workloads as wl
+    rng = np.random.default_rng(2024 + rt.rank)
+    n = args.serving_requests
+    cells = [wl.serving_cell(rng) for _ in range(n)]
+    free, _ = rt.torch.cuda.mem_get_info()
+    budget = int(0.8 * free)
+    out = {"requests": n, "atoms_mean": float(np.mean([c.nion for c in cells])),
+           "workload": "serving mix: Al/Mg cells, 32-2048 atoms (log-uniform), grids 32^3-256^3, 70% WT / 30% "
+                       "WGC, sigma U[0.03,0.1] A, " + PSP}
+    results = {}
+    for mode in (serving.MODE_MIXED, serving.MODE_FP64):
+        res, cap = _serve(eng, cells, mode, [0.0] * n, budget, args)
+        lam = 0.8 * cap["solves_per_s"]
+        t, arr = 0.0, []
+        prng = np.random.default_rng(77 + rt.rank)
+        for _ in range(n):
+            t += float(prng.exponential(1.0 / lam))
+            arr.append(t)
+        _, st = _serve(eng, cells, mode, arr, budget, args)
+        results[mode] = res
+        out[mode] = {"capacity_solves_per_s": rt.sum_over_ranks(cap["solves_per_s"]),
+                     "arrival_rate_per_s": lam,
+                     "solves_per_s_at_80pct": rt.sum_over_ranks(st["solves_per_s"]),
+                     "latency_s": {"p50": st["p50_s"], "p99": st["p99_s"]}}
+    out["serving_mixed_over_fp64"] = (out[serving.MODE_MIXED]["capacity_solves_per_s"] /
+                                      out[serving.MODE_FP64]["capacity_solves_per_s"])
+    err = [abs(results[serving.MODE_MIXED][i].energy[0] - results[serving.MODE_FP64][i].energy[0]) * HA_EV /
+           cells[i].nion for i in range(n)]
+    out["energy_error_mixed_vs_fp64_ev_per_atom_max"] = rt.max_over_ranks(max(err))
+    return out
+
+
+def run_serving(args, rt):
     """Poisson stream of mixed-precision requests at 80% of the measured capacity."""
-    import torch
     from profess_b200 import native, serving, workloads as wl
     eng = native.Engine()
-    rng = np.random.default_rng(12345 + rank)
+    rng = np.random.default_rng(12345 + rt.rank)
     nreq = args.requests
     cells = [wl.serving_cell(rng) for _ in range(nreq)]
-    free, _total = torch.cuda.mem_get_info()
+    free, _total = rt.torch.cuda.mem_get_info()
     budget = int(0.8 * free)
-    # capacity: everything arrives at once (saturated server)
-    srv = serving.Server(eng, budget, max_active=args.max_active)
-    for i, c in enumerate(cells):
-        srv.submit(serving.Request(rid=i, cell=c, arrival=0.0, seed=i, fp32_tol=args.fp32_tol,
-                                   refine_iters=args.refine))
-    res = srv.run_until_done(timeout=3600)
-    cap = serving.latency_stats(res)["solves_per_s"]
-    # 80% load, Poisson arrivals
+    _, capst = _serve(eng, cells, serving.MODE_MIXED, [0.0] * nreq, budget, args)
+    cap = capst["solves_per_s"]
     lam = 0.8 * cap
-    t = 0.0
-    srv = serving.Server(eng, budget, max_active=args.max_active)
-    for i, c in enumerate(cells):
+    t, arr = 0.0, []
+    for _ in range(nreq):
         t += float(rng.exponential(1.0 / lam))
-        srv.submit(serving.Request(rid=i, cell=c, arrival=t, seed=i, fp32_tol=args.fp32_tol,
-                                   refine_iters=args.refine))
-    res = srv.run_until_done(timeout=3600)
-    st = serving.latency_stats(res)
-    if rank != 0:
+        arr.append(t)
+    _, st = _serve(eng, cells, serving.MODE_MIXED, arr, budget, args)
+    value = rt.sum_over_ranks(st["solves_per_s"])
+    if rt.rank != 0:
+        rt.close()
         return 0
-    out = {"metric": METRIC, "value": st["solves_per_s"] * ws, "unit": UNIT, "n_gpus": ws, "steps": nreq,
+    out = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": rt.ws, "steps": nreq,
            "warmup": 0, "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32+f64",
            "data": "synthetic Poisson request stream (seeded)",
            "config": {"workload": "serving: Al/Mg cells, 32-2048 atoms (log-uniform), grids 32^3-256^3, "
-                                  "70% WT / 30% WGC, sigma U[0.03,0.1] A; arrivals Poisson at 80% of capacity",
+                                  "70% WT / 30% WGC, sigma U[0.03,0.1] A, " + PSP +
+                                  "; arrivals Poisson at 80% of capacity",
                       "requests": nreq, "capacity_solves_per_s": cap, "arrival_rate_per_s": lam},
            "latency_s": {"p50": st["p50_s"], "p99": st["p99_s"], "mean": st["mean_s"]},
            "atoms_per_request_mean": float(np.mean([c.nion for c in cells]))}
     print(json.dumps(out), flush=True)
+    rt.close()
     return 0
 
 
-def run_md(args, ws, rank, local, dist):
+def run_md(args, rt):
     """NVE molecular dynamics of B replicas of the cfg2 cell (FP64 solves to
     potNorm < 1e-6, warm-started), 600 K, dt = 40 a.u.; replica-steps/s over
-    the wall clock of the timed steps (host Ewald included)."""
-    import torch
+    the wall clock of the timed steps (device Ewald included)."""
     from profess_b200 import md, native, workloads as wl
     eng = native.Engine()
     B = args.batch or 16
-    cells = [wl.config_cell(2, seed=1000 * rank + b) for b in range(B)]
-    run = md.NVE(eng, cells, 40.0, temperature_k=600.0, seed=1000 * rank)
+    cells = [wl.config_cell(2, seed=1000 * rt.rank + b) for b in range(B)]
+    run = md.NVE(eng, cells, 40.0, temperature_k=600.0, seed=1000 * rt.rank)
     try:
         for _ in range(args.warmup):
             run.step()
         h0 = [r.history[-1]["conserved"] if r.history else r.conserved() for r in run.reps]
-        torch.cuda.synchronize()
-        if dist is not None:
-            dist.barrier()
+        rt.barrier()
         t0 = time.perf_counter()
         for _ in range(args.steps):
             run.step()
-        torch.cuda.synchronize()
-        wall = time.perf_counter() - t0
-        if dist is not None:
-            t = torch.tensor([wall], dtype=torch.float64, device="cuda")
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-            wall = float(t.item())
+        rt.barrier()
+        wall = rt.max_over_ranks(time.perf_counter() - t0)
         drift = max(abs(r.history[-1]["conserved"] - h) / r.cell.nion for r, h in zip(run.reps, h0))
         evals = float(np.mean([h["num_evals"] for r in run.reps for h in r.history[-args.steps:]]))
     finally:
         run.close()
-    if rank != 0:
+    if rt.rank != 0:
+        rt.close()
         return 0
-    out = {"metric": "NVE MD replica-steps/s", "value": ws * B * args.steps / wall, "unit": "replica-steps/s",
-           "n_gpus": ws, "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * wall / args.steps,
+    out = {"metric": "NVE MD replica-steps/s", "value": rt.ws * B * args.steps / wall, "unit": "replica-steps/s",
+           "n_gpus": rt.ws, "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * wall / args.steps,
            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
            "data": "synthetic (seeded cells and velocities)",
            "config": {"workload": WORKLOADS["cfg2"] + "; NVE velocity Verlet, 600 K, dt 40 a.u., FP64 NTN to "
                                                       "potNorm<1e-6 warm-started from the last density",
-                      "replicas_per_step": B, "parallelism": "replicas x%d" % ws},
+                      "replicas_per_step": B, "parallelism": "replicas x%d" % rt.ws},
            "evals_per_solve": evals,
            "conserved_energy_drift_ha_per_atom": drift}
     print(json.dumps(out), flush=True)
+    rt.close()
     return 0
 
 
-def run_relax(args, ws, rank, local, dist):
+def run_relax(args, rt):
     """QuickMin relaxation of B cfg2 cells in lockstep (FP64 solves to potNorm < 1e-6,
     warm-started); cell-steps/s over the wall clock of the timed batched steps."""
-    import torch
     from profess_b200 import native, relax, workloads as wl
     eng = native.Engine()
     B = args.batch or 16
-    cells = [wl.config_cell(2, seed=1000 * rank + b) for b in range(B)]
+    cells = [wl.config_cell(2, seed=1000 * rt.rank + b) for b in range(B)]
     qm = relax.QuickMin(eng, cells, max_steps=args.warmup + args.steps + 1)
     try:
         for _ in range(args.warmup):
             qm.step()
-        torch.cuda.synchronize()
-        if dist is not None:
-            dist.barrier()
+        rt.barrier()
         t0 = time.perf_counter()
         moved = sum(qm.step() for _ in range(args.steps))
-        torch.cuda.synchronize()
-        wall = time.perf_counter() - t0
-        if dist is not None:
-            t = torch.tensor([wall], dtype=torch.float64, device="cuda")
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-            wall = float(t.item())
+        rt.barrier()
+        wall = rt.max_over_ranks(time.perf_counter() - t0)
+        moved = rt.sum_over_ranks(moved)
         f0 = max(st.initial_max_force for st in qm.states)
         f1 = max(st.max_force for st in qm.states)
         undone = sum(h["undone"] for st in qm.states for h in st.history)
     finally:
         qm.close()
-    if rank != 0:
+    if rt.rank != 0:
+        rt.close()
         return 0
-    out = {"metric": "QuickMin relaxation cell-steps/s", "value": ws * moved / wall, "unit": "cell-steps/s",
-           "n_gpus": ws, "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * wall / args.steps,
+    out = {"metric": "QuickMin relaxation cell-steps/s", "value": moved / wall, "unit": "cell-steps/s",
+           "n_gpus": rt.ws, "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * wall / args.steps,
            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
            "data": "synthetic (seeded cells)",
            "config": {"workload": WORKLOADS["cfg2"] + "; QuickMin (time step 0.4 a.u. doubling), FP64 NTN to "
                                                       "potNorm<1e-6 warm-started from the last density",
-                      "cells_per_step": B, "parallelism": "replicas x%d" % ws},
+                      "cells_per_step": B, "parallelism": "replicas x%d" % rt.ws},
            "max_force_ha_per_bohr": {"initial": f0, "final": f1}, "moves_undone": int(undone)}
     print(json.dumps(out), flush=True)
+    rt.close()
     return 0
+
+
+def spawn_ranks(args):
+    """`--gpus N` without a launcher: start N ranks (one GPU each) through
+    torch.distributed.run on this node and return its exit status."""
+    cmd = [sys.executable, "-m", "torch.distributed.run", "--nnodes=1", "--nproc-per-node", str(args.gpus),
+           "--master-addr", "127.0.0.1", "--master-port", str(_free_port()), os.path.abspath(__file__)]
+    cmd += sys.argv[1:]
+    return subprocess.call(cmd)
 
 
 def main():
@@ -577,20 +811,25 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--batch", type=int, default=0, help="cells per step (0: the workload's default)")
     ap.add_argument("--workload", default="cfg2", choices=["cfg2", "cfg1", "cfg3", "cfg4", "serving", "md", "relax"])
-    ap.add_argument("--requests", type=int, default=48, help="serving: number of requests")
+    ap.add_argument("--requests", type=int, default=48, help="serving workload: number of requests")
+    ap.add_argument("--serving-requests", type=int, default=24,
+                    help="requests of the serving comparison in the cfg2 line (0: none)")
     ap.add_argument("--max-active", type=int, default=24, help="serving: concurrent requests")
     # FP32 phase tolerance of the mixed solve: 3e-5 gave the same worst energy
-    # error as 1e-5 on every workload (the two FP64 iterations set it) with
-    # ~15 % fewer FP32 evaluations
+    # error as 1e-5 on every workload (the FP64 iterations set it) with ~15 %
+    # fewer FP32 evaluations
     ap.add_argument("--fp32-tol", type=float, default=3.0e-5)
     # FP64 refinement iterations (each ends early once |dL/dphi| < 1e-6).  On
     # cfg2, 1 and 2 give the same energy error as 3 but forces off the FP64
     # solution by 7.8e-4 and 1.9e-4 eV/A; 3 gives 4e-5 eV/A
     ap.add_argument("--refine", type=int, default=3)
-    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-cpu-baseline", action="store_true",
+                    help="skip the oracle solve (CPU baseline and errors against the oracle)")
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference(args)
+    if args.gpus > 1 and "WORLD_SIZE" not in os.environ:
+        return spawn_ranks(args)
     return run_ours(args)
 
 

@@ -23,17 +23,22 @@ SPLINE_ORDER = 10  # Source/CBSpline.f90:36
 # ----------------------------------------------------------------------------
 # FFT convention of the reference (Source/Fourier_v1.f90:333-465)
 # ----------------------------------------------------------------------------
+# Threads of the oracle's FFTs (scipy.fft workers): -1 = every host core; a
+# timing of the oracle on one core sets 1.
+FFT_WORKERS = -1
+
+
 def fft_r2c(a: np.ndarray) -> np.ndarray:
     """Forward 3D real->half-complex FFT scaled by 1/N (Fourier_v1.f90:389-393).
 
     ``a`` has shape (n1, n2, n3); the result has shape (n1//2+1, n2, n3)."""
-    return sfft.rfftn(a, axes=(1, 2, 0), norm="forward", workers=-1)
+    return sfft.rfftn(a, axes=(1, 2, 0), norm="forward", workers=FFT_WORKERS)
 
 
 def fft_c2r(c: np.ndarray, n1: int) -> np.ndarray:
     """Backward 3D half-complex->real FFT, unscaled (Fourier_v1.f90:400-465)."""
     _, n2, n3 = c.shape
-    return sfft.irfftn(c, s=(n2, n3, n1), axes=(1, 2, 0), norm="forward", workers=-1)
+    return sfft.irfftn(c, s=(n2, n3, n1), axes=(1, 2, 0), norm="forward", workers=FFT_WORKERS)
 
 
 # ----------------------------------------------------------------------------

@@ -81,17 +81,28 @@ static int odd_columns(int nf, int rp, size_t csz) {
 }
 
 // Launch shape of a slot's passes: row pairs per x-forward task (*rp1) and
-// per x-inverse task (s.rp), carrying every field (or ion species) of their
-// row pairs in about 36 KB of shared memory; and the tiles of the split y/z
+// per x-inverse task (s.rp), carrying every field (or ion species) of up to
+// OFDFT_XPASS_POINTS / n1 row pairs in OFDFT_XPASS_KB32 (FP32) or
+// OFDFT_XPASS_KB64 (FP64) KB of shared memory; and the tiles of the split y/z
 // path: z columns per y-pass task (*ty: columns of n2 values at an odd row
 // pitch) and y columns per z-pass task (*tz: a group of gmax fields of n3
 // values each), each in about 48 KB, at least 32 columns when n allows.
 // s needs n1..n3, k1, nf and kinetic; csz is the size of one complex value.
+#ifndef OFDFT_XPASS_KB32
+#define OFDFT_XPASS_KB32 48
+#endif
+#ifndef OFDFT_XPASS_KB64
+#define OFDFT_XPASS_KB64 72
+#endif
+#ifndef OFDFT_XPASS_POINTS
+#define OFDFT_XPASS_POINTS 2048
+#endif
 static void launch_shape(SlotDev& s, size_t csz, int nfx, int* rp1, int* ty, int* tz) {
-  *rp1 = std::max(1, std::min(32, 1024 / s.n1));
-  while (*rp1 > 1 && (size_t)nfx * *rp1 * s.n1 * csz > 36 * 1024) (*rp1)--;
-  s.rp = std::max(1, std::min(32, 1024 / s.n1));
-  while (s.rp > 1 && (size_t)s.nf * s.rp * s.n1 * csz > 36 * 1024) s.rp--;
+  const size_t xkb = (size_t)(csz == 8 ? OFDFT_XPASS_KB32 : OFDFT_XPASS_KB64) * 1024;
+  *rp1 = std::max(1, std::min(32, OFDFT_XPASS_POINTS / s.n1));
+  while (*rp1 > 1 && (size_t)nfx * *rp1 * s.n1 * csz > xkb) (*rp1)--;
+  s.rp = std::max(1, std::min(32, OFDFT_XPASS_POINTS / s.n1));
+  while (s.rp > 1 && (size_t)s.nf * s.rp * s.n1 * csz + NCH * 33 * sizeof(double) > xkb) s.rp--;
   *rp1 = odd_columns(s.nf, *rp1, csz);
   s.rp = odd_columns(s.nf, s.rp, csz);
   const int gmax = s.kinetic == KIN_WGC ? 3 : 1;

@@ -355,6 +355,120 @@ HD void ip_stage(cx<T>* buf, int ncols, unsigned mcols, int cs, int es, const Ff
 #undef OFDFT_IP_CASE
 }
 
+// One stage whose inputs come from src.ld(c, i) and whose outputs go to
+// dst.st(c, i, v) (column c, position i), with the butterfly work split of
+// ip_stage_r: a first forward stage can load straight from global memory, a
+// last inverse stage store straight to it.
+template <typename T, int R, int DIR, class Src, class Dst>
+HD void ip_stage_io(const Src& src, const Dst& dst, int ncols, unsigned mcols, int n, int L, unsigned mm,
+                    const cx<T>* __restrict__ roots, int tid, int nthr) {
+  const int m = L / R;
+  const int total = (n / R) * ncols;
+  const int tstep = n / L;
+  for (int w = tid; w < total; w += nthr) {
+    const int bf = magic_div32(w, mcols), c = w - bf * ncols;
+    const int blk = magic_div32(bf, mm), j0 = bf - blk * m;
+    const int base = blk * L + j0;
+    cx<T> v[R];
+#pragma unroll
+    for (int r = 0; r < R; ++r) v[r] = src.ld(c, base + r * m);
+    const int e = j0 * tstep;
+    if (DIR > 0 && m > 1) {
+#pragma unroll
+      for (int r = 1; r < R; ++r) v[r] = cmul(v[r], conj(roots[r * e]));
+    }
+    Dft<T, R, DIR>::run(v);
+    if (DIR < 0 && m > 1) {
+#pragma unroll
+      for (int r = 1; r < R; ++r) v[r] = cmul(v[r], roots[r * e]);
+    }
+#pragma unroll
+    for (int r = 0; r < R; ++r) dst.st(c, base + r * m, v[r]);
+  }
+}
+
+// Stage s of plan p through accessors (a switch over the radix).
+template <typename T, int DIR, class Src, class Dst>
+HD void ip_stage_acc(const Src& src, const Dst& dst, int ncols, unsigned mcols, const FftPlan& p, int s,
+                     const cx<T>* roots, int tid, int nthr) {
+  constexpr int RM = FftMaxRadix<T>::value;
+  const int n = p.n, L = p.L[s];
+  const unsigned mm = p.m_magic[s];
+#define OFDFT_IO_CASE(r)                                                                              \
+  case r:                                                                                             \
+    if constexpr (r <= RM) ip_stage_io<T, r, DIR>(src, dst, ncols, mcols, n, L, mm, roots, tid, nthr); \
+    break;
+  switch (p.R[s]) {
+    OFDFT_IO_CASE(2)
+    OFDFT_IO_CASE(3)
+    OFDFT_IO_CASE(4)
+    OFDFT_IO_CASE(5)
+    OFDFT_IO_CASE(6)
+    OFDFT_IO_CASE(7)
+    OFDFT_IO_CASE(8)
+    OFDFT_IO_CASE(9)
+    OFDFT_IO_CASE(10)
+    OFDFT_IO_CASE(12)
+    OFDFT_IO_CASE(14)
+    OFDFT_IO_CASE(15)
+    OFDFT_IO_CASE(16)
+    default: break;
+  }
+#undef OFDFT_IO_CASE
+}
+
+// The last forward stage (block length R, stride 1: no twiddles), a real
+// pointwise factor op(c, q) at every position q, and the first inverse stage
+// (the same butterflies) in registers, in place: one shared-memory round trip
+// for a forward transform's end, a k-space operator and an inverse
+// transform's start.
+template <typename T, int R, class Op>
+HD void ip_stage_op_r(cx<T>* __restrict__ buf, int ncols, unsigned mcols, int cs, int es, int n, const Op& op,
+                      int tid, int nthr) {
+  const int total = (n / R) * ncols;
+  for (int w = tid; w < total; w += nthr) {
+    const int blk = magic_div32(w, mcols), c = w - blk * ncols;
+    cx<T>* p = buf + c * cs + blk * R * es;
+    cx<T> v[R];
+#pragma unroll
+    for (int r = 0; r < R; ++r) v[r] = p[r * es];
+    Dft<T, R, -1>::run(v);
+#pragma unroll
+    for (int r = 0; r < R; ++r) v[r] = v[r] * op(c, blk * R + r);
+    Dft<T, R, 1>::run(v);
+#pragma unroll
+    for (int r = 0; r < R; ++r) p[r * es] = v[r];
+  }
+}
+
+template <typename T, class Op>
+HD void ip_stage_op(cx<T>* buf, int ncols, unsigned mcols, int cs, int es, const FftPlan& p, const Op& op, int tid,
+                    int nthr) {
+  constexpr int RM = FftMaxRadix<T>::value;
+  const int n = p.n;
+#define OFDFT_OP_CASE(r)                                                                  \
+  case r:                                                                                 \
+    if constexpr (r <= RM) ip_stage_op_r<T, r>(buf, ncols, mcols, cs, es, n, op, tid, nthr); \
+    break;
+  switch (p.R[p.nst - 1]) {
+    OFDFT_OP_CASE(2)
+    OFDFT_OP_CASE(3)
+    OFDFT_OP_CASE(4)
+    OFDFT_OP_CASE(5)
+    OFDFT_OP_CASE(6)
+    OFDFT_OP_CASE(7)
+    OFDFT_OP_CASE(8)
+    OFDFT_OP_CASE(9)
+    OFDFT_OP_CASE(10)
+    OFDFT_OP_CASE(12)
+    OFDFT_OP_CASE(14)
+    OFDFT_OP_CASE(15)
+    OFDFT_OP_CASE(16)
+    default: break;
+  }
+#undef OFDFT_OP_CASE
+}
+
 // Full in-place transform of ncols columns (element i of column c at
 // buf[c*cs + i*es]).  DIR = -1: forward, natural -> digit-reversed; DIR = +1:
 // inverse, digit-reversed -> natural.  Every thread of the block must call

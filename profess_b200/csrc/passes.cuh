@@ -709,11 +709,45 @@ HD void zpass_block(const Args<T>& a, int bid, int tid, int nthr, char* smem) {
 }
 
 // ------------------------------------------------------------ YZ pass (fused path)
+// Accessors of the fused pass: the plane in global memory (y fastest, row
+// length n2) and in shared memory (rows of odd pitch P); column c is y,
+// position i is z.
+template <typename T>
+struct PlaneIO {
+  cx<T>* p;
+  int pitch;
+  HD cx<T> ld(int y, int z) const { return p[z * pitch + y]; }
+  HD void st(int y, int z, cx<T> v) const { p[z * pitch + y] = v; }
+};
+
+// Operator factors at (column z, y position q) of the fused pass: the WT
+// kernel plane (stored in the transforms' digit-reversed order) times the
+// 1/N forward scale, or the Hartree / vW factor of the frequencies there.
+template <typename T>
+struct KernOp {
+  const T* __restrict__ kern;
+  T sc;
+  int n2;
+  HD T operator()(int z, int q) const { return kern[z * n2 + q] * sc; }
+};
+template <typename T>
+struct GOp {
+  GFactor<T> gf;
+  int kind, kx, n2, n3;
+  const int* __restrict__ permy;
+  const int* __restrict__ permz;
+  HD T operator()(int z, int q) const {
+    return gf(kind, kx, signed_freq(permy[q], n2), signed_freq(permz[z], n3));
+  }
+};
+
 // Task (group g, kx) of a single-field group: the whole (y, z) plane of the
 // field at kx (n2*n3 contiguous values) in shared memory, rows of odd pitch
-// P: forward FFT along y (columns z) and z (columns y), the operator at the
-// digit-reversed positions, inverse FFT along z and y, one read and one
-// write of the plane.
+// P.  The forward FFT along z loads its first stage straight from the
+// spectra (consecutive threads, consecutive y); then the forward FFT along y;
+// its last stage, the operator and the first inverse stage run in registers
+// in one pass; then the inverse along y and z, whose last stage stores
+// straight to the spectra.  One read and one write of the plane in HBM.
 template <typename T>
 HD void yzpass_block(const Args<T>& a, int bid, int tid, int nthr, char* smem) {
   const Task t = a.tasks[bid];
@@ -724,40 +758,48 @@ HD void yzpass_block(const Args<T>& a, int bid, int tid, int nthr, char* smem) {
   const int g = t.a, kx = t.b;
   const int n2 = s.n2, n3 = s.n3, nrows = n2 * n3, P = odd_pitch(n2);
   const int kind = s.group_kind[g];
-  cx<T>* __restrict__ plane = (cx<T>*)s.spec + (size_t)s.group_f0[g] * (size_t)s.Nc + (size_t)kx * nrows;
+  cx<T>* plane = (cx<T>*)s.spec + (size_t)s.group_f0[g] * (size_t)s.Nc + (size_t)kx * nrows;
   cx<T>* buf = (cx<T>*)smem;
-  const unsigned mn2 = magic32(n2);
-  for (int w = tid; w < nrows; w += nthr) {
-    const int z = magic_div32(w, mn2), y = w - z * n2;
-    buf[z * P + y] = plane[w];
-  }
+  const FftPlan& py = s.py;
+  const FftPlan& pz = s.pz;
+  const cx<T>* ry = a.tw + py.root;
+  const cx<T>* rz = a.tw + pz.root;
+  const unsigned mn2 = magic32(n2), mn3 = magic32(n3);
+  const PlaneIO<T> glob{plane, n2}, rows{buf, P};
+  ip_stage_acc<T, -1>(glob, rows, n2, mn2, pz, 0, rz, tid, nthr);
   BLOCK_SYNC();
-  fft_inplace<T, -1>(buf, n3, P, 1, s.py, a.tw, tid, nthr);
-  fft_inplace<T, -1>(buf, n2, 1, P, s.pz, a.tw, tid, nthr);
-  const int* __restrict__ permy = a.idx + s.py.perm;
-  const int* __restrict__ permz = a.idx + s.pz.perm;
+  for (int st = 1; st < pz.nst; ++st) {
+    ip_stage<T, -1>(buf, n2, mn2, 1, P, pz, st, rz, tid, nthr);
+    BLOCK_SYNC();
+  }
+  for (int st = 0; st < py.nst - 1; ++st) {
+    ip_stage<T, -1>(buf, n3, mn3, P, 1, py, st, ry, tid, nthr);
+    BLOCK_SYNC();
+  }
   if (kind == G_KMUL) {
-    const T* __restrict__ kern = (const T*)s.kern + (size_t)kx * nrows;
-    const T sc = (T)s.inv_n;
-    for (int w = tid; w < nrows; w += nthr) {
-      const int z = magic_div32(w, mn2), y = w - z * n2;
-      buf[z * P + y] = buf[z * P + y] * (kern[w] * sc);
-    }
+    const KernOp<T> op{(const T*)s.kern + (size_t)kx * nrows, (T)s.inv_n, n2};
+    ip_stage_op<T>(buf, n3, mn3, P, 1, py, op, tid, nthr);
   } else {
-    GFactor<T> gf;
-    gf.init(s);
-    for (int w = tid; w < nrows; w += nthr) {
-      const int z = magic_div32(w, mn2), y = w - z * n2;
-      buf[z * P + y] = buf[z * P + y] * gf(kind, kx, signed_freq(permy[y], n2), signed_freq(permz[z], n3));
-    }
+    GOp<T> op;
+    op.gf.init(s);
+    op.kind = kind;
+    op.kx = kx;
+    op.n2 = n2;
+    op.n3 = n3;
+    op.permy = a.idx + py.perm;
+    op.permz = a.idx + pz.perm;
+    ip_stage_op<T>(buf, n3, mn3, P, 1, py, op, tid, nthr);
   }
   BLOCK_SYNC();
-  fft_inplace<T, 1>(buf, n2, 1, P, s.pz, a.tw, tid, nthr);
-  fft_inplace<T, 1>(buf, n3, P, 1, s.py, a.tw, tid, nthr);
-  for (int w = tid; w < nrows; w += nthr) {
-    const int z = magic_div32(w, mn2), y = w - z * n2;
-    plane[w] = buf[z * P + y];
+  for (int st = py.nst - 2; st >= 0; --st) {
+    ip_stage<T, 1>(buf, n3, mn3, P, 1, py, st, ry, tid, nthr);
+    BLOCK_SYNC();
   }
+  for (int st = pz.nst - 1; st >= 1; --st) {
+    ip_stage<T, 1>(buf, n2, mn2, 1, P, pz, st, rz, tid, nthr);
+    BLOCK_SYNC();
+  }
+  ip_stage_acc<T, 1>(rows, glob, n2, mn2, pz, 0, rz, tid, nthr);
 }
 
 // ------------------------------------------------------------ pass 5
@@ -800,137 +842,136 @@ struct XinvEpi {
   T lam, muv, al, be, cTF, mu0, ieps, st, ctd, ctf53;
 };
 
+// The epilogue of one point: its potential (stored to the mode's output
+// arrays at idx) and its terms of the mode's sums, added to sums[] in the
+// slot precision.  o[f] are the point's field outputs of the inverse
+// transforms; vi, aa, bx, ex, ey its ion potential and optimiser inputs.
+template <typename T, int KS, int EV, bool ENERGY>
+HD void epi_point(const XinvEpi<T>& e, const T* o, T vi, T aa, T bx, T ex, T ey, int idx, T* sums) {
+  constexpr bool RHO = EV == EV_RHO;  // the input is rho itself
+  const FieldPar<T> fp = e.fp;
+  const T cC = T(0.62035049089940009);
+  T phin, rho, sq;
+  if (RHO) {
+    rho = aa;
+    sq = m_sqrt(rho);
+    phin = sq;
+  } else {
+    phin = e.in.ca * aa + e.in.cb * bx;
+    rho = phin * phin;
+    sq = phin < T(0) ? -phin : phin;
+  }
+  const T x = m_rcbrt(rho);        // rho^(-1/3)
+  const T r13 = rho * x * x;       // rho^(1/3)
+  const T r23 = r13 * r13;
+  const T rinv = x * x * x;        // 1/rho
+  T vxc, exc;
+  lda_point(rho, r13, cC * x, vxc, exc);
+  T vnl, enl, lap;
+  const T al = e.al, be = e.be, cTF = e.cTF;
+  if constexpr (KS == KS_WT) {
+    const T rbeta = fp.pow56 ? sq * r13 : m_pow(rho, be);
+    const T ralpha = fp.aeqb ? rbeta : m_pow(rho, al);
+    const T pa = e.nf > 3 ? o[3] : o[1];
+    vnl = cTF * (al * (ralpha * rinv) * o[1] + be * (rbeta * rinv) * pa);
+    enl = cTF * ralpha * o[1];
+    lap = o[2];
+  } else {
+    const T th = rho - fp.rho_s;
+    const T ralpha = m_pow(rho, al);
+    const T rbeta = fp.sum53 ? rho * r23 / ralpha : m_pow(rho, be);
+    vnl = cTF * ((rbeta * rinv) * (be * o[2] + (rho + be * th) * o[3] + th * (rho + be * th * T(0.5)) * o[4]) +
+                 (ralpha * rinv) * (al * o[5] + (rho + al * th) * o[6] + th * (rho + al * th * T(0.5)) * o[7]));
+    enl = cTF * rbeta * (o[2] + th * o[3] + th * th * T(0.5) * o[4]);
+    lap = o[1];
+  }
+  const T potr = vi + o[0] + vxc + e.ctf53 * r23 + vnl;
+  const T muv = e.muv;
+  const T pot = e.opt_sqrt ? T(2) * sq * potr + muv * lap : potr + muv * lap * (T(0.5) * sq * rinv);
+  if constexpr (ENERGY) {
+    sums[CH_EIE] += rho * vi;
+    sums[CH_EH] += T(0.5) * o[0] * rho;
+    sums[CH_EXC] += exc;
+    sums[CH_ETF] += e.lam * cTF * (rho * r23);
+    sums[CH_EVW] += T(0.5) * muv * sq * lap;
+    sums[CH_ENL] += enl;
+  }
+  const T sg = phin < T(0) ? T(-1) : T(1);
+  if constexpr (EV == EV_RHO) {
+    e.w0[idx] = pot;
+  } else if constexpr (EV == EV_PHI) {
+    const T gg = pot * sg;
+    e.w0[idx] = gg;
+    sums[CH_M0] += gg * phin;
+    sums[CH_M1] += phin * phin;
+  } else if constexpr (EV == EV_CG) {
+    const T gg = pot * sg;
+    const T ap = ((gg - e.mu0 * T(2) * phin) - ex) * e.ieps;
+    e.w1[idx] = ap;
+    sums[CH_M0] += ey * ap;
+  } else {  // EV_LS
+    const T gg = pot * sg;
+    e.w1[idx] = gg;
+    e.trial[idx] = phin;
+    const T dir = -ex * e.st + ey * e.ctd;
+    const T dl = gg - T(2) * phin * e.mu0;
+    sums[CH_M0] += gg * dir;
+    sums[CH_M1] += dl * dl;
+    sums[CH_M2] += gg * phin;
+    sums[CH_M3] += phin * phin;
+  }
+}
+
 // The epilogue over every point of the task, compiled per evaluation mode EV
 // (ENERGY: the six energy channels are summed), so that each loop keeps only
-// its own inputs and FP64 accumulators live.  The sums go to acc_out[NCH].
+// its own inputs and accumulators live.  A work item is one complex output
+// of the inverse transforms: x index i of row pair b, whose real and
+// imaginary parts are the two rows' points (consecutive threads take
+// consecutive i, so every global access is coalesced).  The two points'
+// terms are added in the slot precision, then accumulated in FP64; the sums
+// go to acc_out[NCH].
 template <typename T, int KS, int EV, bool ENERGY>
 HD void xinv_points(const XinvEpi<T>& e, double* acc_out, int tid, int nthr) {
   constexpr int NFM = KinFields<KS>::value;
-  constexpr bool RHO = EV == EV_RHO;  // the input is rho itself
   const T* __restrict__ vion = e.vion;
   const T* __restrict__ A = e.in.A;
   const T* __restrict__ B = e.in.B;
   const T* __restrict__ bb = e.bb;
-  T* __restrict__ w0 = e.w0;
-  T* __restrict__ w1 = e.w1;
-  T* __restrict__ trial = e.trial;
-  const FieldPar<T> fp = e.fp;
   const int NB = e.NB, nb = e.nb, nf = e.nf, n1 = e.n1, nrows = e.nrows, rp0 = e.rp0;
-  const T cC = T(0.62035049089940009);
   double acc[NCH];
 #pragma unroll
   for (int ch = 0; ch < NCH; ++ch) acc[ch] = 0.0;
-  const unsigned m2n1 = magic32(2 * n1);
-  const int total = nb * 2 * n1;
-  for (int w0i = tid; w0i < total; w0i += 2 * nthr) {
-    // two points per iteration: all global loads of both are issued first
-    int idxs[2];
-    bool ok[2];
-    T vi[2], aa[2], bx[2], ex[2], ey[2];
-    int rb[2];
+  const unsigned mn1 = magic32(n1);
+  for (int w = tid; w < nb * n1; w += nthr) {
+    const int b = magic_div32(w, mn1), i = w - b * n1;
+    const int j0 = 2 * (rp0 + b);
+    const bool has1 = j0 + 1 < nrows;
+    const int idx0 = j0 * n1 + i, idx1 = has1 ? idx0 + n1 : idx0;
+    // every global load of both points first
+    const T vi0 = vion[idx0], vi1 = vion[idx1];
+    const T aa0 = A[idx0], aa1 = A[idx1];
+    // the second input (p in CG evaluations, d in line searches; the first
+    // evaluation of a solve has none: its coefficient is 0)
+    constexpr bool HASB = EV == EV_CG || EV == EV_LS;
+    const T bx0 = HASB ? B[idx0] : T(0), bx1 = HASB ? B[idx1] : T(0);
+    // the CG evaluation's second input is p, the line search's are phi and d
+    const T ex0 = EV == EV_CG ? bb[idx0] : EV == EV_LS ? aa0 : T(0);
+    const T ex1 = EV == EV_CG ? bb[idx1] : EV == EV_LS ? aa1 : T(0);
+    T o0[NFM], o1[NFM];
+    const cx<T>* rv = e.res + i * NB + b;
 #pragma unroll
-    for (int u = 0; u < 2; ++u) {
-      const int w = w0i + u * nthr;
-      const int b = magic_div32(w, m2n1), rem = w - b * 2 * n1;
-      const int half = rem >= n1 ? 1 : 0, i = rem - half * n1;
-      const int j = 2 * (rp0 + b) + half;
-      ok[u] = w < total && j < nrows;
-      const int idx = ok[u] ? j * n1 + i : 0;
-      idxs[u] = idx;
-      rb[u] = i * NB + b + (half << 30);
-      vi[u] = vion[idx];
-      aa[u] = A[idx];
-      bx[u] = RHO ? T(0) : B[idx];
-      // the CG evaluation's second input is p, the line search's are phi and d
-      ex[u] = EV == EV_CG ? bb[idx] : EV == EV_LS ? aa[u] : T(0);
-      ey[u] = (EV == EV_CG || EV == EV_LS) ? bx[u] : T(0);
+    for (int f = 0; f < NFM; ++f) {
+      const cx<T> z = f < nf ? rv[f * nb] : mk<T>(T(0), T(0));
+      o0[f] = z.x;
+      o1[f] = z.y;
     }
+    T sums[NCH];
 #pragma unroll
-    for (int u = 0; u < 2; ++u) {
-      if (!ok[u]) continue;
-      const int idx = idxs[u];
-      const int half = rb[u] >> 30;
-      const cx<T>* rv = e.res + (rb[u] & ((1 << 30) - 1));
-      T o[NFM];
+    for (int ch = 0; ch < NCH; ++ch) sums[ch] = T(0);
+    epi_point<T, KS, EV, ENERGY>(e, o0, vi0, aa0, bx0, ex0, bx0, idx0, sums);
+    if (has1) epi_point<T, KS, EV, ENERGY>(e, o1, vi1, aa1, bx1, ex1, bx1, idx1, sums);
 #pragma unroll
-      for (int f = 0; f < NFM; ++f) {
-        if (f < nf) {
-          const cx<T> z = rv[f * nb];
-          o[f] = half == 0 ? z.x : z.y;
-        } else {
-          o[f] = T(0);
-        }
-      }
-      T phin, rho, sq;
-      if (RHO) {
-        rho = aa[u];
-        sq = m_sqrt(rho);
-        phin = sq;
-      } else {
-        phin = e.in.ca * aa[u] + e.in.cb * bx[u];
-        rho = phin * phin;
-        sq = phin < T(0) ? -phin : phin;
-      }
-      const T x = m_rcbrt(rho);        // rho^(-1/3)
-      const T r13 = rho * x * x;       // rho^(1/3)
-      const T r23 = r13 * r13;
-      const T rinv = x * x * x;        // 1/rho
-      T vxc, exc;
-      lda_point(rho, r13, cC * x, vxc, exc);
-      T vnl, enl, lap;
-      const T al = e.al, be = e.be, cTF = e.cTF;
-      if constexpr (KS == KS_WT) {
-        const T rbeta = fp.pow56 ? sq * r13 : m_pow(rho, be);
-        const T ralpha = fp.aeqb ? rbeta : m_pow(rho, al);
-        const T pa = nf > 3 ? o[3] : o[1];
-        vnl = cTF * (al * (ralpha * rinv) * o[1] + be * (rbeta * rinv) * pa);
-        enl = cTF * ralpha * o[1];
-        lap = o[2];
-      } else {
-        const T th = rho - fp.rho_s;
-        const T ralpha = m_pow(rho, al);
-        const T rbeta = fp.sum53 ? rho * r23 / ralpha : m_pow(rho, be);
-        vnl = cTF * ((rbeta * rinv) * (be * o[2] + (rho + be * th) * o[3] + th * (rho + be * th * T(0.5)) * o[4]) +
-                     (ralpha * rinv) * (al * o[5] + (rho + al * th) * o[6] + th * (rho + al * th * T(0.5)) * o[7]));
-        enl = cTF * rbeta * (o[2] + th * o[3] + th * th * T(0.5) * o[4]);
-        lap = o[1];
-      }
-      const T potr = vi[u] + o[0] + vxc + e.ctf53 * r23 + vnl;
-      const T muv = e.muv;
-      const T pot = e.opt_sqrt ? T(2) * sq * potr + muv * lap : potr + muv * lap * (T(0.5) * sq * rinv);
-      if constexpr (ENERGY) {
-        acc[CH_EIE] += (double)rho * (double)vi[u];
-        acc[CH_EH] += 0.5 * (double)o[0] * (double)rho;
-        acc[CH_EXC] += (double)exc;
-        acc[CH_ETF] += (double)(e.lam * cTF) * (double)(rho * r23);
-        acc[CH_EVW] += 0.5 * (double)muv * (double)sq * (double)lap;
-        acc[CH_ENL] += (double)enl;
-      }
-      const T sg = phin < T(0) ? T(-1) : T(1);
-      if constexpr (EV == EV_RHO) {
-        w0[idx] = pot;
-      } else if constexpr (EV == EV_PHI) {
-        const T gg = pot * sg;
-        w0[idx] = gg;
-        acc[CH_M0] += (double)gg * (double)phin;
-        acc[CH_M1] += (double)phin * (double)phin;
-      } else if constexpr (EV == EV_CG) {
-        const T gg = pot * sg;
-        const T ap = ((gg - e.mu0 * T(2) * phin) - ex[u]) * e.ieps;
-        w1[idx] = ap;
-        acc[CH_M0] += (double)ey[u] * (double)ap;
-      } else {  // EV_LS
-        const T gg = pot * sg;
-        w1[idx] = gg;
-        trial[idx] = phin;
-        const T dir = -ex[u] * e.st + ey[u] * e.ctd;
-        const T dl = gg - T(2) * phin * e.mu0;
-        acc[CH_M0] += (double)gg * (double)dir;
-        acc[CH_M1] += (double)dl * (double)dl;
-        acc[CH_M2] += (double)gg * (double)phin;
-        acc[CH_M3] += (double)phin * (double)phin;
-      }
-    }
+    for (int ch = 0; ch < NCH; ++ch) acc[ch] += (double)sums[ch];
   }
 #pragma unroll
   for (int ch = 0; ch < NCH; ++ch) acc_out[ch] = acc[ch];

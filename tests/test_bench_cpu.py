@@ -18,3 +18,20 @@ def test_reference_arm_json_line():
     assert d["impl"] == "reference" and d["value"] > 0
     assert d["cpu_baseline"]["kind"] == "port" and d["cpu_baseline"]["cores"] >= 1
     assert d["e2e"]["h2d_bytes_per_step"] == 0 and d["e2e"]["value"] == d["value"]
+
+
+def test_gpus_flag_starts_its_own_ranks():
+    """`bench.py --gpus 2` without a launcher starts two ranks itself; on a CPU
+    box with the host-emulation build of the engine (PROFESS_B200_LIB) the
+    line reports both ranks' work."""
+    from profess_b200 import build
+    emu = build.build_emu()
+    env = dict(os.environ, PROFESS_B200_LIB=emu)
+    env.pop("WORLD_SIZE", None)
+    out = subprocess.run([sys.executable, os.path.join(ROOT, "bench.py"), "--gpus", "2", "--workload", "cfg1",
+                          "--batch", "1", "--steps", "1", "--warmup", "1", "--no-cpu-baseline"],
+                         capture_output=True, text=True, timeout=900, cwd=ROOT, env=env)
+    assert out.returncode == 0, out.stderr[-3000:]
+    d = json.loads(out.stdout.strip().splitlines()[-1])
+    assert d["n_gpus"] == 2 and d["config"]["parallelism"] == "replicas x2"
+    assert d["value"] > 0 and d["e2e"]["value"] > 0 and "emulated" in d

@@ -643,7 +643,9 @@ def _serve(eng, cells, mode, arrivals, budget, args):
         srv.submit(serving.Request(rid=i, cell=c, arrival=t, seed=i, mode=mode, fp32_tol=args.fp32_tol,
                                    refine_iters=args.refine))
     res = srv.run_until_done(timeout=3600)
-    return {r.rid: r for r in res}, serving.latency_stats(res)
+    st = serving.latency_stats(res)
+    st["host_s"] = {k: round(v, 4) for k, v in sorted(srv.phase_s.items())}
+    return {r.rid: r for r in res}, st
 
 
 def serving_compare(args, eng, rt):
@@ -670,6 +672,7 @@ def serving_compare(args, eng, rt):
         _, st = _serve(eng, cells, mode, arr, budget, args)
         results[mode] = res
         out[mode] = {"capacity_solves_per_s": rt.sum_over_ranks(cap["solves_per_s"]),
+                     "capacity_host_s_by_phase": cap["host_s"],
                      "arrival_rate_per_s": lam,
                      "solves_per_s_at_80pct": rt.sum_over_ranks(st["solves_per_s"]),
                      "latency_s": {"p50": st["p50_s"], "p99": st["p99_s"]}}

@@ -200,6 +200,12 @@ int ofdft_slot_footprint(const ofdft_cell_desc* desc, unsigned long long* bytes)
 int ofdft_slot_set_input(ofdft_engine* e, int slot, const double* rho);
 /* Start a solve from rho (host) or, with rho = NULL, from the resident input. */
 int ofdft_slot_start_solve(ofdft_engine* e, int slot, const double* rho, const ofdft_ntn_options* opts);
+/* The kernel planes, ion potential and ion-ion energy of slot src_slot,
+ * converted on the device into slot `slot` of the same grid and functional
+ * (either precision).  No counterpart in the reference: a mixed-precision
+ * request sets up its FP64 slot once (ofdft_slot_build_* and ofdft_slot_ewald)
+ * and gives its FP32 slot the same tables with this call. */
+int ofdft_slot_copy_tables(ofdft_engine* e, int slot, int src_slot);
 /* Keep the slot's current density (phi^2 of its last solve) on the device as
  * its resident input, so that a later start with rho = NULL resumes from it
  * (no counterpart in the reference, whose rhoR simply persists between

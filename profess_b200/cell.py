@@ -29,13 +29,29 @@ def wgc_tables(lib, alpha: float, beta: float, gamma: float):
     return _WGC_TABLES[key]
 
 
+def _create(eng: native.Engine, cell: Cell, precision, ion_ion) -> int:
+    rho_avg = cell.num_electrons / cell.vol
+    return eng.slot_create(cell.grid, cell.lattice, kinetic=cell.kinetic, alpha=cell.alpha, beta=cell.beta,
+                           gamma=cell.gamma, rho0=rho_avg, rho_s=rho_avg, ion_ion=ion_ion, precision=precision)
+
+
+def slot_like(eng: native.Engine, cell: Cell, src: int, precision=native.FP32) -> int:
+    """A slot for ``cell`` whose kernel planes, ion potential and ion-ion
+    energy are converted on the device from slot ``src`` (already set up for
+    the same cell): the second precision of a mixed-precision request."""
+    s = _create(eng, cell, precision, 0.0)
+    try:
+        eng.copy_tables(s, src)
+    except Exception:
+        eng.slot_destroy(s)
+        raise
+    return s
+
+
 def setup_slot(eng: native.Engine, cell: Cell, precision=native.FP64, ion_ion=None) -> int:
     """Create a slot for ``cell`` and build its kernel and ion potential on the
     device; the Ewald energy is summed on the device unless ``ion_ion`` gives it."""
-    rho_avg = cell.num_electrons / cell.vol
-    s = eng.slot_create(cell.grid, cell.lattice, kinetic=cell.kinetic, alpha=cell.alpha, beta=cell.beta,
-                        gamma=cell.gamma, rho0=rho_avg, rho_s=rho_avg, ion_ion=0.0 if ion_ion is None else ion_ion,
-                        precision=precision)
+    s = _create(eng, cell, precision, 0.0 if ion_ion is None else ion_ion)
     try:
         if cell.kinetic == native.KEDF_WT:
             eng.build_wt_kernel(s)

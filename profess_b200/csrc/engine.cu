@@ -81,15 +81,19 @@ static int odd_columns(int nf, int rp, size_t csz) {
 }
 
 // Launch shape of a slot's passes: row pairs per x-forward task (*rp1) and
-// per x-inverse task (s.rp), carrying every field (or ion species) of up to
-// OFDFT_XPASS_POINTS / n1 row pairs in OFDFT_XPASS_KB32 (FP32) or
+// per x-inverse task (s.rp), up to OFDFT_XPASS_POINTS / n1 of them, whose
+// transform buffers (every field or ion species; the x-forward pass adds its
+// staged input rows) fit OFDFT_XFWD_KB32 / OFDFT_XINV_KB32 (FP32) or
 // OFDFT_XPASS_KB64 (FP64) KB of shared memory; and the tiles of the split y/z
 // path: z columns per y-pass task (*ty: columns of n2 values at an odd row
 // pitch) and y columns per z-pass task (*tz: a group of gmax fields of n3
 // values each), each in about 48 KB, at least 32 columns when n allows.
 // s needs n1..n3, k1, nf and kinetic; csz is the size of one complex value.
-#ifndef OFDFT_XPASS_KB32
-#define OFDFT_XPASS_KB32 48
+#ifndef OFDFT_XFWD_KB32
+#define OFDFT_XFWD_KB32 48
+#endif
+#ifndef OFDFT_XINV_KB32
+#define OFDFT_XINV_KB32 48
 #endif
 #ifndef OFDFT_XPASS_KB64
 #define OFDFT_XPASS_KB64 72
@@ -98,11 +102,13 @@ static int odd_columns(int nf, int rp, size_t csz) {
 #define OFDFT_XPASS_POINTS 2048
 #endif
 static void launch_shape(SlotDev& s, size_t csz, int nfx, int* rp1, int* ty, int* tz) {
-  const size_t xkb = (size_t)(csz == 8 ? OFDFT_XPASS_KB32 : OFDFT_XPASS_KB64) * 1024;
+  const size_t esz = csz / 2;
+  const size_t fkb = (size_t)(csz == 8 ? OFDFT_XFWD_KB32 : OFDFT_XPASS_KB64) * 1024;
+  const size_t ikb = (size_t)(csz == 8 ? OFDFT_XINV_KB32 : OFDFT_XPASS_KB64) * 1024;
   *rp1 = std::max(1, std::min(32, OFDFT_XPASS_POINTS / s.n1));
-  while (*rp1 > 1 && (size_t)nfx * *rp1 * s.n1 * csz > xkb) (*rp1)--;
+  while (*rp1 > 1 && xfwd_smem(s.n1, nfx, *rp1, esz) > fkb) (*rp1)--;
   s.rp = std::max(1, std::min(32, OFDFT_XPASS_POINTS / s.n1));
-  while (s.rp > 1 && (size_t)s.nf * s.rp * s.n1 * csz + NCH * 33 * sizeof(double) > xkb) s.rp--;
+  while (s.rp > 1 && xinv_smem(s.n1, s.nf, s.rp, esz) > ikb) s.rp--;
   *rp1 = odd_columns(s.nf, *rp1, csz);
   s.rp = odd_columns(s.nf, s.rp, csz);
   const int gmax = s.kinetic == KIN_WGC ? 3 : 1;
@@ -210,6 +216,13 @@ constexpr int VCHUNK = 4096;
 #endif
 template <typename T> struct PassMinBlocks { static constexpr int value = OFDFT_MINB_FP32; };
 template <> struct PassMinBlocks<double> { static constexpr int value = OFDFT_MINB_FP64; };
+// The x-inverse pass (transform, then the real-space epilogue of two points
+// per work item) separately: its FP64 epilogue needs more registers.
+#ifndef OFDFT_XINV_MINB_FP64
+#define OFDFT_XINV_MINB_FP64 3
+#endif
+template <typename T> struct XinvMinBlocks { static constexpr int value = OFDFT_MINB_FP32; };
+template <> struct XinvMinBlocks<double> { static constexpr int value = OFDFT_XINV_MINB_FP64; };
 
 #if !defined(OFDFT_EMU)
 template <typename T> __global__ void __launch_bounds__(256) k_vec(Args<T> a) {
@@ -234,7 +247,7 @@ template <typename T, int NT> __global__ void __launch_bounds__(NT, NT == 256 ? 
   extern __shared__ __align__(16) char sm[];
   yzpass_block<T>(a, blockIdx.x, threadIdx.x, blockDim.x, sm);
 }
-template <typename T, int KS> __global__ void __launch_bounds__(256, PassMinBlocks<T>::value) k_xinv(Args<T> a) {
+template <typename T, int KS> __global__ void __launch_bounds__(256, XinvMinBlocks<T>::value) k_xinv(Args<T> a) {
   extern __shared__ __align__(16) char sm[];
   xinv_block<T, KS>(a, blockIdx.x, threadIdx.x, blockDim.x, sm);
 }
@@ -247,6 +260,15 @@ template <typename T> __global__ void __launch_bounds__(256) k_permute_kernel(co
   for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < total;
        i += (long long)gridDim.x * blockDim.x)
     ((T*)s.kern)[i] = (T)src[kernel_source_index(s, idx, i)];
+}
+// keKernel planes of a slot back into the reference layout (FP64).
+template <typename T> __global__ void __launch_bounds__(256) k_unpermute_kernel(const SlotDev* sd, const int* idx,
+                                                                               double* dst, int nplanes) {
+  const SlotDev& s = *sd;
+  const long long total = s.Nc * nplanes;
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < total;
+       i += (long long)gridDim.x * blockDim.x)
+    dst[kernel_source_index(s, idx, i)] = (double)((const T*)s.kern)[i];
 }
 template <typename T> __global__ void __launch_bounds__(256) k_fill_kernel(const SlotDev* sd, const int* idx,
                                                                           KernArgs ka, int kind) {
@@ -292,8 +314,7 @@ template <typename T> __global__ void __launch_bounds__(64) k_ctl(Args<T> a, int
 
 struct LaunchList {
   std::vector<Task> h;
-  Task* d = nullptr;
-  size_t cap = 0;
+  Task* d = nullptr;  // its part of the engine's packed device array
   size_t smem = 0;
   int nthr = 128;
 };
@@ -303,7 +324,7 @@ struct HostSlot {
   bool running = false;
   int prec = 0;
   SlotDev sd;
-  std::vector<void*> allocs;
+  std::vector<std::pair<void*, size_t>> allocs;  // device blocks and their sizes
   int nrowpairs = 0, rp1 = 1;
   int ty = 1, tz = 1;           // z columns per y-pass task and y columns per z-pass task (split path)
   bool setup_pass = false;      // running an ion-potential or force pass (split path)
@@ -316,10 +337,11 @@ struct HostSlot {
   double rho0 = 0, gamma = 2.7;
   std::vector<double> frac, zion;
   void* input = nullptr;        // device-resident input density (ofdft_slot_set_input)
+  size_t input_bytes = 0, stencil_bytes = 0;  // pooled sizes of input and d_stencil
   // pseudopotential tables and B-spline factors of the last ion-potential build
   // (device copy, and the host copy they were uploaded from)
   void* ion_aux = nullptr;
-  size_t ion_aux_bytes = 0;
+  size_t ion_aux_bytes = 0, ion_aux_cap = 0;  // bytes in use, pooled size
   std::vector<double> ion_tab;
   IonAux ion_ax;
 };
@@ -377,7 +399,11 @@ struct Engine {
   int dzero(void* d, size_t n) { return on_stream(cudaMemsetAsync(d, 0, n, stream), "cudaMemsetAsync"); }
   int dmalloc(void** p, size_t n) {
     int rc = cuda_check(cudaMalloc(p, n ? n : 1), "cudaMalloc");
-    return rc ? rc : dzero(*p, n ? n : 1);
+    if (rc) {
+      cudaGetLastError();  // a failed allocation must not show up as a later launch error
+      return rc;
+    }
+    return dzero(*p, n ? n : 1);
   }
 #endif
 
@@ -406,8 +432,9 @@ struct Engine {
     if (stream) cudaStreamSynchronize(stream);
 #endif
     for (int i = 0; i < cap; ++i) free_slot(i);
-    for (auto& pl : lists)
-      for (auto& l : pl) dfree(l.d);
+    pool_flush();
+    dfree(d_tasks);
+    d_tasks = nullptr;
     dfree(d_slots);
     dfree(d_ctl);
     plans.release();
@@ -419,18 +446,63 @@ struct Engine {
 #endif
   }
 
+  // Device memory of destroyed slots, kept for reuse: a serving engine creates
+  // and destroys slots all the time, and cudaMalloc / cudaFree (which
+  // synchronises the device) cost far more than reuse.  A request takes the
+  // smallest pooled block of at least its size and at most twice it; the
+  // bytes it needs are zeroed like a new block's.  The pool is released when
+  // an allocation fails, and holds at most POOL_MAX bytes.
+  std::multimap<size_t, void*> pool;
+  size_t pool_bytes = 0;
+  static constexpr size_t POOL_MAX = size_t(32) << 30;
+  int pmalloc(void** p, size_t n, size_t* got) {
+    n = n ? n : 1;
+    auto it = pool.lower_bound(n);  // the smallest pooled block that holds n bytes, if at most 2n
+    if (it != pool.end() && it->first <= 2 * n) {
+      *p = it->second;
+      *got = it->first;
+      pool_bytes -= it->first;
+      pool.erase(it);
+      return dzero(*p, n);
+    }
+    *got = n;
+    int rc = dmalloc(p, n);
+    if (rc == OFDFT_ENOMEM && !pool.empty()) {
+      pool_flush();
+      rc = dmalloc(p, n);
+    }
+    return rc;
+  }
+  void pfree(void* p, size_t n) {
+    if (!p) return;
+    n = n ? n : 1;
+    if (pool_bytes + n > POOL_MAX) {
+      dfree(p);
+      return;
+    }
+    pool.emplace(n, p);
+    pool_bytes += n;
+  }
+  void pool_flush() {
+    for (auto& kv : pool) dfree(kv.second);
+    pool.clear();
+    pool_bytes = 0;
+  }
+
   void free_slot(int i) {
     HostSlot& h = slots[i];
-    for (void* p : h.allocs) dfree(p);
+    for (auto& a : h.allocs) pfree(a.first, a.second);
     h.allocs.clear();
-    if (h.d_stencil) dfree(h.d_stencil);
+    pfree(h.d_stencil, h.stencil_bytes);
     h.d_stencil = nullptr;
+    h.stencil_bytes = 0;
     h.nion = 0;
-    if (h.input) dfree(h.input);
+    pfree(h.input, h.input_bytes);
     h.input = nullptr;
-    if (h.ion_aux) dfree(h.ion_aux);
+    h.input_bytes = 0;
+    pfree(h.ion_aux, h.ion_aux_cap);
     h.ion_aux = nullptr;
-    h.ion_aux_bytes = 0;
+    h.ion_aux_bytes = h.ion_aux_cap = 0;
     h.ion_tab.clear();
     h.used = false;
     h.running = false;
@@ -438,10 +510,14 @@ struct Engine {
   }
 
   int alloc(HostSlot& h, void** p, size_t bytes) {
-    int rc = dmalloc(p, bytes);
-    if (rc == OFDFT_OK) h.allocs.push_back(*p);
+    size_t got = 0;
+    int rc = pmalloc(p, bytes, &got);
+    if (rc == OFDFT_OK) h.allocs.push_back({*p, got});
     return rc;
   }
+  // A block of the pool for a slot's single buffers (input density, ion
+  // stencils, ion tables): its pooled size is kept in *size.
+  int palloc(void** p, size_t bytes, size_t* size) { return pmalloc(p, bytes, size); }
 
   int upload_slot(int i) { return h2d(d_slots + i, &slots[i].sd, sizeof(SlotDev)); }
 
@@ -674,10 +750,10 @@ struct Engine {
       const std::vector<cx<double>> b1 = bspline_b(s.k1, s.n1), b2 = bspline_b(s.n2, s.n2), b3 = bspline_b(s.n3, s.n3);
       const size_t bytes = sizeof(double) * tab.size() + sizeof(cx<double>) * (b1.size() + b2.size() + b3.size());
       if (h.ion_aux_bytes != bytes) {
-        if (h.ion_aux) dfree(h.ion_aux);
+        pfree(h.ion_aux, h.ion_aux_cap);
         h.ion_aux = nullptr;
-        h.ion_aux_bytes = 0;
-        if ((rc = dmalloc(&h.ion_aux, bytes))) return rc;
+        h.ion_aux_bytes = h.ion_aux_cap = 0;
+        if ((rc = palloc(&h.ion_aux, bytes, &h.ion_aux_cap))) return rc;
         h.ion_aux_bytes = bytes;
       }
       char* cur = (char*)h.ion_aux;
@@ -707,9 +783,11 @@ struct Engine {
       h.zion[k] = charge[species[k]];
     }
     if (h.nion != nion) {
-      if (h.d_stencil) dfree(h.d_stencil);
+      pfree(h.d_stencil, h.stencil_bytes);
       h.d_stencil = nullptr;
-      if ((rc = dmalloc((void**)&h.d_stencil, sizeof(IonStencil) * nion))) return rc;
+      h.stencil_bytes = 0;
+      h.nion = 0;
+      if ((rc = palloc((void**)&h.d_stencil, sizeof(IonStencil) * nion, &h.stencil_bytes))) return rc;
       h.nion = nion;
     }
     if ((rc = h2d(h.d_stencil, h.stencils.data(), sizeof(IonStencil) * nion))) return rc;
@@ -942,7 +1020,7 @@ struct Engine {
     int rc = check_slot(i);
     if (rc) return rc;
     HostSlot& h = slots[i];
-    if (!h.input && (rc = dmalloc(&h.input, elem_size(h.prec) * h.sd.N))) return rc;
+    if (!h.input && (rc = palloc(&h.input, elem_size(h.prec) * h.sd.N, &h.input_bytes))) return rc;
     return upload_real(h.prec, h.input, rho, h.sd.N);
   }
 
@@ -1059,6 +1137,62 @@ struct Engine {
     return upload_slot(i);
   }
 
+  // The kinetic kernel planes, the ion potential and the ion-ion energy of
+  // slot src, converted into slot i (same grid and functional; either
+  // precision) on the device: a mixed-precision request sets up its FP64
+  // slot once and gives its FP32 slot the same tables without a second
+  // set-up.
+  int copy_tables(int i, int src) {
+    int rc = check_slot(i);
+    if (rc) return rc;
+    if ((rc = check_slot(src))) return rc;
+    HostSlot& h = slots[i];
+    const HostSlot& g = slots[src];
+    if (h.sd.n1 != g.sd.n1 || h.sd.n2 != g.sd.n2 || h.sd.n3 != g.sd.n3 || h.sd.kinetic != g.sd.kinetic ||
+        h.nplanes != g.nplanes)
+      return fail(OFDFT_EINVAL, "the slots differ in grid or functional");
+    // the kernel planes are stored in the digit-reversed order of the slot's
+    // own transforms (FP32 and FP64 plans may differ): go through the
+    // reference layout
+    const long long nk = h.sd.Nc * h.nplanes, nv = h.sd.N;
+#if defined(OFDFT_EMU)
+    std::vector<double> ref(nk);
+    for (long long k = 0; k < nk; ++k) {
+      const long long r = kernel_source_index(g.sd, plans.d_idx, k);
+      ref[r] = g.prec == OFDFT_FP32 ? (double)((const float*)g.sd.kern)[k] : ((const double*)g.sd.kern)[k];
+    }
+    if ((rc = set_kernel(i, ref.data()))) return rc;
+    for (long long k = 0; k < nv; ++k) {
+      const double v = g.prec == OFDFT_FP32 ? (double)((const float*)g.sd.vion)[k] : ((const double*)g.sd.vion)[k];
+      if (h.prec == OFDFT_FP32) ((float*)h.sd.vion)[k] = (float)v;
+      else ((double*)h.sd.vion)[k] = v;
+    }
+#else
+    double* io = nullptr;
+    if ((rc = io_scratch(sizeof(double) * (size_t)std::max(nk, nv), (void**)&io))) return rc;
+    if (g.prec == OFDFT_FP32)
+      k_unpermute_kernel<float><<<io_blocks(nk), 256, 0, stream>>>(d_slots + src, plans.d_idx, io, h.nplanes);
+    else
+      k_unpermute_kernel<double><<<io_blocks(nk), 256, 0, stream>>>(d_slots + src, plans.d_idx, io, h.nplanes);
+    if (h.prec == OFDFT_FP32)
+      k_permute_kernel<float><<<io_blocks(nk), 256, 0, stream>>>(d_slots + i, plans.d_idx, io, h.nplanes);
+    else
+      k_permute_kernel<double><<<io_blocks(nk), 256, 0, stream>>>(d_slots + i, plans.d_idx, io, h.nplanes);
+    if (g.prec == OFDFT_FP64 && h.prec == OFDFT_FP32)
+      k_convert<double, float><<<io_blocks(nv), 256, 0, stream>>>((const double*)g.sd.vion, (float*)h.sd.vion, nv);
+    else if (g.prec == OFDFT_FP32 && h.prec == OFDFT_FP64)
+      k_convert<float, double><<<io_blocks(nv), 256, 0, stream>>>((const float*)g.sd.vion, (double*)h.sd.vion, nv);
+    else if (g.prec == OFDFT_FP32)
+      k_convert<float, float><<<io_blocks(nv), 256, 0, stream>>>((const float*)g.sd.vion, (float*)h.sd.vion, nv);
+    else
+      k_convert<double, double><<<io_blocks(nv), 256, 0, stream>>>((const double*)g.sd.vion, (double*)h.sd.vion, nv);
+    if ((rc = cuda_check(cudaGetLastError(), "table copy launch"))) return rc;
+    if ((rc = sync_stream())) return rc;
+#endif
+    h.sd.ion_ion = g.sd.ion_ion;
+    return upload_slot(i);
+  }
+
   // Keep the slot's current density phi^2 as its resident input (device to
   // device), so that a later start with rho = NULL resumes from it after
   // passes that reuse the state arrays (the ion-potential build does).
@@ -1068,7 +1202,7 @@ struct Engine {
     HostSlot& h = slots[i];
     Ctl c;
     if ((rc = get_ctl(i, c))) return rc;
-    if (!h.input && (rc = dmalloc(&h.input, elem_size(h.prec) * h.sd.N))) return rc;
+    if (!h.input && (rc = palloc(&h.input, elem_size(h.prec) * h.sd.N, &h.input_bytes))) return rc;
     const void* sp = h.sd.buf[c.status == ST_IDLE ? B_PHI : c.iphi];
     const long long n = h.sd.N;
 #if defined(OFDFT_EMU)
@@ -1207,7 +1341,7 @@ struct Engine {
       for (int r = 0; r < h.nrowpairs; r += h.rp1)
         L[px1].h.push_back({i, 0, r, std::min(h.rp1, h.nrowpairs - r)});
       L[px1].nthr = 256;
-      L[px1].smem = std::max(L[px1].smem, (size_t)std::max(s.nf, s.ion.nspec) * h.rp1 * s.n1 * cs);
+      L[px1].smem = std::max(L[px1].smem, xfwd_smem(s.n1, std::max(s.nf, s.ion.nspec), h.rp1, cs / 2));
       if (uses_yz(h)) {  // fused y-z pass: one task per (field, kx)
         const size_t sm = yz_smem(s, cs);
         const int pyz = sm <= YZ_SMEM_SMALL ? P_YZ : P_YZB;
@@ -1238,32 +1372,41 @@ struct Engine {
       L[P_CTL].nthr = 64;
       L[P_CTL].smem = 0;
       L[px5].nthr = 256;
-      L[px5].smem = std::max(L[px5].smem, (size_t)std::max(s.nf, s.ion.nspec) * s.rp * s.n1 * cs +
-                                              NCH * 33 * sizeof(double) + 16);
+      L[px5].smem = std::max(L[px5].smem, xinv_smem(s.n1, std::max(s.nf, s.ion.nspec), s.rp, cs / 2));
     }
 #if defined(OFDFT_EMU)
     for (int p = 0; p < 2; ++p)
       for (int k = 0; k < NPASS; ++k) lists[p][k].nthr = 1;
 #endif
+    // every list packed into one device array, uploaded with one copy
+    packed.clear();
+    size_t off[2][NPASS];
     for (int p = 0; p < 2; ++p)
       for (int k = 0; k < NPASS; ++k) {
-        LaunchList& l = lists[p][k];
-        if (l.h.size() > l.cap) {
-          dfree(l.d);
-          l.d = nullptr;
-          size_t nc = std::max<size_t>(l.h.size(), 2 * l.cap);
-          int rc = dmalloc((void**)&l.d, nc * sizeof(Task));
-          if (rc) return rc;
-          l.cap = nc;
-        }
-        if (!l.h.empty()) {
-          int rc = h2d(l.d, l.h.data(), l.h.size() * sizeof(Task));
-          if (rc) return rc;
-        }
+        off[p][k] = packed.size();
+        packed.insert(packed.end(), lists[p][k].h.begin(), lists[p][k].h.end());
       }
+    if (packed.size() > tasks_cap) {
+      dfree(d_tasks);
+      d_tasks = nullptr;
+      tasks_cap = 0;
+      const size_t nc = std::max<size_t>(packed.size(), 2 * tasks_cap + 1024);
+      int rc = dmalloc((void**)&d_tasks, nc * sizeof(Task));
+      if (rc) return rc;
+      tasks_cap = nc;
+    }
+    for (int p = 0; p < 2; ++p)
+      for (int k = 0; k < NPASS; ++k) lists[p][k].d = d_tasks + off[p][k];
+    if (!packed.empty()) {
+      int rc = h2d(d_tasks, packed.data(), packed.size() * sizeof(Task));
+      if (rc) return rc;
+    }
     dirty = false;
     return OFDFT_OK;
   }
+  std::vector<Task> packed;  // host copy of the packed task lists
+  Task* d_tasks = nullptr;
+  size_t tasks_cap = 0;
 
   template <typename T>
   Args<T> args(int prec, int pass) {
@@ -1511,7 +1654,8 @@ int ofdft_slot_create(ofdft_engine* e, const ofdft_cell_desc* d, int* slot) {
 
 int ofdft_slot_destroy(ofdft_engine* e, int slot) {
   if (!e || slot < 0 || slot >= e->eng.cap) return fail(OFDFT_EINVAL, "invalid slot");
-  dsync();
+  int rc = e->eng.sync_stream();  // every use of the slot's memory is on the engine stream
+  if (rc) return rc;
   e->eng.free_slot(slot);
   return OFDFT_OK;
 }
@@ -1536,6 +1680,11 @@ int ofdft_slot_set_ion_potential(ofdft_engine* e, int slot, const double* v) {
 int ofdft_slot_ewald(ofdft_engine* e, int slot, double* energy, double* forces) {
   if (!e) return fail(OFDFT_EINVAL, "null engine");
   return e->eng.slot_ewald(slot, energy, forces);
+}
+
+int ofdft_slot_copy_tables(ofdft_engine* e, int slot, int src_slot) {
+  if (!e) return fail(OFDFT_EINVAL, "null engine");
+  return e->eng.copy_tables(slot, src_slot);
 }
 
 int ofdft_slot_hold_density(ofdft_engine* e, int slot) {
@@ -2028,10 +2177,10 @@ extern "C" int ofdft_calculate_potential_plus_noalloc(const ofdft_cell_desc* d, 
   a.tw = (const cx<double>*)(base + o_tw);
   a.idx = didx;
   a.vchunk = VCHUNK;
-  const size_t sm1 = (size_t)s.nf * rp1 * s.n1 * cs;
+  const size_t sm1 = xfwd_smem(s.n1, s.nf, rp1, cs / 2);
   const size_t sm2 = (size_t)ty * (s.n2 | 1) * cs;
   const size_t sm3 = (size_t)tz * s.n3 * cs;
-  const size_t sm5 = (size_t)s.nf * s.rp * s.n1 * cs + NCH * 33 * sizeof(double) + 16;
+  const size_t sm5 = xinv_smem(s.n1, s.nf, s.rp, cs / 2);
   auto attr = [&](auto kern, size_t sm) -> int {
     if (sm <= 48 * 1024) return OFDFT_OK;
     return cuda_check(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm),

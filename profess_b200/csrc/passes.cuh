@@ -52,6 +52,23 @@ struct Args {
   int vchunk;        // points per task of the vector kernel
 };
 
+// Shared memory of an x-inverse task with nfb transformed fields (or ion
+// species) and nb row pairs, elements of esz bytes: the transform buffer,
+// then the reduction scratch.
+HD size_t align16(size_t x) { return (x + 15) & ~size_t(15); }
+HD size_t xinv_smem(int n1, int nfb, int nb, size_t esz) {
+  return align16((size_t)nfb * nb * n1 * 2 * esz) + NCH * 33 * sizeof(double);
+}
+
+// Shared memory of an x-forward task: the transform buffer, then the task's
+// rows of the two evaluation inputs.
+HD size_t xfwd_stage_offset(int n1, int nfb, int nb, size_t esz) {
+  return align16((size_t)nfb * nb * n1 * 2 * esz);
+}
+HD size_t xfwd_smem(int n1, int nfb, int nb, size_t esz) {
+  return xfwd_stage_offset(n1, nfb, nb, esz) + 2 * align16((size_t)2 * nb * n1 * esz);
+}
+
 // V_loc(|q|) by the index-knot cubic spline (PspRecipCubicSpline, LocalPseudoPot.f90:92-202).
 HD double psp_value(const IonAux& x, int sp, double q) {
   const PspDev& p = x.psp[sp];
@@ -396,7 +413,7 @@ struct EvalIn {
       sq = m_sqrt(rho);
       phin = sq;
     } else {
-      phin = ca * A[i] + cb * B[i];
+      phin = cb == T(0) ? ca * A[i] : ca * A[i] + cb * B[i];
       rho = phin * phin;
       sq = phin < T(0) ? -phin : phin;  // sqrt(rho) = |phi_in|
     }
@@ -476,10 +493,24 @@ HD void xfwd_block(const Args<T>& a, int bid, int tid, int nthr, char* smem) {
   const int n1 = s.n1, k1 = s.k1;
   const int nrows = s.n2 * s.n3;
   const long long Nc = s.Nc;
-  const EvalIn<T> in = eval_in<T>(s, c);
+  EvalIn<T> in = eval_in<T>(s, c);
   const FieldPar<T> fp = field_par<T>(s);
   const FftPlan& px = s.px;
   cx<T>* buf = (cx<T>*)smem;
+  // the task's rows of the evaluation inputs, staged with asynchronous copies
+  // (local row r at [r*n1 + i])
+  const int rows = nrows - 2 * rp0 < 2 * nb ? nrows - 2 * rp0 : 2 * nb;
+  if (ev != EV_ION) {
+    const size_t rbytes = (size_t)rows * n1 * sizeof(T), goff = (size_t)2 * rp0 * n1;
+    T* sa = (T*)(smem + xfwd_stage_offset(n1, nfe, nb, sizeof(T)));
+    T* sb = (T*)((char*)sa + align16((size_t)2 * nb * n1 * sizeof(T)));
+    cp_async_block(sa, in.A + goff, rbytes, (int)sizeof(T), tid, nthr);
+    if (!in.rho_mode && in.cb != T(0)) cp_async_block(sb, in.B + goff, rbytes, (int)sizeof(T), tid, nthr);
+    in.A = sa;
+    in.B = sb;
+    cp_async_wait();
+    BLOCK_SYNC();
+  }
   const unsigned mn1 = magic32(n1);
   for (int w = tid; w < nb * n1; w += nthr) {
     const int b = magic_div32(w, mn1), i = w - b * n1;
@@ -495,13 +526,13 @@ HD void xfwd_block(const Args<T>& a, int bid, int tid, int nthr, char* smem) {
     }
     T v0[NFM], v1[NFM];
     T phin, rho, sq;
-    in.at(j0 * n1 + i, phin, rho, sq);
+    in.at(2 * b * n1 + i, phin, rho, sq);
     if (ev == EV_FORCE) v0[0] = rho;
     else field_values<T, KS>(fp, nfe, rho, sq, v0);
 #pragma unroll
     for (int f = 0; f < NFM; ++f) v1[f] = T(0);
     if (has1) {
-      in.at(j1 * n1 + i, phin, rho, sq);
+      in.at((2 * b + 1) * n1 + i, phin, rho, sq);
       if (ev == EV_FORCE) v1[0] = rho;
       else field_values<T, KS>(fp, nfe, rho, sq, v1);
     }

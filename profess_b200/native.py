@@ -75,6 +75,7 @@ SIGNATURES = {
     "ofdft_slot_set_ion_potential": [_vp, ctypes.c_int, _dp],
     "ofdft_slot_set_ion_ion_energy": [_vp, ctypes.c_int, ctypes.c_double],
     "ofdft_slot_hold_density": [_vp, ctypes.c_int],
+    "ofdft_slot_copy_tables": [_vp, ctypes.c_int, ctypes.c_int],
     "ofdft_engine_capture_stats": [_vp, ctypes.POINTER(ctypes.c_longlong), _dp],
     "ofdft_slot_ewald": [_vp, ctypes.c_int, _dp, _dp],
     "ofdft_slot_build_wt_kernel": [_vp, ctypes.c_int],
@@ -284,6 +285,10 @@ class Engine:
         f = np.zeros((nion, 3)) if want_forces else None
         self._check(self.lib.ofdft_slot_ewald(self.h, slot, _ptr(e), _ptr(f) if want_forces else None))
         return float(e[0]), f
+
+    def copy_tables(self, slot, src):
+        """Kernel planes, ion potential and ion-ion energy of slot src, converted into slot."""
+        self._check(self.lib.ofdft_slot_copy_tables(self.h, slot, src))
 
     def hold_density(self, slot):
         """Keep the slot's solved density as its resident input (start_solve(slot) resumes from it)."""

@@ -11,13 +11,12 @@ admission.
 A mixed-precision request runs an FP32 slot until the FP32 line-search floor
 (or the FP32 tolerance), then FP64 refinement iterations in an FP64 slot
 started from the FP32 density on the device; a plain request runs FP64
-throughout.  A mixed request holds only its FP32 slot's memory during the
-FP32 phase: its FP64 slot is set up when the refinement starts, and the FP32
-slot is released as soon as the refinement has taken its density.  Admission
-keeps free the memory of the largest FP64 slot that a request in its FP32
-phase will need, so a refinement can always start once the requests ahead of
-it finish.  Densities and solver state stay on the device until the result is
-read.  Finished slots are released at once, so waiting requests enter as
+throughout.  A mixed request sets up its FP64 slot at admission (kernel,
+ion potential and Ewald energy built on the device) and gives its FP32 slot
+the same tables by a conversion on the device, so it pays for one set-up like
+a plain request; the FP32 slot is released as soon as the refinement has
+taken its density.  Densities and solver state stay on the device until the
+result is read.  Finished slots are released at once, so waiting requests enter as
 soon as memory frees up.  Latency is arrival to result.
 
 Multi-GPU serving runs one server per GPU (replicas); ``partition`` assigns
@@ -25,7 +24,9 @@ request ids to ranks with no exchange on the data path.
 """
 from __future__ import annotations
 
+import collections
 import concurrent.futures
+import contextlib
 import dataclasses
 import os
 import time
@@ -33,7 +34,7 @@ import time
 import numpy as np
 
 from . import native
-from .cell import setup_slot
+from .cell import setup_slot, slot_like
 from .workloads import Cell, initial_density
 
 MODE_MIXED = "mixed"
@@ -79,12 +80,12 @@ def slot_bytes(lib, cell: Cell, precision) -> int:
 
 
 def footprint(lib, cell: Cell, mode: str) -> int:
-    """Largest device footprint of a request at any time: its FP64 slot (plain
-    or refinement phase) or its FP32 slot (FP32 phase)."""
+    """Largest device footprint of a request: its FP64 slot, plus its FP32
+    slot during the FP32 phase of a mixed request."""
     b64 = slot_bytes(lib, cell, native.FP64)
     if mode == MODE_FP64:
         return b64
-    return max(b64, slot_bytes(lib, cell, native.FP32))
+    return b64 + slot_bytes(lib, cell, native.FP32)
 
 
 def _pool_workers() -> int:
@@ -107,9 +108,18 @@ class Server:
         self.results = []
         self.pool = concurrent.futures.ThreadPoolExecutor(max_workers=_pool_workers())
         self.prep = {}               # rid -> future of (ion-ion energy, initial density)
+        self.phase_s = collections.defaultdict(float)  # host seconds per phase of the loop
 
     def now(self) -> float:
         return self.clock() - self.t0
+
+    @contextlib.contextmanager
+    def _phase(self, name):
+        t0 = self.clock()
+        try:
+            yield
+        finally:
+            self.phase_s[name] += self.clock() - t0
 
     def submit(self, req: Request):
         self.future.append(req)
@@ -127,42 +137,14 @@ class Server:
             self.waiting.append(req)
             self.prep[req.rid] = self.pool.submit(self._prepare, self.eng.lib, req)
 
-    def _reserve(self, extra: int = 0) -> int:
-        """Memory kept free for refinements: the largest FP64 slot a request in
-        its FP32 phase (or one about to enter it, ``extra``) will need."""
-        need = [st["b64"] for st in self.active.values() if st["phase"] in ("fp32", "await")]
-        return max(need + [extra])
-
-    def _start_refinements(self):
-        """Mixed requests whose FP32 phase ended: set up the FP64 slot when its
-        memory is free, hand the density over on the device, free the FP32 slot."""
-        for rid in sorted(self.active, key=lambda r: self.active[r]["admitted"]):
-            st = self.active[rid]
-            if st["phase"] != "await":
-                continue
-            if self.used + st["b64"] > self.budget:
-                return  # in admission order: the oldest refinement goes first
-            req = st["req"]
-            st["s64"] = setup_slot(self.eng, req.cell, native.FP64, ion_ion=st["e_ii"])
-            self.eng.start_solve_from_slot(st["s64"], st["s32"], native.ntn_options(
-                conv_check=native.CONV_POT, pot_tol=req.pot_tol, max_iter=req.refine_iters, stall_line=6))
-            _, _, s32 = self.eng.result(st["s32"], want_rho=False)
-            st["fp32_stats"] = s32
-            self.eng.slot_destroy(st["s32"])
-            st["s32"] = None
-            self.used += st["b64"] - st["b32"]
-            st["phase"] = "refine"
-
     def _admit(self):
-        self._start_refinements()
         while self.waiting and len(self.active) < self.max_active:
             req = self.waiting[0]
             b64 = slot_bytes(self.eng.lib, req.cell, native.FP64)
             b32 = slot_bytes(self.eng.lib, req.cell, native.FP32) if req.mode == MODE_MIXED else 0
-            if max(b64, b32) > self.budget:
-                raise ValueError("request %d needs %d bytes, more than the whole budget" % (req.rid, max(b64, b32)))
-            now_need = b64 if req.mode == MODE_FP64 else b32
-            if self.used + now_need + self._reserve(b64 if req.mode == MODE_MIXED else 0) > self.budget:
+            if b64 + b32 > self.budget:
+                raise ValueError("request %d needs %d bytes, more than the whole budget" % (req.rid, b64 + b32))
+            if self.used + b64 + b32 > self.budget:
                 return
             fut = self.prep[req.rid]
             if not fut.done() and self.active:
@@ -172,19 +154,21 @@ class Server:
             rho0 = fut.result()
             del self.prep[req.rid]
             st = {"req": req, "admitted": t_adm, "phase": None, "s32": None, "s64": None, "b64": b64, "b32": b32,
-                  "e_ii": None, "fp32_stats": None}
-            if req.mode == MODE_FP64:
+                  "fp32_stats": None}
+            with self._phase("setup"):
                 st["s64"] = setup_slot(self.eng, req.cell, native.FP64)  # Ewald summed on the device
-                self.eng.start_solve(st["s64"], rho0, native.ntn_options(
-                    conv_check=native.CONV_POT, pot_tol=req.pot_tol, max_iter=300))
-                st["phase"] = "fp64"
-            else:
-                st["s32"] = setup_slot(self.eng, req.cell, native.FP32)  # Ewald summed on the device
-                st["e_ii"], _ = self.eng.ewald(st["s32"], req.cell.nion, want_forces=False)
-                self.eng.start_solve(st["s32"], rho0, native.ntn_options(
-                    conv_check=native.CONV_POT, pot_tol=req.fp32_tol, max_iter=300, stall_line=6))
-                st["phase"] = "fp32"
-            self.used += now_need
+                if req.mode == MODE_MIXED:
+                    st["s32"] = slot_like(self.eng, req.cell, st["s64"], native.FP32)
+            with self._phase("start"):
+                if req.mode == MODE_FP64:
+                    self.eng.start_solve(st["s64"], rho0, native.ntn_options(
+                        conv_check=native.CONV_POT, pot_tol=req.pot_tol, max_iter=300))
+                    st["phase"] = "fp64"
+                else:
+                    self.eng.start_solve(st["s32"], rho0, native.ntn_options(
+                        conv_check=native.CONV_POT, pot_tol=req.fp32_tol, max_iter=300, stall_line=6))
+                    st["phase"] = "fp32"
+            self.used += b64 + b32
             self.active[req.rid] = st
 
     # ------------------------------------------------------------ progress
@@ -193,15 +177,27 @@ class Server:
             st = self.active[rid]
             req = st["req"]
             if st["phase"] == "fp32" and self.eng.poll(st["s32"]):
-                st["phase"] = "await"
+                # refinement in the FP64 slot from the FP32 density, on the device
+                with self._phase("start"):
+                    self.eng.start_solve_from_slot(st["s64"], st["s32"], native.ntn_options(
+                        conv_check=native.CONV_POT, pot_tol=req.pot_tol, max_iter=req.refine_iters, stall_line=6))
+                with self._phase("result"):
+                    _, _, st["fp32_stats"] = self.eng.result(st["s32"], want_rho=False)
+                with self._phase("release"):
+                    self.eng.slot_destroy(st["s32"])
+                st["s32"] = None
+                self.used -= st["b32"]
+                st["phase"] = "refine"
             elif st["phase"] in ("refine", "fp64") and self.eng.poll(st["s64"]):
-                _, e, stats = self.eng.result(st["s64"], want_rho=False)
+                with self._phase("result"):
+                    _, e, stats = self.eng.result(st["s64"], want_rho=False)
                 if st["fp32_stats"] is not None:
                     s32 = st["fp32_stats"]
                     stats = dict(stats, fp32_evals=s32["num_evals"], fp32_outcome=s32["outcome"])
                 self.results.append(Result(rid, e.copy(), stats, req.arrival, st["admitted"], self.now(),
                                            req.cell.nion, req.cell.grid, req.mode))
-                self.eng.slot_destroy(st["s64"])
+                with self._phase("release"):
+                    self.eng.slot_destroy(st["s64"])
                 self.used -= st["b64"]
                 del self.active[rid]
 
@@ -210,7 +206,8 @@ class Server:
         self._arrivals()
         self._admit()
         if self.active:
-            self.eng.run(self.ticks)
+            with self._phase("run"):
+                self.eng.run(self.ticks)
             self._advance()
             self._admit()
 

@@ -314,3 +314,31 @@ def test_grid_limits(emu_engine, n):
     with pytest.raises(native.OfdftError) as ei:
         emu_engine.slot_create(n, cell.lattice)
     assert ei.value.code == 1
+
+
+def check_copy_tables(eng):
+    """A slot whose tables are converted from another slot of the other
+    precision (ofdft_slot_copy_tables) evaluates exactly like one given the
+    same tables directly."""
+    cell, f, _, _ = cases.golden_case("wgc_al4_fcc")
+    s64 = cases.engine_slot(eng, f, cell, precision=native.FP64)
+    s32 = cases.engine_slot(eng, f, cell, precision=native.FP32)
+    c32 = eng.slot_create(f.n, cell.lattice, kinetic=f.kinetic, lam=f.lam, mu=f.mu, alpha=f.alpha, beta=f.beta,
+                          rho_s=f.rho_s, precision=native.FP32)
+    c64 = eng.slot_create(f.n, cell.lattice, kinetic=f.kinetic, lam=f.lam, mu=f.mu, alpha=f.alpha, beta=f.beta,
+                          rho_s=f.rho_s, precision=native.FP64)
+    try:
+        eng.copy_tables(c32, s64)
+        eng.copy_tables(c64, s64)
+        rho = cases.random_density(f.n, cell.num_electrons, cell.vol, seed=21)
+        for a, b in ((s32, c32), (s64, c64)):
+            pa, ea = eng.calculate_potential_plus(a, rho)
+            pb, eb = eng.calculate_potential_plus(b, rho)
+            assert np.array_equal(pa, pb) and np.array_equal(ea, eb)
+    finally:
+        for s in (s64, s32, c32, c64):
+            eng.slot_destroy(s)
+
+
+def test_copy_tables(emu_engine):
+    check_copy_tables(emu_engine)

@@ -234,3 +234,8 @@ def test_repeated_ion_builds_hold_device_memory(gpu_engine):
         assert free0 - free1 < 2 << 20
     finally:
         gpu_engine.slot_destroy(s)
+
+
+def test_copy_tables_on_gpu(gpu_engine):
+    from test_emu_engine import check_copy_tables
+    check_copy_tables(gpu_engine)

@@ -852,7 +852,7 @@ struct Engine {
     if (h.nion < 1 || s.ion.nspec < 1) return fail(OFDFT_EINVAL, "build the ion potential before the forces");
     Ctl c;
     if ((rc = get_ctl(i, c))) return rc;
-    const int iphi = c.status == ST_IDLE ? B_PHI : c.iphi;
+    const int iphi = c.iphi;  // the current phi (a new slot's record is zero: B_PHI)
     base_ctl(c, h.prec);
     c.iphi = iphi;
     c.ev = EV_FORCE;
@@ -1203,7 +1203,7 @@ struct Engine {
     Ctl c;
     if ((rc = get_ctl(i, c))) return rc;
     if (!h.input && (rc = palloc(&h.input, elem_size(h.prec) * h.sd.N, &h.input_bytes))) return rc;
-    const void* sp = h.sd.buf[c.status == ST_IDLE ? B_PHI : c.iphi];
+    const void* sp = h.sd.buf[c.iphi];  // the current phi, also after a cancel
     const long long n = h.sd.N;
 #if defined(OFDFT_EMU)
     for (long long k = 0; k < n; ++k) {

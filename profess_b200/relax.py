@@ -320,9 +320,12 @@ def cg2_moves(lattice, frac, energy, forces, force_cutoff=FORCE_CUTOFF, max_step
                 n_line += 1
 
 
-class CG2:
-    """Relax ``cells`` (each gets one FP64 slot) with the CG2 optimiser; every
-    batched step solves the densities of all cells that asked for one together."""
+class _GeneratorRelax:
+    """Relax ``cells`` (each gets one FP64 slot) with an optimiser written as a
+    generator of geometries (cg2_moves, lbfgs_moves): every batched step
+    solves the densities of all cells that asked for one together, warm-started
+    from each cell's resident density, and sends each optimiser its energy
+    and forces."""
 
     def __init__(self, eng: native.Engine, cells, max_steps: int = 200, force_cutoff: float = FORCE_CUTOFF,
                  opts=None, nn_dist: float = 2.0):
@@ -342,8 +345,7 @@ class CG2:
             self.gens = []
             for st in self.states:
                 self.traces.append([float(st.energy[0])])
-                gen = cg2_moves(st.cell.lattice, st.cell.frac, float(st.energy[0]), st.forces,
-                                force_cutoff=force_cutoff, max_steps=max_steps, nn_dist=nn_dist)
+                gen = self._moves(st, force_cutoff, max_steps, nn_dist)
                 self.gens.append(gen)
                 self._advance(st, gen, None)
         except Exception:
@@ -395,3 +397,283 @@ class CG2:
         while self.step():
             pass
         return self.states
+
+
+class CG2(_GeneratorRelax):
+    """The CG2 optimiser (ConjugateGradient, Source/IonOptCG2.f90) on batched density solves."""
+
+    def _moves(self, st, force_cutoff, max_steps, nn_dist):
+        return cg2_moves(st.cell.lattice, st.cell.frac, float(st.energy[0]), st.forces,
+                         force_cutoff=force_cutoff, max_steps=max_steps, nn_dist=nn_dist)
+
+
+# ---------------------------------------------------------------------------- BFGS
+# IonLBFGS (Source/IonOptBFGS.f90:39-290) on Nocedal's limited-memory BFGS
+# with the More-Thuente line search (LBFGS / MCSRCH / MCSTEP,
+# Source/MathLBFGS.f): 5 corrections, the driver's own force test, at most
+# 1000 energy and gradient evaluations.
+LBFGS_M = 5                  # corrections kept (IonOptBFGS.f90: M)
+LBFGS_EPS = 1.0e-5           # LBFGS's own gradient test (EPS)
+LBFGS_XTOL = 1.0e-4          # line-search interval tolerance (XTOL)
+LBFGS_FTOL = 1.0e-4          # sufficient decrease (set by LBFGS)
+LBFGS_GTOL = 0.9             # curvature condition (the LB2 default)
+LBFGS_STPMIN, LBFGS_STPMAX = 1.0e-20, 1.0e20
+LBFGS_MAXFEV = 20            # evaluations per line search
+LBFGS_MAX_CALLS = 1000       # IonOptBFGS.f90: nMax
+MT_P66 = float(np.float32(0.66))  # a single-precision literal in MCSTEP
+
+
+def mt_step(stx, fx, dx, sty, fy, dy, stp, fp, dp, brackt, stpmin, stpmax):
+    """One safeguarded step of the More-Thuente interval search (MCSTEP):
+    (stx, fx, dx, sty, fy, dy, stp, brackt, info)."""
+    if ((brackt and (stp <= min(stx, sty) or stp >= max(stx, sty))) or dx * (stp - stx) >= 0.0
+            or stpmax < stpmin):
+        return stx, fx, dx, sty, fy, dy, stp, brackt, 0
+    sgnd = dp * (dx / abs(dx))
+    if fp > fx:
+        info, bound = 1, True
+        theta = 3 * (fx - fp) / (stp - stx) + dx + dp
+        s = max(abs(theta), abs(dx), abs(dp))
+        gamma = s * np.sqrt((theta / s) ** 2 - (dx / s) * (dp / s))
+        if stp < stx:
+            gamma = -gamma
+        r = ((gamma - dx) + theta) / (((gamma - dx) + gamma) + dp)
+        stpc = stx + r * (stp - stx)
+        stpq = stx + ((dx / ((fx - fp) / (stp - stx) + dx)) / 2) * (stp - stx)
+        stpf = stpc if abs(stpc - stx) < abs(stpq - stx) else stpc + (stpq - stpc) / 2
+        brackt = True
+    elif sgnd < 0.0:
+        info, bound = 2, False
+        theta = 3 * (fx - fp) / (stp - stx) + dx + dp
+        s = max(abs(theta), abs(dx), abs(dp))
+        gamma = s * np.sqrt((theta / s) ** 2 - (dx / s) * (dp / s))
+        if stp > stx:
+            gamma = -gamma
+        r = ((gamma - dp) + theta) / (((gamma - dp) + gamma) + dx)
+        stpc = stp + r * (stx - stp)
+        stpq = stp + (dp / (dp - dx)) * (stx - stp)
+        stpf = stpc if abs(stpc - stp) > abs(stpq - stp) else stpq
+        brackt = True
+    elif abs(dp) < abs(dx):
+        info, bound = 3, True
+        theta = 3 * (fx - fp) / (stp - stx) + dx + dp
+        s = max(abs(theta), abs(dx), abs(dp))
+        gamma = s * np.sqrt(max(0.0, (theta / s) ** 2 - (dx / s) * (dp / s)))
+        if stp > stx:
+            gamma = -gamma
+        r = ((gamma - dp) + theta) / ((gamma + (dx - dp)) + gamma)
+        if r < 0.0 and gamma != 0.0:
+            stpc = stp + r * (stx - stp)
+        else:
+            stpc = stpmax if stp > stx else stpmin
+        stpq = stp + (dp / (dp - dx)) * (stx - stp)
+        if brackt:
+            stpf = stpc if abs(stp - stpc) < abs(stp - stpq) else stpq
+        else:
+            stpf = stpc if abs(stp - stpc) > abs(stp - stpq) else stpq
+    else:
+        info, bound = 4, False
+        if brackt:
+            theta = 3 * (fp - fy) / (sty - stp) + dy + dp
+            s = max(abs(theta), abs(dy), abs(dp))
+            gamma = s * np.sqrt((theta / s) ** 2 - (dy / s) * (dp / s))
+            if stp > sty:
+                gamma = -gamma
+            r = ((gamma - dp) + theta) / (((gamma - dp) + gamma) + dy)
+            stpf = stp + r * (sty - stp)
+        else:
+            stpf = stpmax if stp > stx else stpmin
+    if fp > fx:
+        sty, fy, dy = stp, fp, dp
+    else:
+        if sgnd < 0.0:
+            sty, fy, dy = stx, fx, dx
+        stx, fx, dx = stp, fp, dp
+    stp = max(stpmin, min(stpmax, stpf))
+    if brackt and bound:
+        if sty > stx:
+            stp = min(stx + MT_P66 * (sty - stx), stp)
+        else:
+            stp = max(stx + MT_P66 * (sty - stx), stp)
+    return stx, fx, dx, sty, fy, dy, stp, brackt, info
+
+
+class MoreThuente:
+    """The line search of MCSRCH along s from x: start() returns the first trial
+    point (or None when s is not a descent direction), feed(f, g) the next
+    trial point or, once done, None with .info set (1: converged)."""
+
+    def __init__(self, ftol=LBFGS_FTOL, gtol=LBFGS_GTOL, xtol=LBFGS_XTOL, stpmin=LBFGS_STPMIN,
+                 stpmax=LBFGS_STPMAX, maxfev=LBFGS_MAXFEV):
+        self.ftol, self.gtol, self.xtol = ftol, gtol, xtol
+        self.stpmin, self.stpmax, self.maxfev = stpmin, stpmax, maxfev
+        self.info = 0
+
+    def start(self, x, f, g, s, stp):
+        self.s = s
+        self.dginit = float(np.dot(g, s))
+        if self.dginit >= 0.0:
+            self.info = 0
+            return None
+        self.brackt, self.stage1, self.nfev, self.infoc = False, True, 0, 1
+        self.finit, self.dgtest = f, self.ftol * self.dginit
+        self.width = self.stpmax - self.stpmin
+        self.width1 = self.width / 0.5
+        self.wa = x.copy()
+        self.stx, self.fx, self.dgx = 0.0, f, self.dginit
+        self.sty, self.fy, self.dgy = 0.0, f, self.dginit
+        self.stp = stp
+        return self._trial()
+
+    def _trial(self):
+        if self.brackt:
+            self.stmin, self.stmax = min(self.stx, self.sty), max(self.stx, self.sty)
+        else:
+            self.stmin, self.stmax = self.stx, self.stp + 4.0 * (self.stp - self.stx)
+        self.stp = min(max(self.stp, self.stpmin), self.stpmax)
+        if ((self.brackt and (self.stp <= self.stmin or self.stp >= self.stmax)) or self.nfev >= self.maxfev - 1
+                or self.infoc == 0 or (self.brackt and self.stmax - self.stmin <= self.xtol * self.stmax)):
+            self.stp = self.stx
+        return self.wa + self.stp * self.s
+
+    def feed(self, f, g):
+        self.nfev += 1
+        dg = float(np.dot(g, self.s))
+        ftest1 = self.finit + self.stp * self.dgtest
+        info = 0
+        if (self.brackt and (self.stp <= self.stmin or self.stp >= self.stmax)) or self.infoc == 0:
+            info = 6
+        if self.stp == self.stpmax and f <= ftest1 and dg <= self.dgtest:
+            info = 5
+        if self.stp == self.stpmin and (f > ftest1 or dg >= self.dgtest):
+            info = 4
+        if self.nfev >= self.maxfev:
+            info = 3
+        if self.brackt and self.stmax - self.stmin <= self.xtol * self.stmax:
+            info = 2
+        if f <= ftest1 and abs(dg) <= self.gtol * (-self.dginit):
+            info = 1
+        if info:
+            self.info = info
+            return None
+        if self.stage1 and f <= ftest1 and dg >= min(self.ftol, self.gtol) * self.dginit:
+            self.stage1 = False
+        if self.stage1 and f <= self.fx and f > ftest1:
+            # the modified function psi(stp) = f - stp * dgtest while the step is in stage 1
+            t = self.dgtest
+            r = mt_step(self.stx, self.fx - self.stx * t, self.dgx - t, self.sty, self.fy - self.sty * t,
+                        self.dgy - t, self.stp, f - self.stp * t, dg - t, self.brackt, self.stmin, self.stmax)
+            self.stx, fxm, dgxm, self.sty, fym, dgym, self.stp, self.brackt, self.infoc = r
+            self.fx, self.fy = fxm + self.stx * t, fym + self.sty * t
+            self.dgx, self.dgy = dgxm + t, dgym + t
+        else:
+            r = mt_step(self.stx, self.fx, self.dgx, self.sty, self.fy, self.dgy, self.stp, f, dg, self.brackt,
+                        self.stmin, self.stmax)
+            self.stx, self.fx, self.dgx, self.sty, self.fy, self.dgy, self.stp, self.brackt, self.infoc = r
+        if self.brackt:
+            if abs(self.sty - self.stx) >= 0.66 * self.width1:
+                self.stp = self.stx + 0.5 * (self.sty - self.stx)
+            self.width1 = self.width
+            self.width = abs(self.sty - self.stx)
+        return self._trial()
+
+
+class Lbfgs:
+    """Limited-memory BFGS in LBFGS's reverse communication: call(x, f, g,
+    iflag) returns the point to evaluate next and the flag (1: evaluate and
+    call again, 0: converged by the gradient test, < 0: failed).  Calling
+    with iflag 0 (re)starts it from x."""
+
+    def __init__(self, m=LBFGS_M, eps=LBFGS_EPS):
+        self.m, self.eps = m, eps
+
+    def _start(self, x, g):
+        n = len(x)
+        self.s = np.zeros((self.m, n))
+        self.y = np.zeros((self.m, n))
+        self.rho = np.zeros(self.m)
+        self.diag = np.ones(n)
+        self.point, self.it = 0, 0
+        self.s[0] = -g * self.diag
+        self.stp1 = 1.0 / float(np.sqrt(np.dot(g, g)))
+
+    def _iteration(self, x, f, g):
+        """Label 80: the next search direction, then the line search's first trial."""
+        self.it += 1
+        bound = self.it - 1
+        if self.it != 1:
+            bound = min(bound, self.m)
+            last = (self.point - 1) % self.m
+            ys = float(np.dot(self.y[last], self.s[last]))
+            yy = float(np.dot(self.y[last], self.y[last]))
+            self.diag[:] = ys / yy
+            self.rho[last] = 1.0 / ys
+            q = -g
+            alpha = np.zeros(self.m)
+            cp = self.point
+            for _ in range(bound):  # newest correction first
+                cp = (cp - 1) % self.m
+                alpha[cp] = self.rho[cp] * float(np.dot(self.s[cp], q))
+                q = q - alpha[cp] * self.y[cp]
+            q = self.diag * q
+            for _ in range(bound):  # oldest first
+                beta = self.rho[cp] * float(np.dot(self.y[cp], q))
+                q = q + (alpha[cp] - beta) * self.s[cp]
+                cp = (cp + 1) % self.m
+            self.s[self.point] = q
+        self.g_old = g.copy()
+        self.ls = MoreThuente()
+        xt = self.ls.start(x, f, g, self.s[self.point], self.stp1 if self.it == 1 else 1.0)
+        if xt is None:
+            return x, -1
+        return xt, 1
+
+    def call(self, x, f, g, iflag):
+        if iflag == 0:
+            self._start(x, g)
+            return self._iteration(x, f, g)
+        xt = self.ls.feed(f, g)
+        if xt is not None:
+            return xt, 1
+        if self.ls.info != 1:
+            return x, -1
+        p = self.point
+        self.s[p] = self.ls.stp * self.s[p]
+        self.y[p] = g - self.g_old
+        self.point = (p + 1) % self.m
+        if float(np.sqrt(np.dot(g, g))) / max(1.0, float(np.sqrt(np.dot(x, x)))) <= self.eps:
+            return x, 0
+        return self._iteration(x, f, g)
+
+
+def lbfgs_moves(lattice, frac, energy, forces, force_cutoff=FORCE_CUTOFF, max_calls=LBFGS_MAX_CALLS):
+    """The BFGS optimiser (IonLBFGS) as a generator, like cg2_moves: it yields
+    the fractional coordinates of every geometry whose density it needs and
+    receives (total energy, forces) for it; its return value is the final
+    coordinates.  The unknowns are the Cartesian coordinates, ion by ion
+    within each direction (the reference's RESHAPE of cart(numIon, 3)), and
+    the gradient is minus the forces."""
+    cart2frac = np.linalg.inv(lattice)
+    x = (np.asarray(frac) @ lattice.T).ravel(order="F")
+    f, g = float(energy), -np.asarray(forces).ravel(order="F")
+    lb = Lbfgs()
+    iflag, calls = 0, 0
+    while True:
+        x, iflag = lb.call(x, f, g, iflag)
+        frac = x.reshape((-1, 3), order="F") @ cart2frac.T
+        energy, forces = yield frac
+        f, g = float(energy), -np.asarray(forces).ravel(order="F")
+        if _max_force(np.asarray(forces)) < force_cutoff or iflag < 0:
+            return frac
+        calls += 1
+        if calls > max_calls:
+            return frac
+
+
+class BFGS(_GeneratorRelax):
+    """The BFGS optimiser (IonLBFGS, Source/IonOptBFGS.f90:39-290) on batched
+    density solves; max_steps bounds the energy and gradient evaluations."""
+
+    def _moves(self, st, force_cutoff, max_steps, nn_dist):
+        return lbfgs_moves(st.cell.lattice, st.cell.frac, float(st.energy[0]), st.forces,
+                           force_cutoff=force_cutoff, max_calls=max_steps)

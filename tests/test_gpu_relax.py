@@ -13,3 +13,8 @@ def test_quickmin_matches_oracle_on_gpu(gpu_engine):
 def test_cg2_matches_oracle_on_gpu(gpu_engine):
     from test_relax import check_cg2_matches_oracle
     check_cg2_matches_oracle(gpu_engine)
+
+
+def test_bfgs_matches_oracle_on_gpu(gpu_engine):
+    from test_relax import check_bfgs_matches_oracle
+    check_bfgs_matches_oracle(gpu_engine)

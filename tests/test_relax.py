@@ -2,6 +2,7 @@
 oracle's restatement of QuickMinOptimization (oracle/relax.py), on the
 host-emulation build (CPU); test_gpu_relax.py repeats it on the CUDA build."""
 import numpy as np
+import pytest
 
 from oracle import cellsetup as cs
 from oracle import ntn
@@ -104,3 +105,79 @@ def check_cg2_matches_oracle(eng):
 
 def test_cg2_matches_oracle(emu_engine):
     check_cg2_matches_oracle(emu_engine)
+
+
+def _rosenbrock(x):
+    f = float(((1.0 - x[:-1]) ** 2 + 100.0 * (x[1:] - x[:-1] ** 2) ** 2).sum())
+    g = np.zeros_like(x)
+    g[:-1] = -2.0 * (1.0 - x[:-1]) - 400.0 * x[:-1] * (x[1:] - x[:-1] ** 2)
+    g[1:] += 200.0 * (x[1:] - x[:-1] ** 2)
+    return f, g
+
+
+def test_lbfgs_matches_oracle_on_rosenbrock():
+    """The engine's LBFGS (reverse communication) and the oracle's work-array
+    restatement take the same iterates, line-search trials included, on a
+    function whose searches bracket, interpolate and restart."""
+    from oracle import lbfgs as olb
+    for n, seed in ((2, 0), (6, 1), (12, 2)):
+        x0 = np.random.default_rng(seed).uniform(-1.5, 1.5, n)
+        xa, xb = x0.copy(), x0.copy()
+        la, lb = relax.Lbfgs(), olb.LbfgsRC(n)
+        fa, ga = _rosenbrock(xa)
+        ia = ib = 0
+        calls = 0
+        while True:
+            xa, ia = la.call(xa, fa, ga, ia)
+            ib = lb.call(xb, fa, ga, ib)
+            assert ia == ib
+            np.testing.assert_array_equal(xa, xb)
+            fa, ga = _rosenbrock(xa)
+            calls += 1
+            if ia <= 0 or calls > 400:
+                break
+        assert ia == 0 and np.abs(xa - 1.0).max() < 1e-3, (n, ia, xa)
+
+
+@pytest.mark.filterwarnings("ignore:invalid value")
+def test_mcstep_matches_oracle():
+    """MCSTEP on random states, inconsistent ones included (NaN steps where a
+    cubic has no real minimiser, as under IEEE arithmetic)."""
+    from oracle import lbfgs as olb
+    rng = np.random.default_rng(5)
+    same = lambda a, b: a == b or (a != a and b != b)  # noqa: E731
+    for _ in range(2000):
+        stx, sty = 0.0, float(rng.uniform(0.1, 2.0))
+        args = (stx, float(rng.normal()), -abs(float(rng.normal())) - 1e-3, sty, float(rng.normal()),
+                float(rng.normal()), float(rng.uniform(0.05, 3.0)), float(rng.normal()), float(rng.normal()),
+                bool(rng.integers(2)), 0.0, 4.0)
+        ra, rb = relax.mt_step(*args), olb.mcstep(*args)
+        assert all(same(a, b) for a, b in zip(ra, rb)), (args, ra, rb)
+
+
+def check_bfgs_matches_oracle(eng):
+    """IonLBFGS on the engine against the oracle, from the displaced Al4 cell:
+    the same energy after every density solve, the same final geometry."""
+    import cases
+    from oracle import lbfgs as olb
+    cell, f, _, _ = cases.golden_case("wt_al4_displaced")
+    from profess_b200 import recpot
+    z = np.load(cases.GOLDEN + "/al_hc_recpot.npz")
+    sp = recpot.species_from_table(float(z["max_g"]), z["values"], "Al")
+    c = wl.Cell(name="displaced", lattice=cell.lattice, frac=cell.frac, species_of_ion=cell.species_of_ion,
+                species=[sp], grid=tuple(f.n))
+    run = relax.BFGS(eng, [c])
+    try:
+        run.run()
+        frac, trace, forces = olb.bfgs(cell, f.n, ntn.NtnOptions())
+        assert len(run.traces[0]) == len(trace)
+        assert np.abs(np.array(run.traces[0]) - trace).max() < 1e-9
+        assert trace[-1] < trace[0] - 1e-2
+        assert relax._max_force(run.states[0].forces) < relax.FORCE_CUTOFF
+        assert np.abs(run.states[0].cell.frac - frac).max() < 2e-7
+    finally:
+        run.close()
+
+
+def test_bfgs_matches_oracle(emu_engine):
+    check_bfgs_matches_oracle(emu_engine)

@@ -141,6 +141,17 @@ int ofdft_slot_build_ion_potential(ofdft_engine* e, int slot, int nion, const do
  * when include_ewald, the ion-ion Ewald forces (ForcesII_IE,
  * Source/CalForce.f90:134-239).  Needs ofdft_slot_build_ion_potential first. */
 int ofdft_slot_forces(ofdft_engine* e, int slot, const double* rho, int include_ewald, double* forces);
+/* Stress tensor (Ha/bohr^3, stress[9] row-major and symmetric) of the slot's
+ * current density (rho = NULL: phi^2 of the last solve) or of the given rho,
+ * for the WT functional: CalculateStress (Source/CalStress.f90:44-253) with
+ * the TF, vW, WT, Hartree, LDA and B-spline ion-electron terms plus, when
+ * include_ewald, the Ewald term (EwaldStress, Source/Ewald.f90:1857-2535).
+ * terms[7*9] (may be NULL) receives the seven parts in that order.  Runs one
+ * energy evaluation and the forward transforms of the density on the device;
+ * the slot's solve record, current phi and potential are kept.  Needs
+ * ofdft_slot_build_ion_potential first. */
+int ofdft_slot_stress(ofdft_engine* e, int slot, const double* rho, int include_ewald, double* stress,
+                      double* terms);
 
 /* ---------------------------------------------------------------- host set-up helpers */
 /* Ewald ion-ion energy (Ha) and forces (may be NULL) of point charges

@@ -24,6 +24,7 @@
 
 #include "setup.cuh"
 #include "ewald.cuh"
+#include "stress.cuh"
 #include "profess_b200.h"
 
 #if !defined(OFDFT_EMU)
@@ -892,6 +893,228 @@ struct Engine {
       std::vector<double> fii(3 * (size_t)h.nion);
       if ((rc = ewald_device(i, nullptr, fii.data()))) return rc;
       for (size_t k = 0; k < fii.size(); ++k) out[k] += fii[k];
+    }
+    return OFDFT_OK;
+  }
+
+  // Stress tensor (Ha/bohr^3, out[9] row-major, symmetric) of rho (host, FP64)
+  // or, with rho NULL, of the slot's current density phi^2; terms[7*9] (may be
+  // NULL) gets the TF, vW, WT, Hartree, LDA, ion-electron and Ewald parts.
+  // The energies come from one evaluation of the density; the spectral sums
+  // from the EV_STRESS transforms and the stress reduction (stress.cuh).  The
+  // slot's control record, current phi and potential are left as they were.
+  int stress(int i, const double* rho, int include_ewald, double* out, double* terms) {
+    int rc = check_slot(i);
+    if (rc) return rc;
+    HostSlot& h = slots[i];
+    SlotDev& s = h.sd;
+    if (s.kinetic != KIN_WT) return fail(OFDFT_EINVAL, "the stress is implemented for the WT functional");
+    if (h.nion < 1 || s.ion.nspec < 1) return fail(OFDFT_EINVAL, "build the ion potential before the stress");
+    if (!(h.rho0 > 0)) return fail(OFDFT_EINVAL, "rho0 must be positive for the WT stress");
+    Ctl saved;
+    if ((rc = get_ctl(i, saved))) return rc;
+    // two work buffers that hold neither the current phi nor its potential
+    int spare[2], ns = 0;
+    for (int b = 0; b < NBUF && ns < 2; ++b)
+      if (b != saved.iphi && b != saved.iw0) spare[ns++] = b;
+    const int ib = spare[0], iw = spare[1];
+    if (rho) {
+      if ((rc = upload_real(h.prec, s.buf[ib], rho, s.N))) return rc;
+    } else {
+      const void* sp = s.buf[saved.iphi];
+#if defined(OFDFT_EMU)
+      for (long long k = 0; k < s.N; ++k) {
+        if (h.prec == OFDFT_FP32) ((float*)s.buf[ib])[k] = ((const float*)sp)[k] * ((const float*)sp)[k];
+        else ((double*)s.buf[ib])[k] = ((const double*)sp)[k] * ((const double*)sp)[k];
+      }
+#else
+      if (h.prec == OFDFT_FP32)
+        k_square_copy<float, float><<<io_blocks(s.N), 256, 0, stream>>>((const float*)sp, (float*)s.buf[ib], s.N);
+      else
+        k_square_copy<double, double><<<io_blocks(s.N), 256, 0, stream>>>((const double*)sp, (double*)s.buf[ib], s.N);
+      if ((rc = cuda_check(cudaGetLastError(), "square copy launch"))) return rc;
+#endif
+    }
+    // the energy terms of the density
+    Ctl c;
+    base_ctl(c, h.prec);
+    c.ev = EV_RHO;
+    c.iphi = ib;
+    c.iw0 = iw;
+    c.want_energy = 1;
+    if ((rc = put_ctl(i, c))) return rc;
+    if ((rc = run_one(i))) return rc;
+    if ((rc = get_ctl(i, c))) return rc;
+    double et[9];
+    for (int k = 0; k < 9; ++k) et[k] = c.energy[k];
+    // the density's forward spectra
+    base_ctl(c, h.prec);
+    c.ev = EV_STRESS;
+    c.iphi = ib;
+    if ((rc = put_ctl(i, c))) return rc;
+    if ((rc = run_one(i))) return rc;
+    // the spectral sums
+    const int nion = h.nion, L = s.k1 + s.n2 + s.n3;
+    std::vector<int> species(nion);
+    for (int k = 0; k < nion; ++k) species[k] = h.stencils[k].species;
+    StressArgs sa;
+    sa.nion = nion;
+    sa.kf = std::cbrt(3.0 * PI_D * PI_D * h.rho0);
+    const int nblk = (int)std::max<long long>(1, std::min<long long>(2 * (long long)num_sms, (s.Nc + 127) / 128));
+    std::vector<double> part((size_t)NSC * nblk);
+#if defined(OFDFT_EMU)
+    std::vector<cx<double>> sf((size_t)nion * L);
+    for (int k = 0; k < nion; ++k)
+      for (int w = 0; w < L; ++w) sf[(size_t)k * L + w] = stress_sf_entry(s, h.stencils[k], w);
+    sa.permy = plans.d_idx + s.py.perm;
+    sa.permz = plans.d_idx + s.pz.perm;
+    sa.sf = sf.data();
+    sa.species = species.data();
+    double red[NSC];
+    for (int b = 0; b < nblk; ++b) {
+      if (h.prec == OFDFT_FP32) stress_block<float>(s, sa, b, nblk, 0, 1, red, &part[(size_t)NSC * b]);
+      else stress_block<double>(s, sa, b, nblk, 0, 1, red, &part[(size_t)NSC * b]);
+    }
+#else
+    const size_t sf_bytes = sizeof(cx<double>) * (size_t)nion * L;
+    const size_t part_bytes = sizeof(double) * part.size();
+    char* scratch = nullptr;
+    if ((rc = dmalloc((void**)&scratch, sf_bytes + part_bytes + sizeof(int) * (size_t)nion))) return rc;
+    cx<double>* dsf = (cx<double>*)scratch;
+    double* dpart = (double*)(scratch + sf_bytes);
+    int* dspec = (int*)(scratch + sf_bytes + part_bytes);
+    rc = h2d(dspec, species.data(), sizeof(int) * (size_t)nion);
+    if (!rc) {
+      sa.permy = plans.d_idx + s.py.perm;
+      sa.permz = plans.d_idx + s.pz.perm;
+      sa.sf = dsf;
+      sa.species = dspec;
+      k_stress_sf<<<nion, 128, 0, stream>>>(d_slots + i, h.d_stencil, dsf);
+      if (h.prec == OFDFT_FP32) k_stress<float><<<nblk, 128, 0, stream>>>(d_slots + i, sa, dpart);
+      else k_stress<double><<<nblk, 128, 0, stream>>>(d_slots + i, sa, dpart);
+      rc = cuda_check(cudaGetLastError(), "stress launch");
+    }
+    if (!rc) rc = d2h(part.data(), dpart, part_bytes);
+    dfree(scratch);
+    if (rc) return rc;
+#endif
+    double acc[NSC] = {0};
+    for (int b = 0; b < nblk; ++b)
+      for (int k = 0; k < NSC; ++k) acc[k] += part[(size_t)NSC * b + k];
+    if ((rc = put_ctl(i, saved))) return rc;
+    // assembly (CalculateStress): six components per term, then the diagonal terms
+    const double vol = s.vol;
+    double T6[7][6] = {{0}};
+    for (int k = 0; k < 6; ++k) {
+      T6[1][k] = -s.mu * acc[SC_VW + k];
+      const double wtc = PI_D * PI_D / (s.alpha * s.beta * sa.kf * std::pow(h.rho0, s.alpha + s.beta - 2.0));
+      T6[2][k] = wtc * acc[SC_WT + k];
+      T6[3][k] = 8.0 * PI_D * acc[SC_H + k];
+      T6[5][k] = -2.0 * (double)s.N * acc[SC_IE + k] / vol;
+    }
+    double sxc = 0.0;
+    if ((rc = rho_vxc(i, ib, &sxc))) return rc;
+    const int diag[3] = {0, 3, 5};
+    const double wtc = PI_D * PI_D / (s.alpha * s.beta * sa.kf * std::pow(h.rho0, s.alpha + s.beta - 2.0));
+    for (int d : diag) {
+      T6[0][d] += -2.0 / 3.0 * et[6] / vol;
+      T6[2][d] += -wtc * acc[SC_WTTR] / 3.0 - 2.0 / 3.0 * et[8] / vol;
+      T6[3][d] += -et[3] / vol;
+      T6[4][d] += et[4] / vol - sxc;
+      T6[5][d] += -et[2] / vol;
+    }
+    if (include_ewald && (rc = ewald_stress(i, T6[6]))) return rc;
+    const int ab[9] = {0, 1, 2, 1, 3, 4, 2, 4, 5};
+    for (int k = 0; k < 9; ++k) {
+      out[k] = 0.0;
+      for (int t = 0; t < 7; ++t) out[k] += T6[t][ab[k]];
+    }
+    if (terms)
+      for (int t = 0; t < 7; ++t)
+        for (int k = 0; k < 9; ++k) terms[9 * t + k] = T6[t][ab[k]];
+    return OFDFT_OK;
+  }
+
+  // <rho v_xc> over the grid (the mean of rho times the LDA potential) of the
+  // density held in buffer b.
+  int rho_vxc(int i, int b, double* out) {
+    HostSlot& h = slots[i];
+    const SlotDev& s = h.sd;
+    const int nblk = (int)std::max<long long>(1, std::min<long long>(2 * (long long)num_sms, (s.N + 255) / 256));
+    std::vector<double> part(nblk);
+#if defined(OFDFT_EMU)
+    double red[1];
+    for (int k = 0; k < nblk; ++k) {
+      if (h.prec == OFDFT_FP32) rho_vxc_block<float>((const float*)s.buf[b], s.N, k, nblk, 0, 1, red, &part[k]);
+      else rho_vxc_block<double>((const double*)s.buf[b], s.N, k, nblk, 0, 1, red, &part[k]);
+    }
+#else
+    double* dp = nullptr;
+    int rc = dmalloc((void**)&dp, sizeof(double) * nblk);
+    if (rc) return rc;
+    if (h.prec == OFDFT_FP32) k_rho_vxc<float><<<nblk, 256, 0, stream>>>((const float*)s.buf[b], s.N, dp);
+    else k_rho_vxc<double><<<nblk, 256, 0, stream>>>((const double*)s.buf[b], s.N, dp);
+    rc = cuda_check(cudaGetLastError(), "rho vxc launch");
+    if (!rc) rc = d2h(part.data(), dp, sizeof(double) * nblk);
+    dfree(dp);
+    if (rc) return rc;
+#endif
+    double sum = 0.0;
+    for (int k = 0; k < nblk; ++k) sum += part[k];
+    *out = sum / (double)s.N;
+    return OFDFT_OK;
+  }
+
+  // Ewald stress (six upper components, Ha/bohr^3) of the slot's ions.
+  int ewald_stress(int i, double* out6) {
+    HostSlot& h = slots[i];
+    const int nion = h.nion;
+    const EwaldPar p = ewald_par(h.lattice, nion);
+    const int npl = ewald_planes(p);
+    std::vector<double> pos(3 * (size_t)nion);
+    for (int k = 0; k < nion; ++k)
+      for (int r = 0; r < 3; ++r)
+        pos[3 * k + r] = p.A[r][0] * h.frac[3 * k] + p.A[r][1] * h.frac[3 * k + 1] + p.A[r][2] * h.frac[3 * k + 2];
+    std::vector<double> real7(7 * (size_t)nion), plane7(7 * (size_t)npl);
+#if defined(OFDFT_EMU)
+    double red[7];
+    for (int k = 0; k < nion; ++k) ewald_real_stress_block(p, pos.data(), h.zion.data(), k, 0, 1, red, &real7[7 * k]);
+    for (int m = 0; m < npl; ++m)
+      ewald_plane_stress_block(p, h.frac.data(), h.zion.data(), m, 0, 1, red, &plane7[7 * m]);
+#else
+    const size_t nd = 3 * (size_t)nion * 2 + nion + 7 * (size_t)nion + 7 * (size_t)npl;
+    double* dbuf = nullptr;
+    int rc = dmalloc((void**)&dbuf, sizeof(double) * nd);
+    if (rc) return rc;
+    double *dpos = dbuf, *dfrac = dpos + 3 * nion, *dz = dfrac + 3 * nion, *dreal = dz + nion, *dplane = dreal + 7 * nion;
+    rc = h2d(dpos, pos.data(), sizeof(double) * 3 * nion);
+    if (!rc) rc = h2d(dfrac, h.frac.data(), sizeof(double) * 3 * nion);
+    if (!rc) rc = h2d(dz, h.zion.data(), sizeof(double) * nion);
+    if (!rc) {
+      k_ewald_real_stress<<<nion, 128, 0, stream>>>(p, dpos, dz, dreal);
+      k_ewald_plane_stress<<<npl, 128, 0, stream>>>(p, dfrac, dz, dplane);
+      rc = cuda_check(cudaGetLastError(), "Ewald stress launch");
+    }
+    if (!rc) rc = d2h(real7.data(), dreal, sizeof(double) * 7 * nion);
+    if (!rc) rc = d2h(plane7.data(), dplane, sizeof(double) * 7 * npl);
+    dfree(dbuf);
+    if (rc) return rc;
+#endif
+    double qsum = 0.0, e_rec = 0.0, s6[6] = {0};
+    for (int k = 0; k < nion; ++k) {
+      qsum += h.zion[k];
+      for (int c = 0; c < 6; ++c) s6[c] += real7[7 * k + 1 + c];
+    }
+    double r6[6] = {0};
+    for (int m = 0; m < npl; ++m) {
+      e_rec += plane7[7 * m];
+      for (int c = 0; c < 6; ++c) r6[c] += plane7[7 * m + 1 + c];
+    }
+    const double e_bg = -0.5 * PI_D / (p.eta * p.eta) / p.vol * qsum * qsum;
+    for (int c = 0; c < 6; ++c) {
+      double v = s6[c] + r6[c];
+      if (c == 0 || c == 3 || c == 5) v -= e_rec + e_bg;
+      out6[c] = v / p.vol;
     }
     return OFDFT_OK;
   }
@@ -1906,6 +2129,12 @@ int ofdft_slot_build_ion_potential(ofdft_engine* e, int slot, int nion, const do
 int ofdft_slot_forces(ofdft_engine* e, int slot, const double* rho, int include_ewald, double* forces) {
   if (!e || !forces) return fail(OFDFT_EINVAL, "null argument");
   return e->eng.forces(slot, rho, include_ewald, forces);
+}
+
+int ofdft_slot_stress(ofdft_engine* e, int slot, const double* rho, int include_ewald, double* stress,
+                      double* terms) {
+  if (!e || !stress) return fail(OFDFT_EINVAL, "null argument");
+  return e->eng.stress(slot, rho, include_ewald, stress, terms);
 }
 
 int ofdft_ewald(const double* lattice, int nion, const double* frac, const double* charges, double* energy,

@@ -125,6 +125,7 @@ HDNI inline void ntn_after(Ctl& c, const SlotDev& s, const double* red, int kid,
         return;
       case EV_ION:
       case EV_FORCE:
+      case EV_STRESS:
         c.num_evals--;
         ctl_finish(c, ST_DONE, ERR_NONE);
         return;

@@ -427,7 +427,7 @@ HD EvalIn<T> eval_in(const SlotDev& s, const Ctl& c) {
   e.B = (const T*)s.buf[c.evb];
   e.ca = (T)c.ca;
   e.cb = (T)c.cb;
-  e.rho_mode = (c.ev == EV_RHO || (c.ev == EV_FORCE && c.force_rho)) ? 1 : 0;
+  e.rho_mode = (c.ev == EV_RHO || c.ev == EV_STRESS || (c.ev == EV_FORCE && c.force_rho)) ? 1 : 0;
   return e;
 }
 
@@ -678,6 +678,7 @@ HD void ypass_block(const Args<T>& a, int bid, int tid, int nthr, char* smem, in
   const int f = t.a, kx = t.b, z0 = tile_first(t.c), nz = tile_width(t.c);
   if (c.ev == EV_ION && f >= (dir < 0 ? s.ion.nspec : 1)) return;
   if (c.ev == EV_FORCE && f >= (dir < 0 ? 1 : s.ion.nspec)) return;
+  if (c.ev == EV_STRESS && dir > 0) return;  // forward spectra only
   const int n2 = s.n2, P = odd_pitch(n2);
   cx<T>* buf = (cx<T>*)smem;
   cx<T>* __restrict__ sp =
@@ -728,6 +729,14 @@ HD void zpass_block(const Args<T>& a, int bid, int tid, int nthr, char* smem) {
   }
   BLOCK_SYNC();
   fft_inplace<T, -1>(buf, NB, 1, NB, s.pz, a.tw, tid, nthr);
+  if (ev == EV_STRESS) {  // keep the forward spectra
+    for (int w = tid; w < NB * n3; w += nthr) {
+      const int i = magic_div32(w, mNB), qb = w - i * NB;
+      const int q = magic_div32(qb, mnb), b = qb - q * nb;
+      spec[(size_t)q * Nc + i * n2 + b] = buf[w];
+    }
+    return;
+  }
   zpass_operator<T, KS>(s, kind, gn, setup_mode, buf, NB, nb, kx, y0, a.idx + s.py.perm, a.idx + s.pz.perm, tid,
                         nthr);
   BLOCK_SYNC();
@@ -785,7 +794,7 @@ HD void yzpass_block(const Args<T>& a, int bid, int tid, int nthr, char* smem) {
   const SlotDev& s = a.slots[t.slot];
   const Ctl& c = a.ctl[t.slot];
   const int ev = c.ev;
-  if (c.status != ST_RUNNING || ev == EV_NONE || ev == EV_ION || ev == EV_FORCE) return;
+  if (c.status != ST_RUNNING || ev == EV_NONE || ev == EV_ION || ev == EV_FORCE || ev == EV_STRESS) return;
   const int g = t.a, kx = t.b;
   const int n2 = s.n2, n3 = s.n3, nrows = n2 * n3, P = odd_pitch(n2);
   const int kind = s.group_kind[g];
@@ -1024,6 +1033,13 @@ HD void xinv_block(const Args<T>& a, int bid, int tid, int nthr, char* smem) {
   const long long Nc = s.Nc;
   const cx<T>* __restrict__ spec = (const cx<T>*)s.spec;
   cx<T>* buf = (cx<T>*)smem;
+  if (ev == EV_STRESS) {  // the spectra stay; no sums
+    double zero[NCH];
+#pragma unroll
+    for (int ch = 0; ch < NCH; ++ch) zero[ch] = 0.0;
+    store_partials<0, 0>(s, ordinal, zero, (double*)(buf + NB * n1), tid, nthr);
+    return;
+  }
   const int nyq = (n1 % 2) == 0 ? n1 / 2 : -1;
   // gather: consecutive threads read the consecutive row pairs of one kx
   // (kx-major spectra); the packed complex sequence Z = A + i B of the two

@@ -35,7 +35,10 @@ constexpr int MAX_FIELDS = 8;
 constexpr int MAX_GROUPS = 4;
 
 // ---------------------------------------------------------------- modes
-enum EvalMode : int { EV_NONE = 0, EV_RHO = 1, EV_PHI = 2, EV_CG = 3, EV_LS = 4, EV_ION = 5, EV_FORCE = 6 };
+// EV_STRESS: the forward spectra of the density's fields only (x, y and z
+// forward transforms of rho, rho^beta, sqrt(rho), rho^alpha), left in the
+// slot's spectra for the stress reduction; no inverse transforms.
+enum EvalMode : int { EV_NONE = 0, EV_RHO = 1, EV_PHI = 2, EV_CG = 3, EV_LS = 4, EV_ION = 5, EV_FORCE = 6, EV_STRESS = 7 };
 enum VecOp : int {
   OP_NONE = 0,
   OP_SQRT_INIT = 1,  // phi = sqrt|rho|; sum rho

@@ -95,6 +95,7 @@ SIGNATURES = {
     "ofdft_slot_history": [_vp, ctypes.c_int, ctypes.c_int, _dp, _dp, _dp, _ip, _ip, _ip],
     "ofdft_slot_download": [_vp, ctypes.c_int, ctypes.c_int, _dp],
     "ofdft_slot_forces": [_vp, ctypes.c_int, _dp, ctypes.c_int, _dp],
+    "ofdft_slot_stress": [_vp, ctypes.c_int, _dp, ctypes.c_int, _dp, _dp],
     "ofdft_slot_set_input": [_vp, ctypes.c_int, _dp],
     "ofdft_slot_footprint": [ctypes.POINTER(CellDesc), ctypes.POINTER(ctypes.c_ulonglong)],
     "ofdft_engine_stream": [_vp, ctypes.POINTER(_vp)],
@@ -276,6 +277,21 @@ class Engine:
         r = _fortran(rho, self.shapes[slot]) if rho is not None else None
         self._check(self.lib.ofdft_slot_forces(self.h, slot, _ptr(r) if r is not None else None,
                                                int(bool(include_ewald)), _ptr(out)))
+        return out
+
+    STRESS_TERMS = ("TF", "vW", "WT", "Hartree", "LDA", "ion-electron", "Ewald")
+
+    def stress(self, slot, rho=None, include_ewald=True, terms=False):
+        """Stress tensor (3, 3) in Ha/bohr^3 of rho (or the slot's solved
+        density); with terms, also a dict of its seven parts."""
+        out = np.zeros((3, 3))
+        parts = np.zeros((7, 3, 3)) if terms else None
+        r = _fortran(rho, self.shapes[slot]) if rho is not None else None
+        self._check(self.lib.ofdft_slot_stress(self.h, slot, _ptr(r) if r is not None else None,
+                                               int(bool(include_ewald)), _ptr(out),
+                                               _ptr(parts) if terms else None))
+        if terms:
+            return out, dict(zip(self.STRESS_TERMS, parts))
         return out
 
     def ewald(self, slot, nion, want_forces=True):

@@ -154,6 +154,22 @@ int ofdft_slot_stress(ofdft_engine* e, int slot, const double* rho, int include_
                       double* terms);
 
 /* ---------------------------------------------------------------- host set-up helpers */
+/* The More-Thuente line search of the solver (Dcsrch / Dcstep,
+ * Source/MathDCsrch.f, Source/MathDCstep.f) in reverse communication, for host
+ * optimisers (GradientOptimization, Source/IonOptCON.f90:33-241): the record
+ * holds Dcsrch's isave/dsave; set ftol, gtol, xtol, stpmin and stpmax, call
+ * with task OFDFT_LS_START, then with OFDFT_LS_FG at each requested point
+ * while it returns OFDFT_LS_FG.  Returns the new task (CONV, WARN and ERROR
+ * end the search; stp then stays the last step), or -OFDFT_EINVAL for a null
+ * argument or another task. */
+typedef struct {
+  double ftol, gtol, xtol, stpmin, stpmax;
+  int brackt, stage;
+  double ginit, gtest, gx, gy, finit, fx, fy, stx, sty, stmin, stmax, width, width1;
+} ofdft_line_search;
+enum { OFDFT_LS_START = 0, OFDFT_LS_FG = 1, OFDFT_LS_CONV = 2, OFDFT_LS_WARN = 3, OFDFT_LS_ERROR = 4 };
+int ofdft_dcsrch(ofdft_line_search* ls, double* stp, double f, double g, int task);
+
 /* Ewald ion-ion energy (Ha) and forces (may be NULL) of point charges
  * (EwaldEnergy / EwaldForces, Source/Ewald.f90:465-1193,1196+).  lattice as in
  * ofdft_cell_desc; frac[3*nion]; charges[nion]. */

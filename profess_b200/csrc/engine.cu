@@ -2137,6 +2137,18 @@ int ofdft_slot_stress(ofdft_engine* e, int slot, const double* rho, int include_
   return e->eng.stress(slot, rho, include_ewald, stress, terms);
 }
 
+static_assert(sizeof(ofdft_line_search) == sizeof(LineSearch), "line-search record layout");
+
+int ofdft_dcsrch(ofdft_line_search* ls, double* stp, double f, double g, int task) {
+  if (!ls || !stp) return -fail(OFDFT_EINVAL, "null argument");
+  if (task < OFDFT_LS_START || task > OFDFT_LS_FG) return -fail(OFDFT_EINVAL, "task must be START or FG");
+  LineSearch L;
+  memcpy(&L, ls, sizeof(L));
+  const int out = ls_step(L, *stp, f, g, task);
+  memcpy(ls, &L, sizeof(L));
+  return out;
+}
+
 int ofdft_ewald(const double* lattice, int nion, const double* frac, const double* charges, double* energy,
                 double* forces) {
   if (!lattice || !frac || !charges || !energy || nion < 1) return fail(OFDFT_EINVAL, "bad argument");

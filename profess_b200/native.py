@@ -102,6 +102,7 @@ SIGNATURES = {
     "ofdft_engine_counters": [_vp, ctypes.POINTER(ctypes.c_longlong), ctypes.POINTER(ctypes.c_longlong)],
     "ofdft_engine_time_eval": [_vp, ctypes.c_int, _dp],
     "ofdft_ewald": [_dp, ctypes.c_int, _dp, _dp, _dp, _dp],
+    "ofdft_dcsrch": [_vp, _dp, ctypes.c_double, ctypes.c_double, ctypes.c_int],
     "ofdft_grid_size": [ctypes.c_double, _dp, _ip],
     "ofdft_wgc_radial_tables": [ctypes.c_double, ctypes.c_double, ctypes.c_double, ctypes.c_int, _dp, _dp, _dp,
                                 _dp, _ip],
@@ -121,6 +122,34 @@ def ewald(lib, lattice, frac, charges, want_forces=False):
     if rc:
         raise OfdftError(rc, lib.ofdft_last_error().decode())
     return float(e[0]), f
+
+
+class LineSearchRecord(ctypes.Structure):
+    """ofdft_line_search: Dcsrch's saved state."""
+    _fields_ = [(n, ctypes.c_double) for n in ("ftol", "gtol", "xtol", "stpmin", "stpmax")] + \
+               [("brackt", ctypes.c_int), ("stage", ctypes.c_int)] + \
+               [(n, ctypes.c_double) for n in ("ginit", "gtest", "gx", "gy", "finit", "fx", "fy", "stx", "sty",
+                                               "stmin", "stmax", "width", "width1")]
+
+
+LS_START, LS_FG, LS_CONV, LS_WARN, LS_ERROR = range(5)
+
+
+class Dcsrch:
+    """The library's More-Thuente search (ofdft_dcsrch) for host optimisers:
+    step(stp, f, g, task) -> (stp, task), task LS_START first, then LS_FG while
+    it asks for a point."""
+
+    def __init__(self, lib, ftol, gtol, xtol, stpmin, stpmax):
+        self.lib = lib
+        self.rec = LineSearchRecord(ftol=ftol, gtol=gtol, xtol=xtol, stpmin=stpmin, stpmax=stpmax)
+
+    def step(self, stp, f, g, task):
+        s = ctypes.c_double(stp)
+        out = self.lib.ofdft_dcsrch(ctypes.byref(self.rec), ctypes.byref(s), float(f), float(g), int(task))
+        if out < 0:
+            raise OfdftError(-out, self.lib.ofdft_last_error().decode())
+        return s.value, out
 
 
 def slot_footprint(lib, n, kinetic, alpha, beta, precision) -> int:

@@ -1,7 +1,10 @@
-"""QuickMin geometry relaxation of many independent cells on one engine.
+"""Geometry relaxation of many independent cells on one engine: the
+reference's ion optimisers (dispatched at Source/Optimizer.f90:247-260)
+QuickMin (method 2), the old conjugate gradient (3, GradientCG), CG2 (4) and
+BFGS (5).
 
-This is the reference's QuickMin ion optimiser, QuickMinOptimization
-(Source/IonOptQui.f90:33-368), run for a batch of cells in lockstep: every
+QuickMinOptimization (Source/IonOptQui.f90:33-368) runs a batch of cells in
+lockstep: every
 batched step, each cell that is still relaxing takes its own QuickMin move, its ion
 terms are refreshed on the device (B-spline ion potential, Ewald sum), and
 the densities of all moved cells are re-solved together, warm-started from
@@ -677,3 +680,74 @@ class BFGS(_GeneratorRelax):
     def _moves(self, st, force_cutoff, max_steps, nn_dist):
         return lbfgs_moves(st.cell.lattice, st.cell.frac, float(st.energy[0]), st.forces,
                            force_cutoff=force_cutoff, max_calls=max_steps)
+
+
+# ---------------------------------------------------------------- old CG
+# GradientOptimization (Source/IonOptCON.f90:33-241, ion method 3): Polak-
+# Ribiere-type directions (gamma clipped at 0) with the solver's More-Thuente
+# search (Dcsrch with ftol 0.01, gtol 0.1, xtol 1e-10, steps in [1e-100, 1000]);
+# the first step is 5, later first trials scale the last step by the ratio of
+# directional derivatives within [1/4, 2]; a search whose energy changed by
+# less than 1e-9 Ha per ion over its last 5 trials (after more than 10) is
+# cut and the next direction restarts along the forces.
+GRAD_FTOL, GRAD_GTOL, GRAD_XTOL = 0.01, 0.1, 1.0e-10
+GRAD_STPMIN, GRAD_STPMAX = 1.0e-100, 1000.0
+
+
+def gradient_moves(lib, lattice, frac, energy, forces, force_cutoff=FORCE_CUTOFF, max_steps=200):
+    """GradientOptimization as a generator (like cg2_moves); ``lib`` supplies
+    the line search.  The reference loops until the force test passes;
+    max_steps bounds the outer steps."""
+    cart2frac = np.linalg.inv(lattice)
+    frac = np.array(frac, dtype=float)
+    forces = np.asarray(forces, dtype=float)
+    energy = float(energy)
+    nion = len(frac)
+    max_force = _max_force(forces)
+    stp, fp = 0.0, 0.0
+    g = dir_next = None
+    checkpt1 = checkpt2 = 0.0
+    step = 1
+    while max_force >= force_cutoff and step <= max_steps:
+        if step == 1:
+            dir_next = forces.copy()
+            fp = float(np.sum(-forces * dir_next))
+            stp = 5.0
+        else:
+            gamma = max(float(np.sum(forces * (forces - g))) / float(np.sum(g * g)), 0.0)
+            dir_next = forces + gamma * dir_next
+            fp_last = fp
+            fp = float(np.sum(-forces * dir_next))
+            stp = max(min(stp * fp_last / fp, stp * 2.0), stp * 0.25)
+        g = forces.copy()
+        orig = frac.copy()
+        n_line = 0
+        ls = native.Dcsrch(lib, GRAD_FTOL, GRAD_GTOL, GRAD_XTOL, GRAD_STPMIN, GRAD_STPMAX)
+        task = native.LS_START
+        while True:
+            stp, task = ls.step(stp, energy, float(np.sum(-forces * dir_next)), task)
+            if task != native.LS_FG:
+                break
+            if n_line % 5 == 4:
+                checkpt2, checkpt1 = checkpt1, energy
+                if n_line > 10 and abs(checkpt2 - checkpt1) / nion < 1e-9:
+                    stp = 1.0
+                    g = forces.copy()  # the next gamma is 0
+                    break
+            frac = np.mod(orig + (stp * dir_next) @ cart2frac.T, 1.0)
+            energy, forces = yield frac
+            energy = float(energy)
+            forces = np.asarray(forces, dtype=float)
+            max_force = _max_force(forces)
+            n_line += 1
+        step += 1
+    return frac
+
+
+class GradientCG(_GeneratorRelax):
+    """The old conjugate-gradient optimiser (GradientOptimization,
+    Source/IonOptCON.f90:33-241) on batched density solves."""
+
+    def _moves(self, st, force_cutoff, max_steps, nn_dist):
+        return gradient_moves(self.eng.lib, st.cell.lattice, st.cell.frac, float(st.energy[0]), st.forces,
+                              force_cutoff=force_cutoff, max_steps=max_steps)

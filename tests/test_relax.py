@@ -181,3 +181,56 @@ def check_bfgs_matches_oracle(eng):
 
 def test_bfgs_matches_oracle(emu_engine):
     check_bfgs_matches_oracle(emu_engine)
+
+
+def test_library_line_search_matches_oracle(emu_engine):
+    """ofdft_dcsrch (the solver's Dcsrch) takes the same trial steps and ends
+    with the same task as the oracle's Dcsrch on 1D functions."""
+    from oracle.linesearch import Dcsrch
+    codes = {"FG": native.LS_FG, "CONV": native.LS_CONV, "WARN": native.LS_WARN, "ERRO": native.LS_ERROR}
+    funcs = [lambda a: ((a - 0.7) ** 2 - 0.3 * a, 2 * (a - 0.7) - 0.3),
+             lambda a: (np.cos(3 * a) + 0.1 * a * a, -3 * np.sin(3 * a) + 0.2 * a),
+             lambda a: (-np.exp(-a) * a, np.exp(-a) * (a - 1.0))]
+    for fun in funcs:
+        for stp0 in (0.05, 1.0, 5.0):
+            for tols in ((1e-4, 0.9, 1e-10), (0.01, 0.1, 1e-10)):
+                a = native.Dcsrch(emu_engine.lib, *tols, 1e-100, 1000.0)
+                b = Dcsrch(*tols, 1e-100, 1000.0)
+                sa = sb = stp0
+                f, g = fun(0.0)
+                ta, tb = native.LS_START, "START"
+                for _ in range(40):
+                    sa, ta = a.step(sa, f, g, ta)
+                    sb, tb = b.step(sb, f, g, tb)
+                    assert ta == codes[tb[:4]] and sa == sb, (ta, tb, sa, sb)
+                    if ta != native.LS_FG:
+                        break
+                    f, g = fun(sa)
+
+
+def check_gradient_cg_matches_oracle(eng):
+    """GradientOptimization on the engine against the oracle from the
+    displaced Al4 cell: the same energy after every density solve."""
+    import cases
+    from oracle import ioncg
+    cell, f, _, _ = cases.golden_case("wt_al4_displaced")
+    from profess_b200 import recpot
+    z = np.load(cases.GOLDEN + "/al_hc_recpot.npz")
+    sp = recpot.species_from_table(float(z["max_g"]), z["values"], "Al")
+    c = wl.Cell(name="displaced", lattice=cell.lattice, frac=cell.frac, species_of_ion=cell.species_of_ion,
+                species=[sp], grid=tuple(f.n))
+    run = relax.GradientCG(eng, [c], max_steps=12)
+    try:
+        run.run()
+        frac, trace, forces = ioncg.gradient_optimization(cell, f.n, ntn.NtnOptions(), max_steps=12)
+        assert len(run.traces[0]) == len(trace)
+        assert np.abs(np.array(run.traces[0]) - trace).max() < 1e-9
+        assert trace[-1] < trace[0] - 1e-2
+        d = run.states[0].cell.frac - frac
+        assert np.abs(d - np.rint(d)).max() < 2e-7
+    finally:
+        run.close()
+
+
+def test_gradient_cg_matches_oracle(emu_engine):
+    check_gradient_cg_matches_oracle(emu_engine)

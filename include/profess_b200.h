@@ -141,6 +141,17 @@ int ofdft_slot_build_ion_potential(ofdft_engine* e, int slot, int nion, const do
  * when include_ewald, the ion-ion Ewald forces (ForcesII_IE,
  * Source/CalForce.f90:134-239).  Needs ofdft_slot_build_ion_potential first. */
 int ofdft_slot_forces(ofdft_engine* e, int slot, const double* rho, int include_ewald, double* forces);
+/* A new lattice (layout as in ofdft_cell_desc) for the slot, same grid:
+ * RefreshLattice (Source/CellInfo.f90) with the kernel reference densities of
+ * KEDFRefresh (Source/SetupKEDF.f90:620-680).  RefreshCellSetup
+ * (Source/RefreshCell.f90:27-76) then continues with
+ * ofdft_slot_build_wt_kernel (or _wgc_kernel), ofdft_slot_build_ion_potential
+ * and ofdft_slot_ewald. */
+int ofdft_slot_set_lattice(ofdft_engine* e, int slot, const double* lattice, double rho0, double rho_s);
+/* RescaleDensity (Source/RefreshIons.f90:33-122) of the held input density
+ * (ofdft_slot_hold_density): scaled on the device to num_electrons electrons
+ * with the slot's current dV, e.g. after a change of lattice. */
+int ofdft_slot_rescale_input(ofdft_engine* e, int slot, double num_electrons);
 /* Stress tensor (Ha/bohr^3, stress[9] row-major and symmetric) of the slot's
  * current density (rho = NULL: phi^2 of the last solve) or of the given rho,
  * for the WT functional: CalculateStress (Source/CalStress.f90:44-253) with

@@ -159,3 +159,120 @@ def run_nvt(cell: cs.Cell, n, vel0: np.ndarray, dt: float, nsteps: int, opts: nt
         h = 0.5 * st["k2"] + energy + 0.5 * st["v"] ** 2 * q_mass + g * temperature_ha * st["x"]
         out.append((cell.frac.copy(), vel.copy(), energy, h))
     return out
+
+
+def run_npt(cell: cs.Cell, n, vel0: np.ndarray, dt: float, nsteps: int, opts: ntn.NtnOptions, q_mass: float,
+            b_mass: float, temperature_ha: float, ext_pres: float, n_resn: int = 3, n_yosh: int = 3,
+            alpha: float = 5.0 / 6.0, beta: float = 5.0 / 6.0):
+    """Full-cell NPT, NPTFullCell / MVV / NPTFullCell_Integrator / NPTFullCell_Conserved
+    (Source/MolecularDynamicsNPT.f90:76-274, 275-411, 413-640, 691-790), no box
+    constraint and no frozen ions.  Velocities are held (3, numIon) as in the
+    reference.  Returns the list of (lattice, frac, energy, conserved, volume)
+    after the first solve and after each step."""
+    from . import stress as ost
+    cell = dataclasses.replace(cell, frac=np.array(cell.frac, dtype=float), lattice=np.array(cell.lattice, float))
+    mass = np.array([atomic_mass(cell.species[s].name) for s in cell.species_of_ion])
+    nion = len(mass)
+    freedom = 3.0 * nion
+    d = 3.0
+    w = _yoshida(n_yosh)
+    vel = np.array(vel0, dtype=float).T.copy()            # (3, numIon)
+    cart = np.array([cell.lattice @ cell.frac[i] for i in range(nion)]).T   # cartNoWrap (3, numIon)
+    com = (cart * mass[None, :]).sum(axis=1) / mass.sum()  # AdjustCenterOfMass(.TRUE.)
+    cart = cart - com[:, None]
+    inv = np.linalg.inv(cell.lattice)
+    cell.frac = np.array([np.mod(inv @ cart[:, i], 1.0) for i in range(nion)])
+    xlogs = vlogs = 0.0
+    vbox = np.zeros((3, 3))
+
+    def refresh_and_solve(rho):
+        f = functional_for(cell, n, alpha, beta)
+        r = ntn.NtnSolver(f, opts).solve(rho)
+        forces, _, _ = ofo.total_forces(cell, r.rho)
+        return r.rho, float(r.energy[0]), forces, ost.stress(cell, f, r.rho)
+
+    rho, energy, forces, stress = refresh_and_solve(cs.uniform_density(cell, *n))
+
+    def atom_ke():
+        return sum(0.5 * mass[i] * float(vel[:, i] @ vel[:, i]) for i in range(nion))
+
+    def atom_ke_tensor():
+        t = np.zeros((3, 3))
+        for a in range(3):
+            for b in range(3):
+                t[a, b] = sum(0.5 * mass[i] * vel[a, i] * vel[b, i] for i in range(nion))
+        return t
+
+    def box_ke():
+        return 0.5 * b_mass * float((vbox ** 2).sum())
+
+    def diag_exp(m, scale):
+        eig, v = np.linalg.eigh(m, UPLO="U")
+        return v @ np.diag(np.exp(scale * eig)) @ v.T
+
+    def integrator():
+        nonlocal vlogs, xlogs, vbox, vel
+        ke, ket = atom_ke(), atom_ke_tensor()
+        glogs = (2.0 * ke + 2.0 * box_ke() - (freedom + 3.0 ** 2) * temperature_ha) / q_mass
+        pint = -stress
+        gbox = (2.0 * ket + cell.vol * pint) / b_mass
+        gbox = gbox + np.eye(3) * (2.0 * ke / freedom - cell.vol * ext_pres) / b_mass
+        for _ in range(n_resn):
+            for wi in w:
+                wdt2 = wi * dt / (2.0 * n_resn)
+                wdt4 = wi * dt / (4.0 * n_resn)
+                wdt8 = wi * dt / (8.0 * n_resn)
+                vlogs = vlogs + glogs * wdt4
+                aa = np.exp(-wdt8 * vlogs)
+                vbox = vbox * aa * aa + wdt4 * gbox * aa
+                trvg = (vbox[0, 0] + vbox[1, 1] + vbox[2, 2]) / freedom
+                vt = vbox.copy()
+                for k in range(3):
+                    vt[k, k] += trvg + vlogs
+                vt = diag_exp(vt, -wdt2)
+                for i in range(nion):
+                    vel[:, i] = vt @ vel[:, i]
+                xlogs = xlogs + vlogs * wdt2
+                ke, ket = atom_ke(), atom_ke_tensor()
+                gbox = (2.0 * ket + cell.vol * pint) / b_mass
+                gbox = gbox + np.eye(3) * (2.0 * ke / freedom - cell.vol * ext_pres) / b_mass
+                aa = np.exp(-wdt8 * vlogs)
+                vbox = vbox * aa * aa + wdt4 * gbox * aa
+                glogs = (2.0 * ke + 2.0 * box_ke() - (freedom + 3.0 ** 2) * temperature_ha) / q_mass
+                vlogs = vlogs + glogs * wdt4
+
+    def conserved():
+        return (atom_ke() + energy + ext_pres * cell.vol + box_ke() + 0.5 * vlogs ** 2 * q_mass +
+                (freedom + d ** 2) * temperature_ha * xlogs)
+
+    out = [(cell.lattice.copy(), cell.frac.copy(), energy, conserved(), cell.vol)]
+    for _ in range(nsteps):
+        integrator()
+        dt2 = dt / 2.0
+        for i in range(nion):
+            vel[:, i] = vel[:, i] + dt2 * forces[i, :] / mass[i]
+        eig, v = np.linalg.eigh(vbox, UPLO="U")
+        ie = np.diag(np.exp(dt * eig))
+        arg2 = (eig * dt2) ** 2
+        poly = 1.0 + arg2 / 6.0 + arg2 ** 2 / 120.0 + arg2 ** 3 / 5040.0 + arg2 ** 4 / 362880.0
+        is_ = np.diag(np.exp(dt2 * eig) * poly)
+        vt1 = v @ (ie @ v.T)
+        vt2 = v @ (is_ @ v.T)
+        for i in range(nion):
+            cart[:, i] = vt1 @ cart[:, i] + dt * (vt2 @ vel[:, i])
+        lat = vt1 @ cell.lattice
+        sym = lat.copy()
+        for a in range(3):
+            for b in range(3):
+                if a != b:
+                    sym[a, b] = (lat[a, b] + lat[b, a]) / 2.0
+        cell.lattice = sym
+        inv = np.linalg.inv(cell.lattice)
+        cell.frac = np.array([np.mod(inv @ cart[:, i], 1.0) for i in range(nion)])
+        rho = rho * (cell.num_electrons / (rho.sum() * cell.vol / rho.size))   # RescaleDensity
+        rho, energy, forces, stress = refresh_and_solve(rho)
+        for i in range(nion):
+            vel[:, i] = vel[:, i] + dt2 * forces[i, :] / mass[i]
+        integrator()
+        out.append((cell.lattice.copy(), cell.frac.copy(), energy, conserved(), cell.vol))
+    return out

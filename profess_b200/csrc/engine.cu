@@ -522,6 +522,54 @@ struct Engine {
 
   int upload_slot(int i) { return h2d(d_slots + i, &slots[i].sd, sizeof(SlotDev)); }
 
+  // Lattice-dependent fields of a slot: cellRecip = TRANSPOSE(Inverse(cellReal))
+  // * 2 pi (CellInfo.f90:281), volume, dV, and the inverse for the forces.
+  static int set_geometry(HostSlot& h, const double* L) {  // L[3*i + k] = component k of vector i
+    SlotDev& s = h.sd;
+    auto A = [&](int r, int c) { return L[3 * c + r]; };
+    const double det = A(0, 0) * (A(1, 1) * A(2, 2) - A(1, 2) * A(2, 1)) -
+                       A(0, 1) * (A(1, 0) * A(2, 2) - A(1, 2) * A(2, 0)) +
+                       A(0, 2) * (A(1, 0) * A(2, 1) - A(1, 1) * A(2, 0));
+    if (!(std::fabs(det) > 0)) return fail(OFDFT_EINVAL, "singular lattice");
+    double inv[3][3];
+    inv[0][0] = (A(1, 1) * A(2, 2) - A(1, 2) * A(2, 1)) / det;
+    inv[0][1] = (A(0, 2) * A(2, 1) - A(0, 1) * A(2, 2)) / det;
+    inv[0][2] = (A(0, 1) * A(1, 2) - A(0, 2) * A(1, 1)) / det;
+    inv[1][0] = (A(1, 2) * A(2, 0) - A(1, 0) * A(2, 2)) / det;
+    inv[1][1] = (A(0, 0) * A(2, 2) - A(0, 2) * A(2, 0)) / det;
+    inv[1][2] = (A(0, 2) * A(1, 0) - A(0, 0) * A(1, 2)) / det;
+    inv[2][0] = (A(1, 0) * A(2, 1) - A(1, 1) * A(2, 0)) / det;
+    inv[2][1] = (A(0, 1) * A(2, 0) - A(0, 0) * A(2, 1)) / det;
+    inv[2][2] = (A(0, 0) * A(1, 1) - A(0, 1) * A(1, 0)) / det;
+    const double twopi = 2.0 * 3.141592653589793238462643;
+    // recip matrix R = inv^T * 2pi; column c (vector b_c) component r = R(r,c) = inv[c][r] * 2pi
+    for (int c = 0; c < 3; ++c)
+      for (int r = 0; r < 3; ++r) s.recip[3 * c + r] = inv[c][r] * twopi;
+    s.vol = std::fabs(det);
+    s.dv = s.vol / (double)s.N;
+    for (int k = 0; k < 9; ++k) h.lattice[k] = L[k];
+    for (int r = 0; r < 3; ++r)
+      for (int c2 = 0; c2 < 3; ++c2) h.cell_inv_t[3 * r + c2] = inv[c2][r];
+    return OFDFT_OK;
+  }
+
+  // A new lattice for slot i (RefreshLattice, Source/CellInfo.f90, with the
+  // reference densities of KEDFRefresh, Source/SetupKEDF.f90:620-680): the
+  // kernel, ion potential and Ewald energy must be rebuilt after it.
+  int set_lattice(int i, const double* L, double rho0, double rho_s) {
+    int rc = check_slot(i);
+    if (rc) return rc;
+    HostSlot& h = slots[i];
+    HostSlot saved = h;
+    if ((rc = set_geometry(h, L))) {
+      h = saved;
+      return rc;
+    }
+    h.rho0 = rho0;
+    h.sd.rho_s = rho_s;
+    return upload_slot(i);
+  }
+
   int create_slot(const ofdft_cell_desc* d, int* out) {
     if (!d) return fail(OFDFT_EINVAL, "null descriptor");
     const int ns[3] = {d->n1, d->n2, d->n3};
@@ -548,32 +596,10 @@ struct Engine {
     s.px = plans.plans[pi][d->n1];
     s.py = plans.plans[pi][d->n2];
     s.pz = plans.plans[pi][d->n3];
-    // cellRecip = TRANSPOSE(Inverse(cellReal)) * 2 pi  (CellInfo.f90:281)
-    const double* L = d->lattice;  // L[3*i + k] = component k of vector i
-    auto A = [&](int r, int c) { return L[3 * c + r]; };
-    const double det = A(0, 0) * (A(1, 1) * A(2, 2) - A(1, 2) * A(2, 1)) -
-                       A(0, 1) * (A(1, 0) * A(2, 2) - A(1, 2) * A(2, 0)) +
-                       A(0, 2) * (A(1, 0) * A(2, 1) - A(1, 1) * A(2, 0));
-    if (!(std::fabs(det) > 0)) return fail(OFDFT_EINVAL, "singular lattice");
-    double inv[3][3];
-    inv[0][0] = (A(1, 1) * A(2, 2) - A(1, 2) * A(2, 1)) / det;
-    inv[0][1] = (A(0, 2) * A(2, 1) - A(0, 1) * A(2, 2)) / det;
-    inv[0][2] = (A(0, 1) * A(1, 2) - A(0, 2) * A(1, 1)) / det;
-    inv[1][0] = (A(1, 2) * A(2, 0) - A(1, 0) * A(2, 2)) / det;
-    inv[1][1] = (A(0, 0) * A(2, 2) - A(0, 2) * A(2, 0)) / det;
-    inv[1][2] = (A(0, 2) * A(1, 0) - A(0, 0) * A(1, 2)) / det;
-    inv[2][0] = (A(1, 0) * A(2, 1) - A(1, 1) * A(2, 0)) / det;
-    inv[2][1] = (A(0, 1) * A(2, 0) - A(0, 0) * A(2, 1)) / det;
-    inv[2][2] = (A(0, 0) * A(1, 1) - A(0, 1) * A(1, 0)) / det;
-    const double twopi = 2.0 * 3.141592653589793238462643;
-    // recip matrix R = inv^T * 2pi; column c (vector b_c) component r = R(r,c) = inv[c][r] * 2pi
-    for (int c = 0; c < 3; ++c)
-      for (int r = 0; r < 3; ++r) s.recip[3 * c + r] = inv[c][r] * twopi;
-    s.vol = std::fabs(det);
-    s.dv = s.vol / (double)s.N;
-    for (int k = 0; k < 9; ++k) h.lattice[k] = L[k];
-    for (int r = 0; r < 3; ++r)
-      for (int c2 = 0; c2 < 3; ++c2) h.cell_inv_t[3 * r + c2] = inv[c2][r];
+    if (int rc = set_geometry(h, d->lattice)) {
+      h.used = false;
+      return rc;
+    }
     h.rho0 = d->rho0;
     h.gamma = d->gamma;
     s.inv_n = 1.0 / (double)s.N;
@@ -1033,6 +1059,51 @@ struct Engine {
       for (int t = 0; t < 7; ++t)
         for (int k = 0; k < 9; ++k) terms[9 * t + k] = T6[t][ab[k]];
     return OFDFT_OK;
+  }
+
+  // RescaleDensity (Source/RefreshIons.f90:33-122) of the held input density:
+  // scaled to num_electrons with the slot's current dV.
+  int rescale_input(int i, double num_electrons) {
+    int rc = check_slot(i);
+    if (rc) return rc;
+    HostSlot& h = slots[i];
+    const SlotDev& s = h.sd;
+    if (!h.input) return fail(OFDFT_EINVAL, "no held input density to rescale");
+    const int nblk = (int)std::max<long long>(1, std::min<long long>(2 * (long long)num_sms, (s.N + 255) / 256));
+    std::vector<double> part(nblk);
+#if defined(OFDFT_EMU)
+    double red[1];
+    for (int k = 0; k < nblk; ++k) {
+      if (h.prec == OFDFT_FP32) sum_block<float>((const float*)h.input, s.N, k, nblk, 0, 1, red, &part[k]);
+      else sum_block<double>((const double*)h.input, s.N, k, nblk, 0, 1, red, &part[k]);
+    }
+#else
+    double* dp = nullptr;
+    if ((rc = dmalloc((void**)&dp, sizeof(double) * nblk))) return rc;
+    if (h.prec == OFDFT_FP32) k_sum<float><<<nblk, 256, 0, stream>>>((const float*)h.input, s.N, dp);
+    else k_sum<double><<<nblk, 256, 0, stream>>>((const double*)h.input, s.N, dp);
+    rc = cuda_check(cudaGetLastError(), "sum launch");
+    if (!rc) rc = d2h(part.data(), dp, sizeof(double) * nblk);
+    dfree(dp);
+    if (rc) return rc;
+#endif
+    double sum = 0.0;
+    for (int k = 0; k < nblk; ++k) sum += part[k];
+    sum *= s.dv;
+    if (!(sum > 0)) return fail(OFDFT_EINVAL, "held density has no electrons");
+    const double f = num_electrons / sum;
+#if defined(OFDFT_EMU)
+    for (long long k = 0; k < s.N; ++k) {
+      if (h.prec == OFDFT_FP32) ((float*)h.input)[k] = (float)((double)((float*)h.input)[k] * f);
+      else ((double*)h.input)[k] *= f;
+    }
+    return OFDFT_OK;
+#else
+    if (h.prec == OFDFT_FP32) k_scale<float><<<io_blocks(s.N), 256, 0, stream>>>((float*)h.input, s.N, f);
+    else k_scale<double><<<io_blocks(s.N), 256, 0, stream>>>((double*)h.input, s.N, f);
+    if ((rc = cuda_check(cudaGetLastError(), "scale launch"))) return rc;
+    return sync_stream();
+#endif
   }
 
   // <rho v_xc> over the grid (the mean of rho times the LDA potential) of the
@@ -2129,6 +2200,16 @@ int ofdft_slot_build_ion_potential(ofdft_engine* e, int slot, int nion, const do
 int ofdft_slot_forces(ofdft_engine* e, int slot, const double* rho, int include_ewald, double* forces) {
   if (!e || !forces) return fail(OFDFT_EINVAL, "null argument");
   return e->eng.forces(slot, rho, include_ewald, forces);
+}
+
+int ofdft_slot_set_lattice(ofdft_engine* e, int slot, const double* lattice, double rho0, double rho_s) {
+  if (!e || !lattice) return fail(OFDFT_EINVAL, "null argument");
+  return e->eng.set_lattice(slot, lattice, rho0, rho_s);
+}
+
+int ofdft_slot_rescale_input(ofdft_engine* e, int slot, double num_electrons) {
+  if (!e) return fail(OFDFT_EINVAL, "null engine");
+  return e->eng.rescale_input(slot, num_electrons);
 }
 
 int ofdft_slot_stress(ofdft_engine* e, int slot, const double* rho, int include_ewald, double* stress,

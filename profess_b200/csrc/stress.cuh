@@ -239,6 +239,15 @@ HD void rho_vxc_block(const T* rho, long long n, int b, int nblk, int tid, int n
   block_sum<1>(red, &acc, tid, nthr, out);
 }
 
+// Sum of v over block b of nblk (strided like rho_vxc_block); thread 0 writes out[0].
+template <typename T>
+HD void sum_block(const T* v, long long n, int b, int nblk, int tid, int nthr, double* red, double* out) {
+  double acc = 0.0;
+  const long long stride = (long long)nblk * nthr;
+  for (long long k = (long long)b * nthr + tid; k < n; k += stride) acc += (double)v[k];
+  block_sum<1>(red, &acc, tid, nthr, out);
+}
+
 // ---------------------------------------------------------------- Ewald stress
 // out7 = (0, the six components of sum 0.5 z_i z_j f'(r)/r d_a d_b) over the
 // images and partners of ion i, f(r) = erfc(eta r)/r.
@@ -313,6 +322,16 @@ template <typename T>
 __global__ void __launch_bounds__(256) k_rho_vxc(const T* rho, long long n, double* out) {
   __shared__ double red[256];
   rho_vxc_block<T>(rho, n, blockIdx.x, gridDim.x, threadIdx.x, blockDim.x, red, out + blockIdx.x);
+}
+template <typename T>
+__global__ void __launch_bounds__(256) k_sum(const T* v, long long n, double* out) {
+  __shared__ double red[256];
+  sum_block<T>(v, n, blockIdx.x, gridDim.x, threadIdx.x, blockDim.x, red, out + blockIdx.x);
+}
+template <typename T>
+__global__ void __launch_bounds__(256) k_scale(T* v, long long n, double f) {
+  for (long long k = (long long)blockIdx.x * blockDim.x + threadIdx.x; k < n; k += (long long)gridDim.x * blockDim.x)
+    v[k] = (T)((double)v[k] * f);
 }
 __global__ void __launch_bounds__(128) k_ewald_real_stress(EwaldPar p, const double* pos, const double* z,
                                                            double* out7) {

@@ -1,5 +1,5 @@
-"""NVE and Nose-Hoover NVT molecular dynamics of many independent cells
-(replicas) on one engine.
+"""NVE, Nose-Hoover NVT and full-cell NPT molecular dynamics of many
+independent cells (replicas) on one engine.
 
 This is the reference's velocity-Verlet NVE driver, RunNVE
 (Source/MolecularDynamicsNVE.f90:33-323), run for a batch of replicas in
@@ -256,3 +256,154 @@ class NVT(NVE):
             self._thermostat(r)
             r.history.append({"energy": float(r.energy[0]), "conserved": self.conserved_nh(r),
                               "temperature": r.temperature(), "num_evals": r.stats["num_evals"]})
+
+
+# ---------------------------------------------------------------------------- NPT
+def box_constraint(m: np.ndarray, constr_type: int) -> np.ndarray:
+    """BoxConstraint (Source/MolecularDynamicsNPT.f90:878-935) on a 3x3 box
+    force or velocity: -1 none, 1 orthogonal box, 3/4/5 x/y/z fixed and
+    orthogonal."""
+    m = np.array(m, dtype=float)
+    if constr_type < 0:
+        return m
+    if constr_type == 1:
+        return np.diag(np.diag(m))
+    if constr_type in (3, 4, 5):
+        m = np.diag(np.diag(m))
+        m[constr_type - 3, constr_type - 3] = 0.0
+        return m
+    raise ValueError("box constraint type %d is not implemented" % constr_type)
+
+
+def _sym_exp(m: np.ndarray, scale: float) -> np.ndarray:
+    """V diag(exp(scale * eig)) V^T of a symmetric 3x3 matrix (Diag, DSPEV on
+    the upper triangle, Source/MathFunctions.f90:762-811)."""
+    eig, v = np.linalg.eigh(m, UPLO="U")
+    return v @ np.diag(np.exp(scale * eig)) @ v.T
+
+
+class NPT(NVE):
+    """Lockstep full-cell NPT dynamics (NPTFullCell, Source/MolecularDynamicsNPT.f90:76-274):
+    the Martyna-Tobias-Klein integrator with a Nose-Hoover thermostat
+    (``q_mass``) and a barostat (``b_mass``) at external pressure ``ext_pres``
+    (Ha/bohr^3).  Each step: NPTFullCell_Integrator over a half step, MVV
+    (a half kick, the positions and the lattice propagated by the barostat
+    velocity, RefreshCellSetup on the device: new lattice, WT kernel, ion
+    potential and Ewald sum; RescaleDensity of the held density; the density
+    solves of all replicas together; forces, stress and a half kick), and the
+    integrator again.  The stress is the device stress of each new density.
+    WT functional only."""
+
+    def __init__(self, eng, cells, dt: float, q_mass: float, b_mass: float, temperature_k: float,
+                 ext_pres: float, velocities=None, seed: int = 0, opts=None, rho0=None, n_resn: int = 3,
+                 n_yosh: int = 3, constr_type: int = -1):
+        self.q_mass, self.b_mass = float(q_mass), float(b_mass)
+        self.t_ha = float(temperature_k) * BOLTZMANN
+        self.ext_pres = float(ext_pres)
+        self.n_resn = int(n_resn)
+        self.w = yoshida_coefficients(int(n_yosh))
+        self.constr = int(constr_type)
+        shifted, carts = [], []
+        for c in cells:  # AdjustCenterOfMass(.TRUE.) before the set-up
+            c = dataclasses.replace(c, frac=np.array(c.frac, dtype=float), lattice=np.array(c.lattice, float))
+            m = masses_of(c)
+            cart = c.frac @ c.lattice.T
+            cart -= (m[:, None] * cart).sum(axis=0) / m.sum()
+            c.frac = np.mod(cart @ np.linalg.inv(c.lattice).T, 1.0)
+            shifted.append(c)
+            carts.append(cart)
+        super().__init__(eng, shifted, dt, velocities=velocities, temperature_k=temperature_k, seed=seed,
+                         opts=opts, rho0=rho0)
+        for r, cart in zip(self.reps, carts):
+            r.cart = cart  # unwrapped (cartNoWrap)
+            r.xlogs, r.vlogs = 0.0, 0.0
+            r.vboxg = box_constraint(np.zeros((3, 3)), self.constr)
+            r.stress = self.eng.stress(r.slot)
+            r.freedom = 3.0 * r.cell.nion
+
+    # ------------------------------------------------------------ pieces
+    def _ke(self, r):
+        return 0.5 * float((r.mass[:, None] * r.vel * r.vel).sum())
+
+    def _ke_tensor(self, r):
+        return 0.5 * (r.mass[:, None] * r.vel).T @ r.vel
+
+    def _box_ke(self, r):
+        return 0.5 * self.b_mass * float((r.vboxg ** 2).sum())
+
+    def _g_box(self, r, ke, ket, pint):
+        g = (2.0 * ket + r.cell.vol * pint) / self.b_mass
+        g += np.eye(3) * (2.0 * ke / r.freedom - r.cell.vol * self.ext_pres) / self.b_mass
+        return box_constraint(g, self.constr)
+
+    def _integrator(self, r):
+        """NPTFullCell_Integrator (MolecularDynamicsNPT.f90:413-640)."""
+        T, Q, f = self.t_ha, self.q_mass, r.freedom
+        ke, ket, boxke = self._ke(r), self._ke_tensor(r), self._box_ke(r)
+        glogs = (2.0 * ke + 2.0 * boxke - (f + 9.0) * T) / Q
+        pint = -r.stress
+        gbox = self._g_box(r, ke, ket, pint)
+        for _ in range(self.n_resn):
+            for w in self.w:
+                wdt2 = w * self.dt / (2.0 * self.n_resn)
+                wdt4 = w * self.dt / (4.0 * self.n_resn)
+                wdt8 = w * self.dt / (8.0 * self.n_resn)
+                r.vlogs += glogs * wdt4
+                aa = np.exp(-wdt8 * r.vlogs)
+                r.vboxg = r.vboxg * aa * aa + wdt4 * gbox * aa
+                vt = r.vboxg + np.eye(3) * (np.trace(r.vboxg) / f + r.vlogs)
+                r.vel = r.vel @ _sym_exp(vt, -wdt2).T
+                r.xlogs += r.vlogs * wdt2
+                ke, ket = self._ke(r), self._ke_tensor(r)
+                gbox = self._g_box(r, ke, ket, pint)
+                aa = np.exp(-wdt8 * r.vlogs)
+                r.vboxg = r.vboxg * aa * aa + wdt4 * gbox * aa
+                boxke = self._box_ke(r)
+                glogs = (2.0 * ke + 2.0 * boxke - (f + 9.0) * T) / Q
+                r.vlogs += glogs * wdt4
+
+    def conserved_npt(self, r) -> float:
+        """NPTFullCell_Conserved (MolecularDynamicsNPT.f90:691-790)."""
+        return (self._ke(r) + float(r.energy[0]) + self.ext_pres * r.cell.vol + self._box_ke(r) +
+                0.5 * r.vlogs ** 2 * self.q_mass + (r.freedom + 9.0) * self.t_ha * r.xlogs)
+
+    def step(self):
+        """One NPT step of every replica (MolecularDynamicsNPT.f90:226-265)."""
+        dt, dt2 = self.dt, 0.5 * self.dt
+        for r in self.reps:
+            self._integrator(r)
+            # MVV (MolecularDynamicsNPT.f90:275-411)
+            r.vel += dt2 * r.forces / r.mass[:, None]
+            eig, v = np.linalg.eigh(r.vboxg, UPLO="U")
+            arg2 = (eig * dt2) ** 2
+            poly = 1.0 + arg2 / 6.0 + arg2 ** 2 / 120.0 + arg2 ** 3 / 5040.0 + arg2 ** 4 / 362880.0
+            vt1 = v @ np.diag(np.exp(dt * eig)) @ v.T
+            vt2 = v @ np.diag(np.exp(dt2 * eig) * poly) @ v.T
+            r.cart = r.cart @ vt1.T + dt * r.vel @ vt2.T
+            lat = vt1 @ r.cell.lattice
+            lat = _symmetrize(lat)
+            c = r.cell
+            c.lattice = lat
+            c.frac = np.mod(r.cart @ np.linalg.inv(lat).T, 1.0)
+            # RefreshCellSetup and RescaleDensity on the device, then the solve
+            self.eng.hold_density(r.slot)
+            rho_avg = c.num_electrons / c.vol
+            self.eng.set_lattice(r.slot, lat, rho_avg, rho_avg)
+            self.eng.rescale_input(r.slot, c.num_electrons)
+            self.eng.build_wt_kernel(r.slot)
+            self.eng.build_ion_potential(r.slot, c.frac, c.species_of_ion, c.species)
+            self._refresh_ewald(r)
+            self.eng.start_solve(r.slot, None, self.opts)
+        self._finish_solves()
+        for r in self.reps:
+            r.stress = self.eng.stress(r.slot)
+            r.vel += dt2 * r.forces / r.mass[:, None]
+            self._integrator(r)
+            r.history.append({"energy": float(r.energy[0]), "conserved": self.conserved_npt(r),
+                              "volume": r.cell.vol, "temperature": r.temperature(),
+                              "num_evals": r.stats["num_evals"]})
+
+
+def _symmetrize(a: np.ndarray) -> np.ndarray:
+    """Symmetrize (Source/MathFunctions.f90:813-850): off-diagonal pairs averaged."""
+    return 0.5 * (a + a.T)

@@ -96,6 +96,8 @@ SIGNATURES = {
     "ofdft_slot_download": [_vp, ctypes.c_int, ctypes.c_int, _dp],
     "ofdft_slot_forces": [_vp, ctypes.c_int, _dp, ctypes.c_int, _dp],
     "ofdft_slot_stress": [_vp, ctypes.c_int, _dp, ctypes.c_int, _dp, _dp],
+    "ofdft_slot_set_lattice": [_vp, ctypes.c_int, _dp, ctypes.c_double, ctypes.c_double],
+    "ofdft_slot_rescale_input": [_vp, ctypes.c_int, ctypes.c_double],
     "ofdft_slot_set_input": [_vp, ctypes.c_int, _dp],
     "ofdft_slot_footprint": [ctypes.POINTER(CellDesc), ctypes.POINTER(ctypes.c_ulonglong)],
     "ofdft_engine_stream": [_vp, ctypes.POINTER(_vp)],
@@ -307,6 +309,16 @@ class Engine:
         self._check(self.lib.ofdft_slot_forces(self.h, slot, _ptr(r) if r is not None else None,
                                                int(bool(include_ewald)), _ptr(out)))
         return out
+
+    def set_lattice(self, slot, lattice, rho0, rho_s=None):
+        """New lattice (3x3, columns are the lattice vectors, bohr) for the slot."""
+        lat = np.ascontiguousarray(np.asarray(lattice, float).ravel(order="F"))
+        self._check(self.lib.ofdft_slot_set_lattice(self.h, slot, _ptr(lat), float(rho0),
+                                                    float(rho0 if rho_s is None else rho_s)))
+
+    def rescale_input(self, slot, num_electrons):
+        """RescaleDensity of the held input density to num_electrons."""
+        self._check(self.lib.ofdft_slot_rescale_input(self.h, slot, float(num_electrons)))
 
     STRESS_TERMS = ("TF", "vW", "WT", "Hartree", "LDA", "ion-electron", "Ewald")
 

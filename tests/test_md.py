@@ -111,3 +111,41 @@ def check_nvt_matches_oracle(eng):
 def test_yoshida_weights_sum_to_one():
     for n in (1, 3, 5):
         assert abs(md.yoshida_coefficients(n).sum() - 1.0) < 1e-15
+
+
+NPT_Q, NPT_B, NPT_P = 2.0e3, 2.0e5, 1.0e-5
+
+
+def check_npt_matches_oracle(eng, nsteps=3):
+    """Full-cell NPT (NPTFullCell) on the engine, with the device stress and
+    the device lattice refresh, against the oracle's restatement: the same
+    lattice, positions, energy and conserved quantity after every step."""
+    c, ocell = _cells()
+    v0 = md.initial_velocities(c, 600.0, seed=4)
+    opts = native.ntn_options(conv_check=native.CONV_POT, pot_tol=1.0e-6)
+    run = md.NPT(eng, [c], DT, NPT_Q, NPT_B, 600.0, NPT_P, velocities=[v0], opts=opts)
+    try:
+        run.run(nsteps)
+        rep = run.reps[0]
+        ref = omd.run_npt(ocell, c.grid, v0, DT, nsteps, ntn.NtnOptions(conv_check="POT", pot_tol=1.0e-6),
+                          NPT_Q, NPT_B, 600.0 * md.BOLTZMANN, NPT_P)
+        lat, frac, energy, cons, vol = ref[-1]
+        assert np.abs(rep.cell.lattice - lat).max() < 1e-11
+        assert np.abs(_wrap(rep.cell.frac - frac)).max() < 1e-10
+        assert abs(float(rep.energy[0]) - energy) < 1e-8
+        for h, r in zip(rep.history, ref[1:]):
+            assert abs(h["conserved"] - r[3]) < 1e-8 and abs(h["volume"] - r[4]) < 1e-9
+        assert abs(ref[-1][4] - ref[0][4]) > 1e-3  # the cell did move
+    finally:
+        run.close()
+
+
+def test_npt_matches_oracle(emu_engine):
+    check_npt_matches_oracle(emu_engine)
+
+
+def test_box_constraint():
+    m = np.arange(9.0).reshape(3, 3) + 1.0
+    assert np.array_equal(md.box_constraint(m, -1), m)
+    assert np.array_equal(md.box_constraint(m, 1), np.diag(np.diag(m)))
+    assert np.array_equal(md.box_constraint(m, 4), np.diag([1.0, 0.0, 9.0]))

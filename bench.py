@@ -424,6 +424,19 @@ def run_ours(args):
         eng.set_input(b, r)
         s32.append(a)
         s64.append(b)
+    # autotuning (the engine's planning step): one slot of each kind of cell,
+    # outside the timed regions; the shapes apply to every slot of that kind
+    tuning = []
+    if not args.no_tune:
+        seen = set()
+        for c, a, b in zip(cells, s32, s64):
+            for s, prec in ((a, "fp32"), (b, "fp64")):
+                key = (tuple(c.grid), prec, c.kinetic)
+                if key in seen:
+                    continue
+                seen.add(key)
+                t = eng.tune(s, iters=5)
+                tuning.append(dict(t, grid=list(c.grid), precision=prec))
     o32 = native.ntn_options(conv_check=native.CONV_POT, pot_tol=args.fp32_tol, max_iter=300, stall_line=6)
     oref = native.ntn_options(conv_check=native.CONV_POT, pot_tol=1.0e-6, max_iter=args.refine, stall_line=6)
     # The plain FP64 path runs the same solver rules in FP64 throughout, the
@@ -598,6 +611,7 @@ def run_ours(args):
         "e2e": {"value": ws * B * args.steps / t_e2e, "unit": UNIT, "h2d_bytes_per_step": h2d,
                 "d2h_bytes_per_step": d2h},
         "roofline": roofline,
+        "tuning": tuning,
         "cpu_baseline": cpu,
         "serving": serving_line,
         "clocks": clk,
@@ -828,6 +842,7 @@ def main():
     ap.add_argument("--refine", type=int, default=3)
     ap.add_argument("--no-cpu-baseline", action="store_true",
                     help="skip the oracle solve (CPU baseline and errors against the oracle)")
+    ap.add_argument("--no-tune", action="store_true", help="keep the default launch shapes (no autotuning)")
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference(args)

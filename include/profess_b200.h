@@ -141,6 +141,25 @@ int ofdft_slot_build_ion_potential(ofdft_engine* e, int slot, int nion, const do
  * when include_ewald, the ion-ion Ewald forces (ForcesII_IE,
  * Source/CalForce.f90:134-239).  Needs ofdft_slot_build_ion_potential first. */
 int ofdft_slot_forces(ofdft_engine* e, int slot, const double* rho, int include_ewald, double* forces);
+/* Autotuner, the planning step of the engine (the reference plans its FFTs
+ * with FFTW, PlanFFT in Source/Fourier_v1.f90:103-190): times one evaluation
+ * of the slot's resident input density (ofdft_slot_set_input) per candidate
+ * launch shape - the radix cap of the x-axis FFT plan, row pairs per
+ * x-forward and x-inverse task, and the block size of the fused y-z pass -
+ * and keeps the fastest.  The choice is cached in the engine for the slot's
+ * grid, precision and functional and applied to every such slot, also to
+ * those created later.  ms_default / ms_tuned: the median evaluation time
+ * before and after; shape[4] (may be NULL): radix cap, x-forward and
+ * x-inverse row pairs, y-z threads (0: split y/z path).  No slot may be
+ * running; the slot's solve record is overwritten. */
+int ofdft_engine_tune(ofdft_engine* e, int slot, int iters, double* ms_default, double* ms_tuned, int* shape);
+/* Pin the slot's launch shape (the four values ofdft_engine_tune reports, e.g.
+ * a shape tuned in an earlier run; radix cap 0 and y-z threads 0 mean the
+ * defaults).  OFDFT_EINVAL for a cap without a plan or tasks whose shared
+ * memory would not fit. */
+int ofdft_slot_set_shape(ofdft_engine* e, int slot, const int* shape);
+/* The slot's current launch shape, as ofdft_engine_tune reports it. */
+int ofdft_slot_shape(ofdft_engine* e, int slot, int* shape);
 /* A new lattice (layout as in ofdft_cell_desc) for the slot, same grid:
  * RefreshLattice (Source/CellInfo.f90) with the kernel reference densities of
  * KEDFRefresh (Source/SetupKEDF.f90:620-680).  RefreshCellSetup

@@ -137,8 +137,12 @@ static bool seven_smooth(int n) {
 
 constexpr int MAX_N = 512;
 
+// Radix caps the tuner may give an x-axis plan (the first is the default).
+static const int kCaps[2][3] = {{12, 8, 0}, {16, 12, 8}};  // [0] FP64, [1] FP32
+
 struct PlanTable {
-  std::map<int, FftPlan> plans[2];  // [0] FP64 (OFDFT_FP64), [1] FP32
+  std::map<int, FftPlan> plans[2];  // [0] FP64 (OFDFT_FP64), [1] FP32: default radix cap
+  std::map<int, FftPlan> capped[2];  // key cap * 1024 + n: the plans of the other caps
   void* d_tw64 = nullptr;           // exp(-2 pi i e / n), e < n, for every 7-smooth n <= MAX_N
   void* d_tw32 = nullptr;
   int* d_idx = nullptr;             // perm and iperm of every plan
@@ -159,18 +163,21 @@ struct PlanTable {
     for (int pi = 0; pi < 2; ++pi)
       for (int n = 1; n <= MAX_N; ++n) {
         if (!seven_smooth(n)) continue;
-        int rad[FFT_MAX_STAGES];
-        const int nst = fft_radices(n, pi == 0 ? FftMaxRadix<double>::value : FftMaxRadix<float>::value, rad);
-        FftPlan p;
-        memset(&p, 0, sizeof(p));
-        std::vector<int> perm(n), iperm(n);
-        fft_plan_fill(p, n, rad, nst, perm.data(), iperm.data());
-        p.root = root_off[n];
-        p.perm = (int)idx.size();
-        idx.insert(idx.end(), perm.begin(), perm.end());
-        p.iperm = (int)idx.size();
-        idx.insert(idx.end(), iperm.begin(), iperm.end());
-        plans[pi][n] = p;
+        for (int ci = 0; ci < 3 && kCaps[pi][ci]; ++ci) {
+          int rad[FFT_MAX_STAGES];
+          const int nst = fft_radices(n, kCaps[pi][ci], rad);
+          FftPlan p;
+          memset(&p, 0, sizeof(p));
+          std::vector<int> perm(n), iperm(n);
+          fft_plan_fill(p, n, rad, nst, perm.data(), iperm.data());
+          p.root = root_off[n];
+          p.perm = (int)idx.size();
+          idx.insert(idx.end(), perm.begin(), perm.end());
+          p.iperm = (int)idx.size();
+          idx.insert(idx.end(), iperm.begin(), iperm.end());
+          if (ci == 0) plans[pi][n] = p;
+          else capped[pi][kCaps[pi][ci] * 1024 + n] = p;
+        }
       }
     const size_t nt = re.size();
     std::vector<cx<double>> t64(nt);
@@ -186,6 +193,11 @@ struct PlanTable {
     if (!rc) rc = h2d(d_tw32, t32.data(), nt * sizeof(cx<float>));
     if (!rc) rc = h2d(d_idx, idx.data(), idx.size() * sizeof(int));
     return rc;
+  }
+  // The plan of length n with radix cap cap (0 or the default cap: the default plan).
+  const FftPlan& get(int pi, int n, int cap) const {
+    auto it = capped[pi].find(cap * 1024 + n);
+    return it == capped[pi].end() ? plans[pi].at(n) : it->second;
   }
   void release() {
     dfree(d_tw64);
@@ -328,6 +340,8 @@ struct HostSlot {
   std::vector<std::pair<void*, size_t>> allocs;  // device blocks and their sizes
   int nrowpairs = 0, rp1 = 1;
   int ty = 1, tz = 1;           // z columns per y-pass task and y columns per z-pass task (split path)
+  int xcap = 0;                 // radix cap of the x-axis plan (0: the default)
+  int yzt = 0;                  // threads of the fused y-z pass (0: by plane size)
   bool setup_pass = false;      // running an ion-potential or force pass (split path)
   int nplanes = 0;
   int nion = 0;                 // ions of the last ion-potential build
@@ -642,9 +656,11 @@ struct Engine {
     if ((rc = alloc(h, &s.vion, es * s.N))) { free_slot(idx); return rc; }
     if ((rc = alloc(h, &s.kern, es * s.Nc * h.nplanes))) { free_slot(idx); return rc; }
     if ((rc = alloc(h, &s.spec, 2 * es * s.Nc * s.nf))) { free_slot(idx); return rc; }
-    const int ntmax = std::max(s.ntask[K_VEC], s.ntask[K_X5]);
+    const int ntmax = std::max(s.ntask[K_VEC], h.nrowpairs);  // any x-inverse task size the tuner picks
     if ((rc = alloc(h, (void**)&s.partials, sizeof(double) * NCH * ntmax))) { free_slot(idx); return rc; }
     if ((rc = alloc(h, (void**)&s.hist, sizeof(HistEntry) * HIST_MAX))) { free_slot(idx); return rc; }
+    auto tuned = tune_cache.find(tune_key(h));
+    if (tuned != tune_cache.end()) set_shape(h, tuned->second);
     if ((rc = upload_slot(idx))) { free_slot(idx); return rc; }
     Ctl c;
     memset(&c, 0, sizeof(c));
@@ -1559,6 +1575,189 @@ struct Engine {
   // Back-to-back potential evaluations of every slot that has a resident
   // input density; returns the mean device time of one batched evaluation
   // (passes 1-5 and the controller kernel), timed with events on the engine stream.
+  // ---------------------------------------------------------- autotuning
+  // The launch shape a tuner may change, per slot: the radix cap of the x-axis
+  // FFT plan, row pairs per x-forward and per x-inverse task, and the block
+  // size of the fused y-z pass (256 or 512 threads; 0 = by plane size).  The
+  // y and z plans stay fixed: the kernel planes are stored in their order.
+  struct Shape {
+    int xcap, rp1, rp, yzt;
+  };
+  std::map<std::vector<long long>, Shape> tune_cache;  // by grid, precision and functional
+  static std::vector<long long> tune_key(const HostSlot& h) {
+    const SlotDev& s = h.sd;
+    return {s.n1, s.n2, s.n3, h.prec, s.kinetic, s.nf};
+  }
+  Shape shape_of(const HostSlot& h) const { return {h.xcap, h.rp1, h.sd.rp, h.yzt}; }
+  bool shape_ok(const HostSlot& h, const Shape& c) const {
+    const SlotDev& s = h.sd;
+    const size_t esz = elem_size(h.prec);
+    if (c.rp1 < 1 || c.rp1 > 32 || c.rp < 1 || c.rp > 32) return false;
+    if (xfwd_smem(s.n1, std::max(s.nf, MAX_SPECIES), c.rp1, esz) > 200 * 1024) return false;
+    if (xinv_smem(s.n1, std::max(s.nf, MAX_SPECIES), c.rp, esz) > 200 * 1024) return false;
+    if (c.yzt != 0 && c.yzt != 256 && c.yzt != 512) return false;
+    return true;
+  }
+  void set_shape(HostSlot& h, const Shape& c) {
+    SlotDev& s = h.sd;
+    const int pi = h.prec == OFDFT_FP32 ? 1 : 0;
+    h.xcap = c.xcap;
+    s.px = plans.get(pi, s.n1, c.xcap);
+    h.rp1 = c.rp1;
+    s.rp = c.rp;
+    s.ntask[K_X5] = (h.nrowpairs + s.rp - 1) / s.rp;
+    h.yzt = c.yzt;
+    dirty = true;
+  }
+
+  // Median time (ms) of `iters` one-tick evaluations of the slots ids, each
+  // from its resident input density.
+  int time_ids(const std::vector<int>& ids, int iters, double* ms_out) {
+    int rc;
+    auto start_all = [&]() -> int {
+      for (int i : ids) {
+        int r = start_eval(i, nullptr, 1, 1);
+        if (r) return r;
+      }
+      return OFDFT_OK;
+    };
+    if ((rc = start_all())) return rc;
+    int running = 0;
+    if ((rc = run(2, &running, 1))) return rc;  // warm-up and graph capture for one tick
+#if defined(OFDFT_EMU)
+    *ms_out = 0.0;
+    (void)iters;
+    return OFDFT_OK;
+#else
+    cudaEvent_t e0, e1;
+    cudaEventCreate(&e0);
+    cudaEventCreate(&e1);
+    std::vector<float> t;
+    for (int it = 0; it < iters; ++it) {
+      if ((rc = start_all())) break;
+      if (dirty && (rc = build_lists())) break;
+      if ((rc = capture(1))) break;
+      cudaEventRecord(e0, stream);
+      if ((rc = cuda_check(cudaGraphLaunch(graph_exec, stream), "graph launch"))) break;
+      cudaEventRecord(e1, stream);
+      if ((rc = sync_stream())) break;
+      float ms = 0.0f;
+      cudaEventElapsedTime(&ms, e0, e1);
+      t.push_back(ms);
+      n_ticks += 1;
+      n_launches += launches_per_tick();
+      for (int i : ids) slots[i].running = false;
+      dirty = true;
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    if (rc) return rc;
+    std::sort(t.begin(), t.end());
+    *ms_out = t.empty() ? 0.0 : (double)t[t.size() / 2];
+    return OFDFT_OK;
+#endif
+  }
+
+  // Tune slot i's launch shape by timing one evaluation of its resident input
+  // density per candidate (coordinate descent over the x radix cap, the
+  // x-forward and x-inverse task sizes and the y-z block size; a candidate must
+  // be 1 % faster to replace the incumbent).  The result is cached for the
+  // grid, precision and functional and applied to every slot of that kind,
+  // now and at creation.  The slot's solve record is overwritten.
+  int tune(int i, int iters, double* ms_default, double* ms_tuned, int* shape_out) {
+    int rc = check_slot(i);
+    if (rc) return rc;
+    HostSlot& h = slots[i];
+    if (!h.input) return fail(OFDFT_EINVAL, "tuning needs a resident input density (ofdft_slot_set_input)");
+    for (int k = 0; k < cap; ++k)
+      if (slots[k].used && slots[k].running) return fail(OFDFT_EBUSY, "tune while no slot is running");
+    iters = std::max(iters, 3);
+    const std::vector<int> ids{i};
+    Shape best = shape_of(h);
+    double tbest = 0.0;
+    if ((rc = time_ids(ids, iters, &tbest))) return rc;
+    *ms_default = tbest;
+    auto trial = [&](Shape c) -> int {
+      if (!shape_ok(h, c)) return OFDFT_OK;
+      const Shape keep = shape_of(h);
+      set_shape(h, c);
+      double t = 0.0;
+      int r = upload_slot(i);
+      if (!r) r = time_ids(ids, iters, &t);
+      if (r) {
+        set_shape(h, keep);
+        upload_slot(i);
+        return r;
+      }
+      if (t < 0.99 * tbest) {
+        tbest = t;
+        best = c;
+      }
+      set_shape(h, best);
+      return upload_slot(i);
+    };
+    const int pi = h.prec == OFDFT_FP32 ? 1 : 0;
+    const SlotDev& s = h.sd;
+    const size_t csz = 2 * elem_size(h.prec);
+    for (int ci = 1; ci < 3 && kCaps[pi][ci]; ++ci) {
+      Shape c = best;
+      c.xcap = kCaps[pi][ci];
+      if ((rc = trial(c))) return rc;
+    }
+    const int base1 = best.rp1, base5 = best.rp;
+    for (int r : {base1 / 2, (3 * base1) / 4, (3 * base1) / 2, 2 * base1}) {
+      Shape c = best;
+      c.rp1 = odd_columns(s.nf, std::max(1, r), csz);
+      if (c.rp1 != best.rp1 && (rc = trial(c))) return rc;
+    }
+    for (int r : {base5 / 2, (3 * base5) / 4, (3 * base5) / 2, 2 * base5}) {
+      Shape c = best;
+      c.rp = odd_columns(s.nf, std::max(1, r), csz);
+      if (c.rp != best.rp && (rc = trial(c))) return rc;
+    }
+    if (uses_yz(h))
+      for (int t : {256, 512}) {
+        Shape c = best;
+        c.yzt = t;
+        if ((rc = trial(c))) return rc;
+      }
+    *ms_tuned = tbest;
+    tune_cache[tune_key(h)] = best;
+    for (int k = 0; k < cap; ++k)
+      if (slots[k].used && tune_key(slots[k]) == tune_key(h)) {
+        set_shape(slots[k], best);
+        if ((rc = upload_slot(k))) return rc;
+      }
+    return shape_out ? get_shape(i, shape_out) : OFDFT_OK;
+  }
+
+  // Pin slot i's launch shape (cap, x-forward and x-inverse row pairs, y-z
+  // threads; 0 keeps the default for the cap and the y-z threads).
+  int pin_shape(int i, const int* v) {
+    int rc = check_slot(i);
+    if (rc) return rc;
+    HostSlot& h = slots[i];
+    const int pi = h.prec == OFDFT_FP32 ? 1 : 0;
+    bool cap_ok = v[0] == 0;
+    for (int ci = 0; ci < 3; ++ci) cap_ok = cap_ok || (kCaps[pi][ci] && v[0] == kCaps[pi][ci]);
+    const Shape c{v[0] == kCaps[pi][0] ? 0 : v[0], v[1], v[2], v[3]};
+    if (!cap_ok || !shape_ok(h, c)) return fail(OFDFT_EINVAL, "launch shape out of range");
+    set_shape(h, c);
+    return upload_slot(i);
+  }
+
+  int get_shape(int i, int* v) {
+    if (i < 0 || i >= cap || !slots[i].used) return fail(OFDFT_EINVAL, "invalid slot");
+    const HostSlot& h = slots[i];
+    const int pi = h.prec == OFDFT_FP32 ? 1 : 0;
+    const size_t csz = 2 * elem_size(h.prec);
+    v[0] = h.xcap ? h.xcap : kCaps[pi][0];
+    v[1] = h.rp1;
+    v[2] = h.sd.rp;
+    v[3] = uses_yz(h) ? (h.yzt ? h.yzt : (yz_smem(h.sd, csz) <= YZ_SMEM_SMALL ? 256 : 512)) : 0;
+    return OFDFT_OK;
+  }
+
   int time_eval(int iters, double* ms_out) {
     int rc;
     std::vector<int> ids;
@@ -1638,7 +1837,7 @@ struct Engine {
       L[px1].smem = std::max(L[px1].smem, xfwd_smem(s.n1, std::max(s.nf, s.ion.nspec), h.rp1, cs / 2));
       if (uses_yz(h)) {  // fused y-z pass: one task per (field, kx)
         const size_t sm = yz_smem(s, cs);
-        const int pyz = sm <= YZ_SMEM_SMALL ? P_YZ : P_YZB;
+        const int pyz = h.yzt == 256 ? P_YZ : h.yzt == 512 ? P_YZB : sm <= YZ_SMEM_SMALL ? P_YZ : P_YZB;
         for (int g = 0; g < s.ngroups; ++g)
           for (int kx = 0; kx < s.k1; ++kx) L[pyz].h.push_back({i, g, kx, 0});
         L[pyz].nthr = pyz == P_YZ ? 256 : 512;
@@ -2200,6 +2399,21 @@ int ofdft_slot_build_ion_potential(ofdft_engine* e, int slot, int nion, const do
 int ofdft_slot_forces(ofdft_engine* e, int slot, const double* rho, int include_ewald, double* forces) {
   if (!e || !forces) return fail(OFDFT_EINVAL, "null argument");
   return e->eng.forces(slot, rho, include_ewald, forces);
+}
+
+int ofdft_engine_tune(ofdft_engine* e, int slot, int iters, double* ms_default, double* ms_tuned, int* shape) {
+  if (!e || !ms_default || !ms_tuned) return fail(OFDFT_EINVAL, "null argument");
+  return e->eng.tune(slot, iters, ms_default, ms_tuned, shape);
+}
+
+int ofdft_slot_shape(ofdft_engine* e, int slot, int* shape) {
+  if (!e || !shape) return fail(OFDFT_EINVAL, "null argument");
+  return e->eng.get_shape(slot, shape);
+}
+
+int ofdft_slot_set_shape(ofdft_engine* e, int slot, const int* shape) {
+  if (!e || !shape) return fail(OFDFT_EINVAL, "null argument");
+  return e->eng.pin_shape(slot, shape);
 }
 
 int ofdft_slot_set_lattice(ofdft_engine* e, int slot, const double* lattice, double rho0, double rho_s) {

@@ -97,6 +97,9 @@ SIGNATURES = {
     "ofdft_slot_forces": [_vp, ctypes.c_int, _dp, ctypes.c_int, _dp],
     "ofdft_slot_stress": [_vp, ctypes.c_int, _dp, ctypes.c_int, _dp, _dp],
     "ofdft_slot_set_lattice": [_vp, ctypes.c_int, _dp, ctypes.c_double, ctypes.c_double],
+    "ofdft_engine_tune": [_vp, ctypes.c_int, ctypes.c_int, _dp, _dp, _ip],
+    "ofdft_slot_set_shape": [_vp, ctypes.c_int, _ip],
+    "ofdft_slot_shape": [_vp, ctypes.c_int, _ip],
     "ofdft_slot_rescale_input": [_vp, ctypes.c_int, ctypes.c_double],
     "ofdft_slot_set_input": [_vp, ctypes.c_int, _dp],
     "ofdft_slot_footprint": [ctypes.POINTER(CellDesc), ctypes.POINTER(ctypes.c_ulonglong)],
@@ -309,6 +312,32 @@ class Engine:
         self._check(self.lib.ofdft_slot_forces(self.h, slot, _ptr(r) if r is not None else None,
                                                int(bool(include_ewald)), _ptr(out)))
         return out
+
+    def tune(self, slot, iters=5):
+        """Autotune the launch shape of the slot's kind of cell (it needs a
+        resident input density, set_input).  Returns a dict with the median
+        evaluation time before and after (ms) and the chosen shape."""
+        t0, t1 = np.zeros(1), np.zeros(1)
+        shp = np.zeros(4, dtype=np.int32)
+        self._check(self.lib.ofdft_engine_tune(self.h, slot, int(iters), _ptr(t0), _ptr(t1),
+                                               shp.ctypes.data_as(_ip)))
+        return {"ms_default": float(t0[0]), "ms_tuned": float(t1[0]), "shape": self._shape_dict(shp)}
+
+    SHAPE_KEYS = ("x_radix_cap", "xfwd_row_pairs", "xinv_row_pairs", "yz_threads")
+
+    def _shape_dict(self, v):
+        return dict(zip(self.SHAPE_KEYS, (int(x) for x in v)))
+
+    def shape(self, slot):
+        """The slot's launch shape (as tune reports it)."""
+        shp = np.zeros(4, dtype=np.int32)
+        self._check(self.lib.ofdft_slot_shape(self.h, slot, shp.ctypes.data_as(_ip)))
+        return self._shape_dict(shp)
+
+    def set_shape(self, slot, x_radix_cap=0, xfwd_row_pairs=1, xinv_row_pairs=1, yz_threads=0):
+        """Pin the slot's launch shape (as tune reports it)."""
+        v = np.array([x_radix_cap, xfwd_row_pairs, xinv_row_pairs, yz_threads], dtype=np.int32)
+        self._check(self.lib.ofdft_slot_set_shape(self.h, slot, v.ctypes.data_as(_ip)))
 
     def set_lattice(self, slot, lattice, rho0, rho_s=None):
         """New lattice (3x3, columns are the lattice vectors, bohr) for the slot."""

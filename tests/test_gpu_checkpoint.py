@@ -29,11 +29,14 @@ def check_checkpoint(eng, tmp_path, c, prec):
         path = str(tmp_path / "mid.den")
         df.write_density(path, mid)
         back = df.read_density(path, c.grid, c.num_electrons, c.vol)
-        # the checkpoint holds the resident density to the last bit (up to the
-        # renormalisation to the cell's electron count on reading)
-        assert np.abs(back - mid).max() <= 1e-12 * np.abs(mid).max()
+        # the checkpoint holds the resident density to the last bit; reading
+        # renormalises it to the cell's electron count (a factor 1 + O(1e-15)
+        # for an FP64 slot, 1 + O(1e-8) for an FP32 one)
         raw = df.read_density_file(path)[..., 0]
         assert np.array_equal(raw, mid)
+        scale = c.num_electrons / (mid.sum() * c.vol / mid.size)
+        assert np.abs(back - mid * scale).max() <= 1e-14 * np.abs(mid).max()
+        assert abs(scale - 1.0) < (1e-12 if prec == native.FP64 else 1e-6)
         eng.hold_density(s)
         eng.start_solve(s, None, opts)
         while eng.run(8):

@@ -424,8 +424,9 @@ def run_ours(args):
         eng.set_input(b, r)
         s32.append(a)
         s64.append(b)
-    # autotuning (the engine's planning step): one slot of each kind of cell,
-    # outside the timed regions; the shapes apply to every slot of that kind
+    # autotuning (the engine's planning step), outside the timed regions: each
+    # kind of cell is tuned on the batch of its slots and the shape applies to
+    # every slot of that kind
     tuning = []
     if not args.no_tune:
         seen = set()

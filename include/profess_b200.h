@@ -142,16 +142,17 @@ int ofdft_slot_build_ion_potential(ofdft_engine* e, int slot, int nion, const do
  * Source/CalForce.f90:134-239).  Needs ofdft_slot_build_ion_potential first. */
 int ofdft_slot_forces(ofdft_engine* e, int slot, const double* rho, int include_ewald, double* forces);
 /* Autotuner, the planning step of the engine (the reference plans its FFTs
- * with FFTW, PlanFFT in Source/Fourier_v1.f90:103-190): times one evaluation
- * of the slot's resident input density (ofdft_slot_set_input) per candidate
- * launch shape - the radix cap of the x-axis FFT plan, row pairs per
- * x-forward and x-inverse task, and the block size of the fused y-z pass -
- * and keeps the fastest.  The choice is cached in the engine for the slot's
- * grid, precision and functional and applied to every such slot, also to
- * those created later.  ms_default / ms_tuned: the median evaluation time
+ * with FFTW, PlanFFT in Source/Fourier_v1.f90:103-190): for the slot's kind
+ * of cell (grid, precision, functional), times one batched evaluation of
+ * every idle slot of that kind holding a resident input density
+ * (ofdft_slot_set_input) per candidate launch shape - the radix cap of the
+ * x-axis FFT plan, row pairs per x-forward and x-inverse task, and the block
+ * size of the fused y-z pass - and keeps the fastest.  The choice is cached
+ * in the engine for that kind and applied to every such slot, also to those
+ * created later.  ms_default / ms_tuned: the median batched evaluation time
  * before and after; shape[4] (may be NULL): radix cap, x-forward and
  * x-inverse row pairs, y-z threads (0: split y/z path).  No slot may be
- * running; the slot's solve record is overwritten. */
+ * running; the timed slots' solve records are overwritten. */
 int ofdft_engine_tune(ofdft_engine* e, int slot, int iters, double* ms_default, double* ms_tuned, int* shape);
 /* Pin the slot's launch shape (the four values ofdft_engine_tune reports, e.g.
  * a shape tuned in an earlier run; radix cap 0 and y-z threads 0 mean the

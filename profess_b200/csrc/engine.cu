@@ -1658,12 +1658,15 @@ struct Engine {
 #endif
   }
 
-  // Tune slot i's launch shape by timing one evaluation of its resident input
-  // density per candidate (coordinate descent over the x radix cap, the
-  // x-forward and x-inverse task sizes and the y-z block size; a candidate must
-  // be 1 % faster to replace the incumbent).  The result is cached for the
-  // grid, precision and functional and applied to every slot of that kind,
-  // now and at creation.  The slot's solve record is overwritten.
+  // Tune the launch shape of slot i's kind of cell (grid, precision and
+  // functional) by timing one batched evaluation, per candidate, of every idle
+  // slot of that kind that holds a resident input density - the batch the
+  // shape will serve, since a lone slot leaves most SMs idle and favours other
+  // shapes.  Coordinate descent over the x radix cap, the x-forward and
+  // x-inverse task sizes and the y-z block size; a candidate must be 1 %
+  // faster to replace the incumbent.  The result is cached for the kind and
+  // applied to every slot of it, now and at creation.  The timed slots' solve
+  // records are overwritten.
   int tune(int i, int iters, double* ms_default, double* ms_tuned, int* shape_out) {
     int rc = check_slot(i);
     if (rc) return rc;
@@ -1672,29 +1675,36 @@ struct Engine {
     for (int k = 0; k < cap; ++k)
       if (slots[k].used && slots[k].running) return fail(OFDFT_EBUSY, "tune while no slot is running");
     iters = std::max(iters, 3);
-    const std::vector<int> ids{i};
+    std::vector<int> ids;
+    for (int k = 0; k < cap; ++k)
+      if (slots[k].used && slots[k].input && tune_key(slots[k]) == tune_key(h)) ids.push_back(k);
+    auto apply = [&](const Shape& c) -> int {
+      for (int k : ids) {
+        set_shape(slots[k], c);
+        const int r = upload_slot(k);
+        if (r) return r;
+      }
+      return OFDFT_OK;
+    };
     Shape best = shape_of(h);
+    if ((rc = apply(best))) return rc;
     double tbest = 0.0;
     if ((rc = time_ids(ids, iters, &tbest))) return rc;
     *ms_default = tbest;
     auto trial = [&](Shape c) -> int {
       if (!shape_ok(h, c)) return OFDFT_OK;
-      const Shape keep = shape_of(h);
-      set_shape(h, c);
       double t = 0.0;
-      int r = upload_slot(i);
+      int r = apply(c);
       if (!r) r = time_ids(ids, iters, &t);
       if (r) {
-        set_shape(h, keep);
-        upload_slot(i);
+        apply(best);
         return r;
       }
       if (t < 0.99 * tbest) {
         tbest = t;
         best = c;
       }
-      set_shape(h, best);
-      return upload_slot(i);
+      return apply(best);
     };
     const int pi = h.prec == OFDFT_FP32 ? 1 : 0;
     const SlotDev& s = h.sd;

@@ -399,7 +399,37 @@ def _term_errors(e_gpu, e_ref, nion):
     return {k: float(v) for k, v in zip(names, err)}, float(err.max())
 
 
+def run_eval_probe(args):
+    """Time batched potential evaluations only (the roofline probe): every
+    cell of the workload in the requested precisions, one evaluation each per
+    tick, median over --steps ticks after the engine's warm-up.  The command
+    the ncu summaries in profiles/ are taken on."""
+    from profess_b200 import cell as pcell
+    from profess_b200 import native, workloads as wl
+    eng = native.Engine()
+    cells = make_cells(args, 0)
+    precs = {"fp32": [native.FP32], "fp64": [native.FP64], "both": [native.FP32, native.FP64]}[args.eval_only]
+    for b, c in enumerate(cells):
+        r = wl.initial_density(c, seed=b)
+        e_ii = pcell.ion_ion_energy(eng.lib, c)
+        for p in precs:
+            s = pcell.setup_slot(eng, c, p, ion_ion=e_ii)
+            eng.set_input(s, r)
+    ms = eng.time_eval(iters=max(args.steps, 3))
+    alg = sum(eval_bytes(c, 4 if p == native.FP32 else 8) for c in cells for p in precs)
+    peak, kind = _peaks()
+    gbs = alg / (ms / 1e3) / 1e9 if ms > 0 else None  # the host emulation reports no time
+    print(json.dumps({"probe": "batched potential evaluation", "workload": args.workload, "cells": len(cells),
+                      "precisions": args.eval_only, "ms_per_eval": ms, "algorithmic_bytes": alg,
+                      "achieved_gbs": gbs, "frac": gbs / peak if gbs else None,
+                      "peak_gbs": peak, "peak_source": kind, "source_sha": source_sha()}), flush=True)
+    eng.close()
+    return 0
+
+
 def run_ours(args):
+    if args.eval_only:
+        return run_eval_probe(args)
     rt = Runtime(args)
     ws, rank = rt.ws, rt.rank
     from profess_b200 import cell as pcell
@@ -844,6 +874,8 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true",
                     help="skip the oracle solve (CPU baseline and errors against the oracle)")
     ap.add_argument("--no-tune", action="store_true", help="keep the default launch shapes (no autotuning)")
+    ap.add_argument("--eval-only", choices=["fp32", "fp64", "both"], default=None,
+                    help="only time batched potential evaluations of the workload's cells (profiling probe)")
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference(args)

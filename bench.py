@@ -772,11 +772,21 @@ def run_md(args, rt):
     eng = native.Engine()
     B = args.batch or 16
     cells = [wl.config_cell(2, seed=1000 * rt.rank + b) for b in range(B)]
-    run = md.NVE(eng, cells, 40.0, temperature_k=600.0, seed=1000 * rt.rank)
+    ens = args.md_ensemble
+    if ens == "nve":
+        run = md.NVE(eng, cells, 40.0, temperature_k=600.0, seed=1000 * rt.rank)
+    elif ens == "nvt":
+        run = md.NVT(eng, cells, 40.0, q_mass=1.0e4, temperature_k=600.0, seed=1000 * rt.rank)
+    else:
+        run = md.NPT(eng, cells, 40.0, q_mass=1.0e4, b_mass=1.0e6, temperature_k=600.0, ext_pres=0.0,
+                     seed=1000 * rt.rank)
+    conserved = {"nve": lambda r: r.history[-1]["conserved"] if r.history else r.conserved(),
+                 "nvt": lambda r: r.history[-1]["conserved"] if r.history else run.conserved_nh(r),
+                 "npt": lambda r: r.history[-1]["conserved"] if r.history else run.conserved_npt(r)}[ens]
     try:
         for _ in range(args.warmup):
             run.step()
-        h0 = [r.history[-1]["conserved"] if r.history else r.conserved() for r in run.reps]
+        h0 = [conserved(r) for r in run.reps]
         rt.barrier()
         t0 = time.perf_counter()
         for _ in range(args.steps):
@@ -790,12 +800,17 @@ def run_md(args, rt):
     if rt.rank != 0:
         rt.close()
         return 0
-    out = {"metric": "NVE MD replica-steps/s", "value": rt.ws * B * args.steps / wall, "unit": "replica-steps/s",
+    out = {"metric": "%s MD replica-steps/s" % ens.upper(), "value": rt.ws * B * args.steps / wall,
+           "unit": "replica-steps/s",
            "n_gpus": rt.ws, "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * wall / args.steps,
            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
            "data": "synthetic (seeded cells and velocities)",
-           "config": {"workload": WORKLOADS["cfg2"] + "; NVE velocity Verlet, 600 K, dt 40 a.u., FP64 NTN to "
-                                                      "potNorm<1e-6 warm-started from the last density",
+           "config": {"workload": WORKLOADS["cfg2"] + "; %s, 600 K, dt 40 a.u., FP64 NTN to potNorm<1e-6 "
+                                                      "warm-started from the last density" % {
+                                                          "nve": "NVE velocity Verlet",
+                                                          "nvt": "Nose-Hoover NVT, Q 1e4",
+                                                          "npt": "full-cell NPT, Q 1e4, barostat 1e6, P 0 (device "
+                                                                 "stress, lattice refresh)"}[ens],
                       "replicas_per_step": B, "parallelism": "replicas x%d" % rt.ws},
            "evals_per_solve": evals,
            "conserved_energy_drift_ha_per_atom": drift}
@@ -811,7 +826,13 @@ def run_relax(args, rt):
     eng = native.Engine()
     B = args.batch or 16
     cells = [wl.config_cell(2, seed=1000 * rt.rank + b) for b in range(B)]
-    qm = relax.QuickMin(eng, cells, max_steps=args.warmup + args.steps + 1)
+    method = args.relax_method
+    nmax = args.warmup + args.steps + 1
+    if method == "quickmin":
+        qm = relax.QuickMin(eng, cells, max_steps=nmax)
+    else:
+        cls = {"cg": relax.GradientCG, "cg2": relax.CG2, "bfgs": relax.BFGS}[method]
+        qm = cls(eng, cells, max_steps=1000)
     try:
         for _ in range(args.warmup):
             qm.step()
@@ -821,22 +842,29 @@ def run_relax(args, rt):
         rt.barrier()
         wall = rt.max_over_ranks(time.perf_counter() - t0)
         moved = rt.sum_over_ranks(moved)
-        f0 = max(st.initial_max_force for st in qm.states)
-        f1 = max(st.max_force for st in qm.states)
-        undone = sum(h["undone"] for st in qm.states for h in st.history)
+        if method == "quickmin":
+            f0 = max(st.initial_max_force for st in qm.states)
+            f1 = max(st.max_force for st in qm.states)
+            undone = int(sum(h["undone"] for st in qm.states for h in st.history))
+        else:
+            f0 = None
+            f1 = max(float(np.sqrt((st.forces ** 2).sum(axis=1)).max()) for st in qm.states)
+            undone = None
     finally:
         qm.close()
     if rt.rank != 0:
         rt.close()
         return 0
-    out = {"metric": "QuickMin relaxation cell-steps/s", "value": moved / wall, "unit": "cell-steps/s",
+    names = {"quickmin": "QuickMin", "cg": "old CG (GradientOptimization)", "cg2": "CG2", "bfgs": "BFGS (IonLBFGS)"}
+    out = {"metric": "%s relaxation cell-steps/s" % names[method], "value": moved / wall, "unit": "cell-steps/s",
            "n_gpus": rt.ws, "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * wall / args.steps,
            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
            "data": "synthetic (seeded cells)",
-           "config": {"workload": WORKLOADS["cfg2"] + "; QuickMin (time step 0.4 a.u. doubling), FP64 NTN to "
-                                                      "potNorm<1e-6 warm-started from the last density",
+           "config": {"workload": WORKLOADS["cfg2"] + "; %s, FP64 NTN to potNorm<1e-6 warm-started from the "
+                                                      "last density; a cell-step is one density solve of a cell" %
+                                   names[method],
                       "cells_per_step": B, "parallelism": "replicas x%d" % rt.ws},
-           "max_force_ha_per_bohr": {"initial": f0, "final": f1}, "moves_undone": int(undone)}
+           "max_force_ha_per_bohr": {"initial": f0, "final": f1}, "moves_undone": undone}
     print(json.dumps(out), flush=True)
     rt.close()
     return 0
@@ -874,6 +902,9 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true",
                     help="skip the oracle solve (CPU baseline and errors against the oracle)")
     ap.add_argument("--no-tune", action="store_true", help="keep the default launch shapes (no autotuning)")
+    ap.add_argument("--md-ensemble", choices=["nve", "nvt", "npt"], default="nve", help="--workload md ensemble")
+    ap.add_argument("--relax-method", choices=["quickmin", "cg", "cg2", "bfgs"], default="quickmin",
+                    help="--workload relax ion optimiser")
     ap.add_argument("--eval-only", choices=["fp32", "fp64", "both"], default=None,
                     help="only time batched potential evaluations of the workload's cells (profiling probe)")
     args = ap.parse_args()

@@ -256,17 +256,33 @@ class IonLineSearch:
 
 
 def nearest_distance(lattice: np.ndarray, frac: np.ndarray) -> float:
-    """Shortest ion-ion distance (bohr) over the cell and its 26 neighbour images."""
-    cart = frac @ lattice.T
-    n = len(frac)
-    best = np.inf
+    """Shortest ion-ion distance (bohr) over the cell and its 26 neighbour images
+    (CheckNearestDistanceAtoms, Source/Neighbor.f90:45-400, for cells within one
+    neighbour shell).  Candidates come from |a|^2 + |b|^2 - 2 a.b per image (one
+    matrix product each); every pair within a relative 1e-9 of the smallest is
+    then measured as |R_j + T - R_i|, so the result is that distance's value."""
+    cart = np.asarray(frac, dtype=float) @ lattice.T
+    n = len(cart)
+    c2 = (cart * cart).sum(axis=1)
+    cands = []
+    best2 = np.inf
     for t in np.ndindex(3, 3, 3):
         shift = lattice @ (np.array(t, dtype=float) - 1.0)
-        d = cart[None, :, :] + shift[None, None, :] - cart[:, None, :]
-        r = np.sqrt((d * d).sum(axis=2))
+        b = cart + shift
+        r2 = c2[:, None] + (b * b).sum(axis=1)[None, :] - 2.0 * (cart @ b.T)
         if t == (1, 1, 1):
-            r = r + np.diag(np.full(n, np.inf))
-        best = min(best, float(r.min()))
+            r2[np.diag_indices(n)] = np.inf
+        m = float(r2.min())
+        cands.append((shift, r2, m))
+        best2 = min(best2, m)
+    lim = best2 + 1e-9 * abs(best2) + 1e-12
+    best = np.inf
+    for shift, r2, m in cands:
+        if m > lim:
+            continue
+        for i, j in zip(*np.nonzero(r2 <= lim)):
+            d = cart[j] + shift - cart[i]
+            best = min(best, float(np.sqrt((d * d).sum())))
     return best
 
 

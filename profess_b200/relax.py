@@ -18,6 +18,7 @@ at most 200 steps.
 """
 from __future__ import annotations
 
+import concurrent.futures
 import dataclasses
 
 import numpy as np
@@ -386,13 +387,20 @@ class _GeneratorRelax:
             st.forces = self.eng.forces(st.slot, st.cell.nion, include_ewald=False) + st.f_ewald
             st.num_solves += 1
 
-    def _advance(self, st, gen, sent):
-        """Move the cell's optimiser to its next density request (or its end)."""
+    @staticmethod
+    def _next(gen, sent):
+        """The optimiser's next geometry, or (None, final coordinates) at its end."""
         try:
-            frac = next(gen) if sent is None else gen.send(sent)
+            return (next(gen) if sent is None else gen.send(sent)), None
         except StopIteration as stop:
+            return None, stop.value
+
+    def _apply(self, st, nxt):
+        """Start the density solve of the cell's next geometry (or mark it done)."""
+        frac, final = nxt
+        if frac is None:
             st.done = True
-            st.cell.frac = stop.value
+            st.cell.frac = final
             return
         st.cell.frac = frac
         self.eng.hold_density(st.slot)
@@ -400,16 +408,30 @@ class _GeneratorRelax:
         _, st.f_ewald = self.eng.ewald(st.slot, st.cell.nion)
         self.eng.start_solve(st.slot, None, self.opts)
 
+    def _advance(self, st, gen, sent):
+        """Move the cell's optimiser to its next density request (or its end)."""
+        self._apply(st, self._next(gen, sent))
+
     def step(self) -> int:
-        """Solve every pending geometry together and advance each optimiser."""
+        """Solve every pending geometry together and advance each optimiser.  The
+        optimisers' host work (independent per cell, mostly NumPy) runs on a
+        thread pool; the engine calls that follow are made in cell order."""
         pending = [k for k, st in enumerate(self.states) if not st.done]
         if not pending:
             return 0
         self._finish([self.states[k] for k in pending])
+        sent = []
         for k in pending:
             st = self.states[k]
             self.traces[k].append(float(st.energy[0]))
-            self._advance(st, self.gens[k], (float(st.energy[0]), st.forces))
+            sent.append((float(st.energy[0]), st.forces))
+        if len(pending) > 1:
+            with concurrent.futures.ThreadPoolExecutor(max_workers=min(8, len(pending))) as ex:
+                nxt = list(ex.map(self._next, [self.gens[k] for k in pending], sent))
+        else:
+            nxt = [self._next(self.gens[pending[0]], sent[0])]
+        for k, n in zip(pending, nxt):
+            self._apply(self.states[k], n)
         return len(pending)
 
     def run(self):

@@ -437,6 +437,9 @@ struct Engine {
     rc = dmalloc((void**)&d_ctl, sizeof(Ctl) * cap);
     if (rc) return rc;
     if ((rc = plans.build())) return rc;
+#if !defined(OFDFT_EMU)
+    if ((rc = preload_kernels())) return rc;
+#endif
     return dsync();  // the plan tables were copied on the legacy stream
   }
 
@@ -1987,6 +1990,52 @@ struct Engine {
   }
 
 #if !defined(OFDFT_EMU)
+  // Load every kernel of the library now: with CUDA's lazy module loading the
+  // first launch of each kernel would otherwise pay its load (10-30 ms), which
+  // a serving engine would see as latency on its first requests.
+  template <typename T>
+  int preload_prec() {
+    cudaFuncAttributes fa;
+    int rc = OFDFT_OK;
+    auto load = [&](auto kern) {
+      if (!rc) rc = cuda_check(cudaFuncGetAttributes(&fa, kern), "kernel load");
+    };
+    load(k_vec<T>);
+    load(k_ctl<T>);
+    load(k_xfwd<T, KS_WT>);
+    load(k_xfwd<T, KS_WGC>);
+    load(k_ypass<T>);
+    load(k_zpass<T, KS_WT>);
+    load(k_zpass<T, KS_WGC>);
+    load(k_yzpass<T, 256>);
+    load(k_yzpass<T, 512>);
+    load(k_xinv<T, KS_WT>);
+    load(k_xinv<T, KS_WGC>);
+    load(k_permute_kernel<T>);
+    load(k_unpermute_kernel<T>);
+    load(k_fill_kernel<T>);
+    load(k_spread<T>);
+    load(k_force_gather<T>);
+    load(k_square_copy<T, T>);
+    load(k_square_copy<T, double>);
+    load(k_convert<double, T>);
+    load(k_convert<T, double>);
+    load(k_stress<T>);
+    load(k_rho_vxc<T>);
+    load(k_sum<T>);
+    load(k_scale<T>);
+    return rc;
+  }
+  int preload_kernels() {
+    cudaFuncAttributes fa;
+    int rc = preload_prec<float>();
+    if (!rc) rc = preload_prec<double>();
+    for (const void* k : {(const void*)k_ewald_real, (const void*)k_ewald_plane, (const void*)k_ewald_recip_force,
+                          (const void*)k_ewald_real_stress, (const void*)k_ewald_plane_stress, (const void*)k_stress_sf})
+      if (!rc) rc = cuda_check(cudaFuncGetAttributes(&fa, k), "kernel load");
+    return rc;
+  }
+
   // Kernels whose dynamic shared memory exceeds the default 48 KB need the
   // opt-in attribute; it must be set outside stream capture.
   template <typename T>

@@ -1,7 +1,7 @@
 """Geometry relaxation of many independent cells on one engine: the
 reference's ion optimisers (dispatched at Source/Optimizer.f90:247-260)
 QuickMin (method 2), the old conjugate gradient (3, GradientCG), CG2 (4) and
-BFGS (5).
+BFGS (5), and its cell optimiser (SteepestDecent, CellRelax).
 
 QuickMinOptimization (Source/IonOptQui.f90:33-368) runs a batch of cells in
 lockstep: every
@@ -789,3 +789,119 @@ class GradientCG(_GeneratorRelax):
     def _moves(self, st, force_cutoff, max_steps, nn_dist):
         return gradient_moves(self.eng.lib, st.cell.lattice, st.cell.frac, float(st.energy[0]), st.forces,
                               force_cutoff=force_cutoff, max_steps=max_steps)
+
+
+# ---------------------------------------------------------------- cell optimiser
+CELL_MAX_STEPS = 100   # Source/CellOptimizers.f90: maxCellStep
+CELL_TOLS = 5.0e-7     # Source/CellOptimizers.f90: tols (Ha/bohr^3)
+
+
+@dataclasses.dataclass
+class CellState:
+    cell: Cell
+    slot: int
+    dt: float = 10.0
+    old_energy: float = 0.0
+    energy: np.ndarray = None
+    stress: np.ndarray = None
+    steps: int = 0
+    done: bool = False
+    history: list = dataclasses.field(default_factory=list)
+
+
+class CellRelax:
+    """The reference's cell optimiser, SteepestDecent
+    (Source/CellOptimizers.f90:107-304), for a batch of cells: each cell step
+    solves the density at fixed fractional ion positions (ion method "non"),
+    takes the device stress, and moves the lattice down the stress,
+    L <- L - V dt sigma L^-T, with dt 10 at the start, x1.2 after a lower
+    energy and /4 after a higher one; it stops when max |sigma| < tols
+    (5e-7 Ha/bohr^3) or after max_steps.  axis 1-3 relaxes one diagonal
+    component only.  A lattice move runs RefreshCellSetup and RescaleDensity
+    on the device (ofdft_slot_set_lattice, the WT kernel, ion potential and
+    Ewald rebuilt, ofdft_slot_rescale_input), and the next solve starts from
+    the held density.  All cells' solves run together.  WT functional."""
+
+    def __init__(self, eng: native.Engine, cells, max_steps: int = CELL_MAX_STEPS, tols: float = CELL_TOLS,
+                 axis: int = 0, opts=None):
+        self.eng = eng
+        self.opts = opts or native.ntn_options()
+        self.max_steps, self.tols, self.axis = int(max_steps), float(tols), int(axis)
+        self.states = []
+        try:
+            for c in cells:
+                c = dataclasses.replace(c, frac=np.array(c.frac, dtype=float), lattice=np.array(c.lattice, float))
+                self.states.append(CellState(cell=c, slot=pcell.setup_slot(eng, c, native.FP64)))
+            for st in self.states:
+                rho = np.full(st.cell.grid, st.cell.num_electrons / st.cell.vol)
+                self.eng.start_solve(st.slot, np.asfortranarray(rho), self.opts)
+        except Exception:
+            self.close()
+            raise
+
+    def close(self):
+        for st in self.states:
+            self.eng.slot_destroy(st.slot)
+        self.states = []
+
+    def _move(self, st):
+        """The cell step after a solve (SteepestDecent's loop body)."""
+        c = st.cell
+        stress = st.stress
+        if self.axis in (1, 2, 3):
+            a = self.axis - 1
+            keep = stress[a, a]
+            stress = np.zeros((3, 3))
+            stress[a, a] = keep
+            if abs(keep) < self.tols:
+                st.done = True
+                return
+        elif float(np.abs(stress).max()) < self.tols:
+            st.done = True
+            return
+        e = float(st.energy[0])
+        st.dt = st.dt / 4.0 if e > st.old_energy else st.dt * 1.2
+        st.old_energy = e
+        new = c.lattice - c.vol * st.dt * (stress @ np.linalg.inv(c.lattice).T)
+        if self.axis in (1, 2, 3):
+            a = self.axis - 1
+            keep = new[a, a]
+            new = c.lattice.copy()
+            new[a, a] = keep
+        if st.steps >= self.max_steps:  # the reference moves the cell, then stops before its next solve
+            c.lattice = new
+            st.done = True
+            return
+        self.eng.hold_density(st.slot)
+        c.lattice = new
+        rho_avg = c.num_electrons / c.vol
+        self.eng.set_lattice(st.slot, new, rho_avg, rho_avg)
+        self.eng.rescale_input(st.slot, c.num_electrons)
+        self.eng.build_wt_kernel(st.slot)
+        self.eng.build_ion_potential(st.slot, c.frac, c.species_of_ion, c.species)
+        self.eng.ewald(st.slot, c.nion, want_forces=False)
+        self.eng.start_solve(st.slot, None, self.opts)
+
+    def step(self) -> int:
+        """Finish the pending solves, take every cell's stress and move its lattice."""
+        pending = [st for st in self.states if not st.done]
+        if not pending:
+            return 0
+        while self.eng.run(8):
+            pass
+        for st in pending:
+            _, st.energy, stats = self.eng.result(st.slot, want_rho=False)
+            if stats["outcome"] != 0:
+                raise native.OfdftError(7, "density solve did not converge (slot %d)" % st.slot)
+            st.stress = self.eng.stress(st.slot)
+            st.steps += 1
+            st.history.append({"energy": float(st.energy[0]), "stress": st.stress.copy(),
+                               "lattice": st.cell.lattice.copy()})
+        for st in pending:
+            self._move(st)
+        return len(pending)
+
+    def run(self):
+        while self.step():
+            pass
+        return self.states

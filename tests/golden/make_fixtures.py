@@ -78,6 +78,30 @@ def _stress_au(lines, rel):
     return {"value": rows, "source": "%s:%d-%d" % (rel, src[0], src[-1])}
 
 
+def _cell_relax(lines, rel, geom_path, geom_rel):
+    """The cell relaxation trace: per cell step the TOTAL ENERGY (eV) of its
+    density solve, the ST_AU stress (Ha/bohr^3) and the step's summary line;
+    then the final lattice (Angstrom rows) of the .final.geom file."""
+    steps, energy, stress, src = [], None, [], None
+    for i, ln in enumerate(lines):
+        m = re.search(r"TOTAL ENERGY =\s+(\S+) eV", ln)
+        if m:
+            energy, src = float(m.group(1)), i + 1
+        m = re.match(r"\s*ST_AU\s+(\d)\s+(\S+)\s+(\S+)\s+(\S+)", ln)
+        if m:
+            stress.append([float(m.group(k).replace("D", "E")) for k in (2, 3, 4)])
+        m = re.search(r"; Cell optimization at step\s*(\d+), max\(stress\):\s*(\S+), total energy:\s*(\S+)", ln)
+        if m:
+            steps.append({"step": int(m.group(1)), "energy_ev": energy, "energy_source": "%s:%d" % (rel, src),
+                          "stress_au": stress[-3:], "max_stress": float(m.group(2)),
+                          "energy_ha_line": float(m.group(3)), "source": "%s:%d" % (rel, i + 1)})
+            stress = []
+    final = _ion_block(geom_path)
+    return {"steps": steps, "final_lattice_angstrom_rows": final["lattice_angstrom_rows"],
+            "final_source": geom_rel, "max_cell_step": 100, "tols": 5.0e-7,
+            "params_source": "Source/CellOptimizers.f90 (maxCellStep, tols)"}
+
+
 def _final_terms(lines, rel, nonlocal_label):
     labels = {"tf": r"Thomas-Fermi Kin\. Energy =\s+(\S+) eV",
               "vw": r"Von-Weizsacker Kin\. Ener =\s+(\S+) eV",
@@ -146,6 +170,8 @@ def main(root=None):
         "final": {"total": dict(zip(("value_ev", "source"),
                                     _find(lines, r"TOTAL ENERGY =\s+(\S+) eV", rel)))},
         "stress_au": _stress_au(lines, rel),
+        "cell_relax": _cell_relax(lines, rel, os.path.join(REF, "optCell/sampleoutput/displaced.final.geom"),
+                                  "test/optCell/sampleoutput/displaced.final.geom"),
     }
     for c in cases.values():
         c["dv"] = dict(zip(("value", "source"), c["dv"])) if "dv" in c else None

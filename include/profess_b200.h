@@ -173,11 +173,12 @@ int ofdft_slot_set_lattice(ofdft_engine* e, int slot, const double* lattice, dou
  * with the slot's current dV, e.g. after a change of lattice. */
 int ofdft_slot_rescale_input(ofdft_engine* e, int slot, double num_electrons);
 /* Stress tensor (Ha/bohr^3, stress[9] row-major and symmetric) of the slot's
- * current density (rho = NULL: phi^2 of the last solve) or of the given rho,
- * for the WT functional: CalculateStress (Source/CalStress.f90:44-253) with
- * the TF, vW, WT, Hartree, LDA and B-spline ion-electron terms plus, when
- * include_ewald, the Ewald term (EwaldStress, Source/Ewald.f90:1857-2535).
- * terms[7*9] (may be NULL) receives the seven parts in that order.  Runs one
+ * current density (rho = NULL: phi^2 of the last solve) or of the given rho:
+ * CalculateStress (Source/CalStress.f90:44-253) with the TF, vW, nonlocal
+ * kinetic (WTStress or, for second-order WGC slots, WGCStress), Hartree, LDA
+ * and B-spline ion-electron terms plus, when include_ewald, the Ewald term
+ * (EwaldStress, Source/Ewald.f90:1857-2535).  terms[7*9] (may be NULL)
+ * receives the seven parts in that order.  Runs one
  * energy evaluation and the forward transforms of the density on the device;
  * the slot's solve record, current phi and potential are kept.  Needs
  * ofdft_slot_build_ion_potential first. */

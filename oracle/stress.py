@@ -1,7 +1,8 @@
 """Test infrastructure (the oracle): the stress tensor of a converged density,
 a CPU restatement of CalculateStress (Source/CalStress.f90:44-253) for the WT
-functional with LDA, the B-spline ion-electron term and the Ewald sum.  Only
-tests import it.  Stress = (1/volume) dE/d(strain), Ha/bohr^3.
+and the second-order WGC functionals with LDA, the B-spline ion-electron term
+and the Ewald sum.  Only tests import it.  Stress = (1/volume) dE/d(strain),
+Ha/bohr^3.
 
 Terms:
   TF           -2/3 E_TF / vol on the diagonal            (TFStress, KEDF_TF.f90:283-334)
@@ -9,6 +10,8 @@ Terms:
   WT           sum over the half spectrum of -eta G'(eta) F[rho^a] F[rho^b]* (q_a q_b / q^2
                - delta_ab / 3) pi^2 / (alpha beta kF rho0^(a+b-2)), - 2/3 E_WT / vol on the
                diagonal                                  (WTStress, KEDF_WT.f90:263-394)
+  WGC          the kernel-derivative sums of WGCStress over the half spectrum of
+               F[rho^x], x = a, b, a+1, b+1, a+2, b+2     (WGCStress, KEDF_WGC.f90:519-745)
   Hartree      8 pi sum_half |rho(q)|^2 q_a q_b / q^4 - E_H / vol   (JStress, Hartree.f90:173-247)
   LDA          E_xc / vol - <rho v_xc> on the diagonal   (LDAStress, XC_LDA.f90:663-732)
   ion-electron -2 N sum_half q_a q_b / q Re(rho(q) S_s(q)) V_s'(q), - E_ie, / vol
@@ -28,7 +31,7 @@ import numpy as np
 
 from . import cellsetup as cs
 from . import functional as fn
-from .consts import PI
+from .consts import C_TF, PI
 
 
 def q_mask(n1: int, n2: int, n3: int) -> np.ndarray:
@@ -127,9 +130,51 @@ def ewald_stress(lattice: np.ndarray, frac: np.ndarray, z: np.ndarray) -> np.nda
     return s / vol
 
 
-def stress(cell: cs.Cell, f: fn.Functional, rho: np.ndarray) -> np.ndarray:
-    """The stress tensor (Ha/bohr^3) of density rho for the WT functional f."""
-    assert f.kinetic == fn.KEDF_WT
+def wgc_stress(cell: cs.Cell, f: fn.Functional, rho: np.ndarray, gamma: float, rho0: float) -> np.ndarray:
+    """WGCStress (Source/KEDF_WGC.f90:519-745) for the second-order WGC kernel
+    (WGCT = 2) with rho0 and rho* not held (hold0 = holdS = .FALSE.): upper
+    triangle, before CalculateStress symmetrises."""
+    n1, n2, n3 = f.n
+    g = cs.g_vectors(cell.recip, n1, n2, n3)
+    q = np.sqrt((g * g).sum(-1))
+    mask = q_mask(n1, n2, n3)
+    qm = np.where(mask, q, 1.0)
+    a, b, rs, mu = f.alpha, f.beta, f.rho_s, f.mu
+    kf = (3.0 * PI ** 2 * rs) ** (1.0 / 3.0)
+    fa = np.conj(cs.fft_r2c(rho ** a))
+    fb = cs.fft_r2c(rho ** b)
+    fa1 = np.conj(cs.fft_r2c(rho ** (a + 1.0)))
+    fb1 = cs.fft_r2c(rho ** (b + 1.0))
+    fa2 = np.conj(cs.fft_r2c(rho ** (a + 2.0)))
+    fb2 = cs.fft_r2c(rho ** (b + 2.0))
+    ki = 20.0 * rho0 ** (5.0 / 3.0 - (a + b))
+    c001, c002, c003 = -2.0 / 3.0, rs * 4.0 / 3.0, -rs ** 2 * 2.0 / 3.0
+    c011, c012, c021, c111 = -5.0 / 3.0, rs * 5.0 / 3.0, -4.0 / 3.0, -8.0 / 3.0
+    c011, c012, c021, c111, diff = c011 + 1.0, c012 - rs, c021 + 1.0, c111 + 2.0, -1.0 / 3.0
+    K1, K2, K3, K4 = f.kernel[0], f.kernel[1], f.kernel[2], f.kernel[3]
+    eta = np.where(mask, q / (2.0 * kf), 0.0)
+    c00 = c001 * K1 + c002 * K2 + c003 * (K3 + K4)
+    c01 = c011 * K2 + c012 * (K3 + K4)
+    c02 = c021 * K3
+    c11 = c111 * K4
+    diago = fa * c00 * fb + fa1 * c01 * fb + fa * c01 * fb1 + fa2 * c02 * fb + fa * c02 * fb2 + fa1 * c11 * fb1
+    gp = g_prime(eta, mu)
+    d11 = -ki * eta / (36.0 * rs ** 2) * gp - K4 * 6.0 * (a + b) - K2 * (gamma * (a + b) + 6.0 * a * b) / rs
+    d02 = (-ki * eta / (72.0 * rs ** 2) * gp - K4 * (3.0 * (a + b + 1.0) - gamma)
+           - K2 * (3.0 * gamma * (a + b + 1.0) - gamma ** 2 + 18.0 * a * b) / (6.0 * rs))
+    d01 = K4 * 6.0 * rs + K2 * gamma
+    d00 = 6.0 * rs * K2 - 2.0 * rs * d01 + rs ** 2 * (2.0 * d02 + d11)
+    d01 = -rs * (d11 + 2.0 * d02) + d01
+    offdia = fa * d00 * fb + fa1 * d01 * fb + fa * d01 * fb1 + fa2 * d02 * fb + fa * d02 * fb2 + fa1 * d11 * fb1
+    dg = float(np.where(mask, np.real(diago + offdia * diff), 0.0).sum())
+    s = np.eye(3) * dg + _outer(g, np.where(mask, np.real(offdia) / qm ** 2, 0.0))
+    return np.triu(s) * 2.0 * C_TF
+
+
+def stress(cell: cs.Cell, f: fn.Functional, rho: np.ndarray, gamma: float = 2.7, rho0: float = None) -> np.ndarray:
+    """The stress tensor (Ha/bohr^3) of density rho for the WT or WGC functional
+    f (gamma and rho0: the WGC kernel's parameters; rho0 defaults to N / V)."""
+    assert f.kinetic in (fn.KEDF_WT, fn.KEDF_WGC)
     n1, n2, n3 = f.n
     N = n1 * n2 * n3
     vol = cell.vol
@@ -148,16 +193,18 @@ def stress(cell: cs.Cell, f: fn.Functional, rho: np.ndarray) -> np.ndarray:
     for a in range(3):
         for b in range(a, 3):
             s[a, b] += -f.mu * float((grads[a] * grads[b]).sum()) / N
-    # WT
-    rho0 = cell.num_electrons / vol
-    kf = (3.0 * PI ** 2 * rho0) ** (1.0 / 3.0)
-    fa = cs.fft_r2c(rho ** f.alpha)
-    fb = np.conj(cs.fft_r2c(rho ** f.beta))
-    eta = np.where(mask, q / (2.0 * kf), 0.0)
-    diff = np.where(mask, np.real(-eta * g_prime(eta, f.mu) * fa * fb), 0.0)
-    wt = _outer(g, diff / qm ** 2) - eye / 3.0 * float(diff.sum())
-    s += wt * PI ** 2 / (f.alpha * f.beta * kf * rho0 ** (f.alpha + f.beta - 2.0))
-    s += -2.0 / 3.0 * et[8] / vol * eye
+    if f.kinetic == fn.KEDF_WGC:
+        s += wgc_stress(cell, f, rho, gamma, cell.num_electrons / vol if rho0 is None else rho0)
+    else:  # WT
+        rho0 = cell.num_electrons / vol
+        kf = (3.0 * PI ** 2 * rho0) ** (1.0 / 3.0)
+        fa = cs.fft_r2c(rho ** f.alpha)
+        fb = np.conj(cs.fft_r2c(rho ** f.beta))
+        eta = np.where(mask, q / (2.0 * kf), 0.0)
+        diff = np.where(mask, np.real(-eta * g_prime(eta, f.mu) * fa * fb), 0.0)
+        wt = _outer(g, diff / qm ** 2) - eye / 3.0 * float(diff.sum())
+        s += wt * PI ** 2 / (f.alpha * f.beta * kf * rho0 ** (f.alpha + f.beta - 2.0))
+        s += -2.0 / 3.0 * et[8] / vol * eye
     # Hartree
     rq = cs.fft_r2c(rho)
     s += 8.0 * PI * _outer(g, np.where(mask, np.abs(rq) ** 2 / qm ** 4, 0.0)) - et[3] / vol * eye

@@ -944,7 +944,8 @@ struct Engine {
 
   // Stress tensor (Ha/bohr^3, out[9] row-major, symmetric) of rho (host, FP64)
   // or, with rho NULL, of the slot's current density phi^2; terms[7*9] (may be
-  // NULL) gets the TF, vW, WT, Hartree, LDA, ion-electron and Ewald parts.
+  // NULL) gets the TF, vW, nonlocal (WT or WGC), Hartree, LDA, ion-electron
+  // and Ewald parts.
   // The energies come from one evaluation of the density; the spectral sums
   // from the EV_STRESS transforms and the stress reduction (stress.cuh).  The
   // slot's control record, current phi and potential are left as they were.
@@ -953,9 +954,9 @@ struct Engine {
     if (rc) return rc;
     HostSlot& h = slots[i];
     SlotDev& s = h.sd;
-    if (s.kinetic != KIN_WT) return fail(OFDFT_EINVAL, "the stress is implemented for the WT functional");
+    const bool wgc = s.kinetic == KIN_WGC;
     if (h.nion < 1 || s.ion.nspec < 1) return fail(OFDFT_EINVAL, "build the ion potential before the stress");
-    if (!(h.rho0 > 0)) return fail(OFDFT_EINVAL, "rho0 must be positive for the WT stress");
+    if (!(h.rho0 > 0) || (wgc && !(s.rho_s > 0))) return fail(OFDFT_EINVAL, "rho0 (and rho* for WGC) must be positive");
     Ctl saved;
     if ((rc = get_ctl(i, saved))) return rc;
     // two work buffers that hold neither the current phi nor its potential
@@ -1004,7 +1005,9 @@ struct Engine {
     for (int k = 0; k < nion; ++k) species[k] = h.stencils[k].species;
     StressArgs sa;
     sa.nion = nion;
-    sa.kf = std::cbrt(3.0 * PI_D * PI_D * h.rho0);
+    sa.kf = std::cbrt(3.0 * PI_D * PI_D * (wgc ? s.rho_s : h.rho0));
+    sa.ki = 20.0 * std::pow(h.rho0, 5.0 / 3.0 - (s.alpha + s.beta));
+    sa.gamma = h.gamma;
     const int nblk = (int)std::max<long long>(1, std::min<long long>(2 * (long long)num_sms, (s.Nc + 127) / 128));
     std::vector<double> part((size_t)NSC * nblk);
 #if defined(OFDFT_EMU)
@@ -1050,9 +1053,11 @@ struct Engine {
     // assembly (CalculateStress): six components per term, then the diagonal terms
     const double vol = s.vol;
     double T6[7][6] = {{0}};
+    // the kinetic nonlocal term: WT (WTStress) or WGC (WGCStress, x 2 cTF)
+    const double wtc = wgc ? 2.0 * C_TF
+                           : PI_D * PI_D / (s.alpha * s.beta * sa.kf * std::pow(h.rho0, s.alpha + s.beta - 2.0));
     for (int k = 0; k < 6; ++k) {
       T6[1][k] = -s.mu * acc[SC_VW + k];
-      const double wtc = PI_D * PI_D / (s.alpha * s.beta * sa.kf * std::pow(h.rho0, s.alpha + s.beta - 2.0));
       T6[2][k] = wtc * acc[SC_WT + k];
       T6[3][k] = 8.0 * PI_D * acc[SC_H + k];
       T6[5][k] = -2.0 * (double)s.N * acc[SC_IE + k] / vol;
@@ -1060,10 +1065,9 @@ struct Engine {
     double sxc = 0.0;
     if ((rc = rho_vxc(i, ib, &sxc))) return rc;
     const int diag[3] = {0, 3, 5};
-    const double wtc = PI_D * PI_D / (s.alpha * s.beta * sa.kf * std::pow(h.rho0, s.alpha + s.beta - 2.0));
     for (int d : diag) {
       T6[0][d] += -2.0 / 3.0 * et[6] / vol;
-      T6[2][d] += -wtc * acc[SC_WTTR] / 3.0 - 2.0 / 3.0 * et[8] / vol;
+      T6[2][d] += wgc ? wtc * acc[SC_WTTR] : -wtc * acc[SC_WTTR] / 3.0 - 2.0 / 3.0 * et[8] / vol;
       T6[3][d] += -et[3] / vol;
       T6[4][d] += et[4] / vol - sxc;
       T6[5][d] += -et[2] / vol;

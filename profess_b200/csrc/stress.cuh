@@ -1,6 +1,7 @@
 // Stress tensor of a density on the device (CalculateStress,
-// Source/CalStress.f90:44-253) for the WT functional with LDA exchange-
-// correlation, the B-spline ion-electron term and the Ewald sum.
+// Source/CalStress.f90:44-253) for the WT and second-order WGC functionals
+// with LDA exchange-correlation, the B-spline ion-electron term and the
+// Ewald sum.
 //
 // The density's forward spectra (rho, rho^beta, sqrt(rho), rho^alpha) come
 // from the engine's own transforms (EV_STRESS passes: x, y and z forward, in
@@ -13,6 +14,8 @@
 //                                                  (VWStress, KEDF_VW.f90:365-449)
 //   WT        -eta G'(eta) Re(F[rho^a] F[rho^b]*) (q_a q_b / q^2, and its trace)
 //                                                  (WTStress, KEDF_WT.f90:263-394)
+//   WGC       the kernel-derivative sums of F[rho^x], x = a, b, a+1, b+1, a+2,
+//             b+2 (stress_wgc_point)               (WGCStress, KEDF_WGC.f90:519-745)
 //   Hartree   |rho(q)|^2 q_a q_b / q^4                (JStress, Hartree.f90:173-247)
 //   ion-elec. Re(rho(q) S_s(q)) V_s'(q) q_a q_b / q, S_s the B-spline
 //             structure factor of species s       (IonElectronStressSpline,
@@ -44,7 +47,8 @@ struct StressArgs {
   const cx<double>* sf;      // A_d(ion, k): per ion k1 + n2 + n3 entries (x, then y, then z)
   const int* species;        // species of each ion
   int nion;
-  double kf;                 // (3 pi^2 rho0)^(1/3)
+  double kf;                 // (3 pi^2 rho0)^(1/3) (WT), (3 pi^2 rho*)^(1/3) (WGC)
+  double ki, gamma;          // WGC: 20 rho0^(5/3 - alpha - beta), the kernel's gamma
 };
 
 // qMask (PlaneWave.f90:255-296) at natural indices (kx < k1, ky, kz): the
@@ -144,6 +148,51 @@ HD cx<double> spec_at(const SlotDev& s, int f, long long p) {
   return mk<double>((double)v.x * s.inv_n, (double)v.y * s.inv_n);
 }
 
+// Re(conj(a) b).
+HD double re_cb(cx<double> a, cx<double> b) { return a.x * b.x + a.y * b.y; }
+
+// The WGC kinetic terms of one masked frequency (WGCStress, KEDF_WGC.f90:
+// 519-745, WGCT = 2, rho0 and rho* refreshed with the cell): acc[SC_WTTR]
+// gets the diagonal sum (diago + offdia diff), acc[SC_WT..] offdia q_a q_b / q^2;
+// both are scaled by 2 cTF on the host.  F[rho^(x+1)] and F[rho^(x+2)] come
+// from the evaluation's fields rho^x, theta rho^x, theta^2 rho^x / 2 (theta =
+// rho - rho*) by linearity.
+template <typename T>
+HD void stress_wgc_point(const SlotDev& s, const StressArgs& sa, long long p, const double* g, double q2,
+                         double eta, double* acc) {
+  const double a = s.alpha, b = s.beta, rs = s.rho_s, gm = sa.gamma;
+  const cx<double> A = spec_at<T>(s, 2, p), At = spec_at<T>(s, 3, p), Ah = spec_at<T>(s, 4, p);
+  const cx<double> B = spec_at<T>(s, 5, p), Bt = spec_at<T>(s, 6, p), Bh = spec_at<T>(s, 7, p);
+  const cx<double> A1 = mk<double>(At.x + rs * A.x, At.y + rs * A.y);
+  const cx<double> B1 = mk<double>(Bt.x + rs * B.x, Bt.y + rs * B.y);
+  const cx<double> A2 = mk<double>(2.0 * Ah.x + 2.0 * rs * At.x + rs * rs * A.x, 2.0 * Ah.y + 2.0 * rs * At.y + rs * rs * A.y);
+  const cx<double> B2 = mk<double>(2.0 * Bh.x + 2.0 * rs * Bt.x + rs * rs * B.x, 2.0 * Bh.y + 2.0 * rs * Bt.y + rs * rs * B.y);
+  const T* kern = (const T*)s.kern;
+  const double K1 = (double)kern[p], K2 = (double)kern[s.Nc + p], K3 = (double)kern[2 * s.Nc + p],
+               K4 = (double)kern[3 * s.Nc + p];
+  // hold0 = holdS = .FALSE.
+  const double c001 = -2.0 / 3.0, c002 = rs * 4.0 / 3.0, c003 = -rs * rs * 2.0 / 3.0;
+  const double c011 = -5.0 / 3.0 + 1.0, c012 = rs * 5.0 / 3.0 - rs, c021 = -4.0 / 3.0 + 1.0, c111 = -8.0 / 3.0 + 2.0;
+  const double diff = -1.0 / 3.0;
+  const double c00 = c001 * K1 + c002 * K2 + c003 * (K3 + K4);
+  const double c01 = c011 * K2 + c012 * (K3 + K4);
+  const double c02 = c021 * K3;
+  const double c11 = c111 * K4;
+  const double p00 = re_cb(A, B), p10 = re_cb(A1, B), p01 = re_cb(A, B1), p20 = re_cb(A2, B), p02 = re_cb(A, B2),
+               p11 = re_cb(A1, B1);
+  const double diago = c00 * p00 + c01 * (p10 + p01) + c02 * (p20 + p02) + c11 * p11;
+  const double gp = wt_g_prime(eta, s.mu);
+  const double d11 = -sa.ki * eta / (36.0 * rs * rs) * gp - K4 * 6.0 * (a + b) - K2 * (gm * (a + b) + 6.0 * a * b) / rs;
+  const double d02 = -sa.ki * eta / (72.0 * rs * rs) * gp - K4 * (3.0 * (a + b + 1.0) - gm) -
+                     K2 * (3.0 * gm * (a + b + 1.0) - gm * gm + 18.0 * a * b) / (6.0 * rs);
+  double d01 = K4 * 6.0 * rs + K2 * gm;
+  const double d00 = 6.0 * rs * K2 - 2.0 * rs * d01 + rs * rs * (2.0 * d02 + d11);
+  d01 = -rs * (d11 + 2.0 * d02) + d01;
+  const double offdia = d00 * p00 + d01 * (p10 + p01) + d02 * (p20 + p02) + d11 * p11;
+  acc[SC_WTTR] += diago + offdia * diff;
+  sym_add(acc + SC_WT, g, offdia / q2);
+}
+
 // The terms of stored frequency p (kx-major position) added to acc[NSC].
 template <typename T>
 HD void stress_point(const SlotDev& s, const StressArgs& sa, long long p, double* acc) {
@@ -155,8 +204,8 @@ HD void stress_point(const SlotDev& s, const StressArgs& sa, long long p, double
   const double* R = s.recip;
   double g[3], ge[3];
   for (int r = 0; r < 3; ++r) g[r] = R[r] * kx + R[3 + r] * m2 + R[6 + r] * m3;
-  const cx<double> F0 = spec_at<T>(s, 0, p), Fb = spec_at<T>(s, 1, p), Fs = spec_at<T>(s, 2, p);
-  const cx<double> Fa = s.nf > 3 ? spec_at<T>(s, 3, p) : Fb;
+  const bool wgc = s.kinetic == KIN_WGC;  // WGC fields: rho, sqrt(rho), then the alpha and beta triples
+  const cx<double> F0 = spec_at<T>(s, 0, p), Fs = spec_at<T>(s, wgc ? 1 : 2, p);
   // vW
   const bool edge = kx == 0 || ((n1 % 2) == 0 && kx == n1 / 2);
   if (edge) {
@@ -173,11 +222,16 @@ HD void stress_point(const SlotDev& s, const StressArgs& sa, long long p, double
   const double q = sqrt(q2);
   // Hartree
   sym_add(acc + SC_H, g, (F0.x * F0.x + F0.y * F0.y) / (q2 * q2));
-  // WT
   const double eta = q / (2.0 * sa.kf);
-  const double diff = -eta * wt_g_prime(eta, s.mu) * (Fa.x * Fb.x + Fa.y * Fb.y);
-  sym_add(acc + SC_WT, g, diff / q2);
-  acc[SC_WTTR] += diff;
+  if (wgc) {
+    stress_wgc_point<T>(s, sa, p, g, q2, eta, acc);
+  } else {  // WT
+    const cx<double> Fb = spec_at<T>(s, 1, p);
+    const cx<double> Fa = s.nf > 3 ? spec_at<T>(s, 3, p) : Fb;
+    const double diff = -eta * wt_g_prime(eta, s.mu) * (Fa.x * Fb.x + Fa.y * Fb.y);
+    sym_add(acc + SC_WT, g, diff / q2);
+    acc[SC_WTTR] += diff;
+  }
   // ion-electron
   if (sa.nion > 0) {
     double vp[MAX_SPECIES];

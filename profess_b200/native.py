@@ -349,7 +349,7 @@ class Engine:
         """RescaleDensity of the held input density to num_electrons."""
         self._check(self.lib.ofdft_slot_rescale_input(self.h, slot, float(num_electrons)))
 
-    STRESS_TERMS = ("TF", "vW", "WT", "Hartree", "LDA", "ion-electron", "Ewald")
+    STRESS_TERMS = ("TF", "vW", "nonlocal", "Hartree", "LDA", "ion-electron", "Ewald")
 
     def stress(self, slot, rho=None, include_ewald=True, terms=False):
         """Stress tensor (3, 3) in Ha/bohr^3 of rho (or the slot's solved

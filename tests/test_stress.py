@@ -2,7 +2,8 @@
 CalculateStress restatement on the same density: the optCell Al4 cell (a
 sheared lattice, so the off-diagonal and Nyquist terms are exercised) and a
 larger synthetic fcc cell; both the given-density and the resident-density
-forms, and that the call leaves the slot's solve record as it was."""
+forms, and that the call leaves the slot's solve record as it was; and the
+second-order WGC functional's stress on a strained WGC Al4 cell."""
 import numpy as np
 import pytest
 
@@ -88,7 +89,7 @@ def test_stress_on_fcc_on_gpu(gpu_engine, grid):
     check_stress_on_fcc(gpu_engine, grid=grid)
 
 
-def test_stress_needs_ions_and_the_wt_functional(emu_engine):
+def test_stress_needs_ions(emu_engine):
     c = wl.fcc_al((1, 1, 1), sigma_ang=0.0, grid=(16, 16, 16), seed=0)
     rho = np.full(c.grid, c.num_electrons / c.vol)
     s = pcell._create(emu_engine, c, native.FP64, 0.0)
@@ -98,10 +99,39 @@ def test_stress_needs_ions_and_the_wt_functional(emu_engine):
             emu_engine.stress(s, rho=rho)
     finally:
         emu_engine.slot_destroy(s)
-    g = wl.fcc_al((1, 1, 1), sigma_ang=0.0, grid=(16, 16, 16), seed=0, kinetic=native.KEDF_WGC)
-    s = pcell.setup_slot(emu_engine, g, native.FP64)
+
+
+def check_wgc_stress_matches_oracle(eng, grid=(16, 16, 16), prec=native.FP64, tol=1e-10):
+    """The second-order WGC stress (WGCStress) on a strained WGC Al4 cell."""
+    cell0, f0, _, c = cases.golden_case("wgc_al4_fcc")
+    strain = np.array([[0.02, 0.01, 0.0], [0.01, -0.01, 0.0], [0.0, 0.0, 0.015]])
+    lat = (np.eye(3) + strain) @ cell0.lattice
+    oc = cases.cs.Cell(lattice=lat, frac=cell0.frac, species_of_ion=cell0.species_of_ion, species=cell0.species)
+    f = cases.functional_for(oc, grid, cases.fn.KEDF_WGC, c["alpha"], c["beta"], c["lambda"], c["mu"],
+                             c.get("gamma", 2.7))
+    z = np.load(cases.GOLDEN + "/al_hc_recpot.npz")
+    sp = recpot.species_from_table(float(z["max_g"]), z["values"], "Al")
+    wc = wl.Cell(name="wgc", lattice=lat, frac=cell0.frac, species_of_ion=cell0.species_of_ion, species=[sp],
+                 grid=tuple(grid), kinetic=native.KEDF_WGC, alpha=c["alpha"], beta=c["beta"],
+                 gamma=c.get("gamma", 2.7))
+    s = pcell.setup_slot(eng, wc, prec)
     try:
-        with pytest.raises(native.OfdftError, match="WT functional"):
-            emu_engine.stress(s, rho=rho)
+        rho = cases.random_density(grid, oc.num_electrons, oc.vol, seed=9, amp=0.2)
+        got, parts = eng.stress(s, rho=rho, terms=True)
+        ref = ost.stress(oc, f, rho, gamma=c.get("gamma", 2.7))
+        assert np.abs(got - ref).max() < tol, np.abs(got - ref).max()
+        assert np.abs(parts["nonlocal"]).max() > 1e-6
     finally:
-        emu_engine.slot_destroy(s)
+        eng.slot_destroy(s)
+
+
+def test_wgc_stress_matches_oracle(emu_engine):
+    check_wgc_stress_matches_oracle(emu_engine)
+    check_wgc_stress_matches_oracle(emu_engine, prec=native.FP32, tol=5e-9)
+
+
+@pytest.mark.gpu
+def test_wgc_stress_matches_oracle_on_gpu(gpu_engine):
+    check_wgc_stress_matches_oracle(gpu_engine)
+    check_wgc_stress_matches_oracle(gpu_engine, grid=(32, 30, 36))
+    check_wgc_stress_matches_oracle(gpu_engine, prec=native.FP32, tol=5e-9)

@@ -24,7 +24,7 @@ LIB_PATH = os.path.join(LIB_DIR, "libprofess_b200.so")
 EMU_PATH = os.path.join(EMU_DIR, "libprofess_b200_emu.so")
 
 SOURCES = ["engine.cu"]
-HEADERS = ["cx.cuh", "fft.cuh", "dcsrch.cuh", "slot.cuh", "ntn_ctl.cuh", "passes.cuh", "setup.cuh", "ewald.cuh"]
+HEADERS = ["cx.cuh", "fft.cuh", "dcsrch.cuh", "slot.cuh", "ntn_ctl.cuh", "passes.cuh", "setup.cuh", "ewald.cuh", "stress.cuh"]
 
 NVCC_FLAGS = [
     "-O3", "-std=c++17", "-lineinfo",

@@ -320,7 +320,7 @@ template <typename S, typename D> __global__ void __launch_bounds__(256) k_conve
     dst[i] = (D)src[i];
 }
 template <typename T> __global__ void __launch_bounds__(64) k_ctl(Args<T> a, int kid) {
-  __shared__ double sm[NCH * 33 + 2];
+  __shared__ double sm[CTL_SMEM_BYTES / sizeof(double)];
   ctl_block(a.slots, a.ctl, a.tasks, kid, blockIdx.x, threadIdx.x, blockDim.x, (char*)sm);
 }
 #endif
@@ -1940,7 +1940,7 @@ struct Engine {
       Args<T> a = args<T>(prec, pass);
       for (int b = 0; b < (int)l.h.size(); ++b) fn(a, b, emu_smem.data());
     };
-    static double ctl_sm[NCH * 33 + 2];
+    static double ctl_sm[CTL_SMEM_BYTES / sizeof(double)];
     for (int v = 0; v < VEC_PER_TICK; ++v) {
       run(P_VEC, [](Args<T>& a, int b, char* sm) { vec_block<T>(a, b, 0, 1, sm); });
       run(P_CTL, [](Args<T>& a, int b, char*) { ctl_block(a.slots, a.ctl, a.tasks, K_VEC, b, 0, 1, (char*)ctl_sm); });

@@ -16,6 +16,14 @@ namespace ofdft {
 
 HD bool bad(double v) { return !(v == v) || v > 1.0e300 || v < -1.0e300; }
 
+// The slot quantities the state machine reads, loaded once before it runs.
+struct CtlSlot {
+  double dv, ion_ion;
+  long long N;
+  HistEntry* hist;
+};
+HD CtlSlot ctl_slot(const SlotDev& s) { return CtlSlot{s.dv, s.ion_ion, s.N, s.hist}; }
+
 HDNI inline void ctl_finish(Ctl& c, int status, int err) {
   c.status = status;
   c.error = err;
@@ -23,7 +31,7 @@ HDNI inline void ctl_finish(Ctl& c, int status, int err) {
   c.ev = EV_NONE;
 }
 
-HDNI inline void ctl_push_hist(Ctl& c, const SlotDev& s, int ncg, int nline) {
+HDNI inline void ctl_push_hist(Ctl& c, const CtlSlot& s, int ncg, int nline) {
   if (c.hist_n < HIST_MAX && s.hist != nullptr) {
     HistEntry& h = s.hist[c.hist_n];
     h.energy = c.energy[0];
@@ -36,7 +44,7 @@ HDNI inline void ctl_push_hist(Ctl& c, const SlotDev& s, int ncg, int nline) {
 }
 
 // Energy table from the reduced energy densities (CalculateEnergy, CalPotential.f90:610-644).
-HDNI inline void ctl_energy(Ctl& c, const SlotDev& s, const double* red) {
+HDNI inline void ctl_energy(Ctl& c, const CtlSlot& s, const double* red) {
   double loc[9] = {0, 0, red[CH_EIE], red[CH_EH], red[CH_EXC], 0, red[CH_ETF], red[CH_EVW], red[CH_ENL]};
   loc[1] = loc[6] + loc[7] + loc[8];
   for (int i = 0; i < 9; ++i) c.energy[i] = loc[i] * s.dv;
@@ -67,7 +75,7 @@ HDNI inline void ctl_cg_eval(Ctl& c) {
 
 // getNextGradient first half (RhoLineSearch.f90:88-96) once sum (phi+d)^2 and
 // sum phi.d are known.
-HDNI inline void ctl_next_gradient(Ctl& c, const SlotDev& s) {
+HDNI inline void ctl_next_gradient(Ctl& c, const CtlSlot& s) {
   c.norm_phi_dir = sqrt(c.s_phid2 * s.dv);
   ctl_op(c, OP_NG2, c.s_phid * s.dv / c.tot_ele);
 }
@@ -80,7 +88,7 @@ HDNI inline void ctl_ls_trial(Ctl& c) {
 
 // Accept the line-search result: StepInformation, CheckExit, phi = tempPhi,
 // ChemicalPotential and dL/dphi (RhoOptN.f90:603-630).
-HDNI inline void ctl_accept(Ctl& c, const SlotDev& s, const double* red) {
+HDNI inline void ctl_accept(Ctl& c, const CtlSlot& s, const double* red) {
   const double npts = (double)s.N;
   c.pot_norm = sqrt(red[CH_M1] / npts);  // StepInformation uses the old mu
   ctl_push_hist(c, s, c.cg_iter, c.nline);
@@ -113,7 +121,7 @@ HDNI inline void ctl_accept(Ctl& c, const SlotDev& s, const double* red) {
 
 // Called after a vector op (kid = K_VEC, what = op) or an evaluation
 // (kid = K_X5, what = eval mode) with the slot's reduced sums.
-HDNI inline void ntn_after(Ctl& c, const SlotDev& s, const double* red, int kid, int what) {
+HDNI inline void ntn_after(Ctl& c, const CtlSlot& s, const double* red, int kid, int what) {
   for (int i = 0; i < NCH; ++i)
     if (bad(red[i])) { ctl_finish(c, ST_ERROR, ERR_NAN); return; }
   if (kid == K_X5) {

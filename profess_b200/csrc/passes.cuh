@@ -141,10 +141,26 @@ HDNI inline void store_partials(SlotDev& s, int task_idx, const double* acc, dou
   }
 }
 
+// Shared memory of the controller block: the reduction scratch, then a copy
+// of the slot's controller record.
+constexpr size_t CTL_SRED_BYTES = (NCH * 33 + 2) * sizeof(double);
+constexpr size_t CTL_SMEM_BYTES = CTL_SRED_BYTES + sizeof(Ctl);
+static_assert(sizeof(Ctl) % 8 == 0, "the controller record is copied as 8-byte words");
+
+// Copy nbytes (a multiple of 8) as 8-byte words spread over the block.
+HDNI inline void copy_words(void* dst, const void* src, size_t nbytes, int tid, int nthr) {
+  unsigned long long* d = (unsigned long long*)dst;
+  const unsigned long long* s = (const unsigned long long*)src;
+  for (int w = tid; w < (int)(nbytes / 8); w += nthr) d[w] = s[w];
+}
+
 // Controller kernel body, one block per running slot: reduce the partials
 // of the work kernel that just ran (in a fixed order, independent of block
 // scheduling) and advance the slot's NTN state machine.  kid = K_VEC after the
-// vector kernel, K_X5 after pass 5.
+// vector kernel, K_X5 after pass 5.  The block copies the controller record
+// into shared memory with all its threads; the one thread that runs the
+// state machine reads and writes only the fields it needs there, and the
+// block writes the record back.
 HDNI inline void ctl_block(SlotDev* slots, Ctl* ctls, const Task* tasks, int kid, int bid, int tid, int nthr,
                            char* smem) {
   const int si = tasks[bid].slot;
@@ -154,6 +170,9 @@ HDNI inline void ctl_block(SlotDev* slots, Ctl* ctls, const Task* tasks, int kid
   const int what = kid == K_VEC ? c.op : c.ev;
   if (what == 0) return;
   double* sred = (double*)smem;
+  Ctl* cs = (Ctl*)(smem + CTL_SRED_BYTES);
+  copy_words(cs, &c, sizeof(Ctl), tid, nthr);
+  const CtlSlot sl = ctl_slot(s);
   const int nt = s.ntask[kid];
   double part[NCH];
 #pragma unroll
@@ -162,15 +181,15 @@ HDNI inline void ctl_block(SlotDev* slots, Ctl* ctls, const Task* tasks, int kid
 #pragma unroll
     for (int ch = 0; ch < NCH; ++ch) part[ch] += s.partials[(size_t)t * NCH + ch];
   }
-  block_reduce(sred, part, tid, nthr);
+  block_reduce(sred, part, tid, nthr);  // its barriers also publish the copy
   if (tid == 0) {
     double red[NCH];
 #pragma unroll
     for (int ch = 0; ch < NCH; ++ch) red[ch] = sred[ch];
-    Ctl local = c;
-    ntn_after(local, s, red, kid, what);
-    c = local;
+    ntn_after(*cs, sl, red, kid, what);
   }
+  BLOCK_SYNC();
+  copy_words(&c, cs, sizeof(Ctl), tid, nthr);
 }
 
 // ------------------------------------------------------------ vector ops

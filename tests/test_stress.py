@@ -125,6 +125,32 @@ def check_wgc_stress_matches_oracle(eng, grid=(16, 16, 16), prec=native.FP64, to
         eng.slot_destroy(s)
 
 
+def check_wgc_stress_on_hcp(eng, grid=(16, 16, 24), prec=native.FP64, tol=1e-10):
+    """WGC stress on a non-orthogonal (120 degree) hcp Mg cell of the product
+    set-up path (Heine-Abarenkov Mg, rho0 = rho* = N/V)."""
+    c = wl.hcp_mg((2, 2, 2), sigma_ang=0.05, grid=grid, seed=3)
+    assert c.kinetic == native.KEDF_WGC
+    oc, f = cases.workload_functional(c)
+    s = pcell.setup_slot(eng, c, prec)
+    try:
+        rho = cases.random_density(grid, c.num_electrons, c.vol, seed=5, amp=0.2)
+        got = eng.stress(s, rho=rho)
+        ref = ost.stress(oc, f, rho, gamma=c.gamma)
+        assert np.abs(got - ref).max() < tol, np.abs(got - ref).max()
+        assert abs(got[0, 1]) > 1e-7  # the 120 degree cell has shear terms
+    finally:
+        eng.slot_destroy(s)
+
+
+def test_wgc_stress_on_hcp(emu_engine):
+    check_wgc_stress_on_hcp(emu_engine)
+
+
+@pytest.mark.gpu
+def test_wgc_stress_on_hcp_on_gpu(gpu_engine):
+    check_wgc_stress_on_hcp(gpu_engine, grid=(24, 24, 40))
+
+
 def test_wgc_stress_matches_oracle(emu_engine):
     check_wgc_stress_matches_oracle(emu_engine)
     check_wgc_stress_matches_oracle(emu_engine, prec=native.FP32, tol=5e-9)

@@ -385,6 +385,13 @@ struct Engine {
   int d2h_stream(void* h, const void* d, size_t n) { return d2h(h, d, n); }
 #else
   cudaStream_t stream = nullptr;
+  // A captured graph of ticks with running slots of both precisions forks
+  // into an FP64 and an FP32 branch (the two share no slot, task list or
+  // table they write): stream2 carries the FP32 branch during the capture,
+  // and lstream is the stream the tick launches go to.
+  cudaStream_t stream2 = nullptr;
+  cudaStream_t lstream = nullptr;
+  cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
   cudaGraphExec_t graph_exec = nullptr;
   int graph_ticks = 0;
   int d2h_stream(void* h, const void* d, size_t n) {
@@ -428,6 +435,10 @@ struct Engine {
 #if !defined(OFDFT_EMU)
     int rs = cuda_check(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking), "stream create");
     if (rs) return rs;
+    if ((rs = cuda_check(cudaStreamCreateWithFlags(&stream2, cudaStreamNonBlocking), "stream create"))) return rs;
+    if ((rs = cuda_check(cudaEventCreateWithFlags(&ev_fork, cudaEventDisableTiming), "event create"))) return rs;
+    if ((rs = cuda_check(cudaEventCreateWithFlags(&ev_join, cudaEventDisableTiming), "event create"))) return rs;
+    lstream = stream;
     int dev = 0;
     if ((rs = cuda_check(cudaGetDevice(&dev), "get device"))) return rs;
     if ((rs = cuda_check(cudaDeviceGetAttribute(&num_sms, cudaDevAttrMultiProcessorCount, dev), "SM count"))) return rs;
@@ -460,7 +471,11 @@ struct Engine {
     dfree(d_io);
     d_io = nullptr;
     if (stream) cudaStreamDestroy(stream);
-    stream = nullptr;
+    if (stream2) cudaStreamDestroy(stream2);
+    if (ev_fork) cudaEventDestroy(ev_fork);
+    if (ev_join) cudaEventDestroy(ev_join);
+    stream = stream2 = lstream = nullptr;
+    ev_fork = ev_join = nullptr;
 #endif
   }
 
@@ -1963,7 +1978,7 @@ struct Engine {
   int launch_one(int prec, int pass, K kern, X... extra) {
     LaunchList& l = lists[prec][pass];
     if (l.h.empty()) return OFDFT_OK;
-    kern<<<(unsigned)l.h.size(), l.nthr, l.smem, stream>>>(args<T>(prec, pass), extra...);
+    kern<<<(unsigned)l.h.size(), l.nthr, l.smem, lstream>>>(args<T>(prec, pass), extra...);
     return cuda_check(cudaGetLastError(), "kernel launch");
   }
   template <typename T>
@@ -1991,6 +2006,11 @@ struct Engine {
     int rc;
     if ((rc = launch_prec<double>(OFDFT_FP64))) return rc;
     return launch_prec<float>(OFDFT_FP32);
+  }
+  bool has_work(int prec) const {
+    for (int k = 0; k < NPASS; ++k)
+      if (!lists[prec][k].h.empty()) return true;
+    return false;
   }
 
 #if !defined(OFDFT_EMU)
@@ -2084,7 +2104,21 @@ struct Engine {
     if (rc) return rc;
     if ((rc = cuda_check(cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal), "begin capture")))
       return rc;
-    for (int k = 0; k < nticks && rc == OFDFT_OK; ++k) rc = tick();
+    if (!(has_work(OFDFT_FP64) && has_work(OFDFT_FP32))) {
+      for (int k = 0; k < nticks && rc == OFDFT_OK; ++k) rc = tick();
+    } else {  // one branch per precision
+      rc = cuda_check(cudaEventRecord(ev_fork, stream), "event record");
+      if (!rc) rc = cuda_check(cudaStreamWaitEvent(stream2, ev_fork, 0), "stream wait");
+      if (!rc) {
+        for (int k = 0; k < nticks && rc == OFDFT_OK; ++k) rc = launch_prec<double>(OFDFT_FP64);
+        lstream = stream2;
+        for (int k = 0; k < nticks && rc == OFDFT_OK; ++k) rc = launch_prec<float>(OFDFT_FP32);
+        lstream = stream;
+        const int rj = cuda_check(cudaEventRecord(ev_join, stream2), "event record");
+        const int rw = cuda_check(cudaStreamWaitEvent(stream, ev_join, 0), "stream wait");
+        if (!rc) rc = rj ? rj : rw;
+      }
+    }
     cudaGraph_t g = nullptr;
     const int rc2 = cuda_check(cudaStreamEndCapture(stream, &g), "end capture");
     if (rc) { if (g) cudaGraphDestroy(g); return rc; }

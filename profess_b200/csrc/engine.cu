@@ -234,7 +234,10 @@ template <> struct PassMinBlocks<double> { static constexpr int value = OFDFT_MI
 #ifndef OFDFT_XINV_MINB_FP64
 #define OFDFT_XINV_MINB_FP64 3
 #endif
-template <typename T> struct XinvMinBlocks { static constexpr int value = OFDFT_MINB_FP32; };
+#ifndef OFDFT_XINV_MINB_FP32
+#define OFDFT_XINV_MINB_FP32 OFDFT_MINB_FP32
+#endif
+template <typename T> struct XinvMinBlocks { static constexpr int value = OFDFT_XINV_MINB_FP32; };
 template <> struct XinvMinBlocks<double> { static constexpr int value = OFDFT_XINV_MINB_FP64; };
 
 #if !defined(OFDFT_EMU)

@@ -892,13 +892,16 @@ struct Engine {
   }
 
   // Run a slot that needs a single evaluation tick (the ion-potential and
-  // force set-up passes, which take the split y/z path).
+  // force set-up passes, which take the split y/z path).  The tick advances
+  // every running slot; it is repeated (up to 4 times) only while this slot
+  // has not finished, so the other solves are not held in un-graphed ticks.
   int run_one(int i) {
     slots[i].running = true;
     slots[i].setup_pass = true;
     dirty = true;
     int running = 0;
-    int rc = run(4, &running, 1);
+    int rc = OFDFT_OK;
+    for (int t = 0; t < 4 && slots[i].running && rc == OFDFT_OK; ++t) rc = run(1, &running, 1);
     slots[i].setup_pass = false;
     dirty = true;
     if (rc) return rc;

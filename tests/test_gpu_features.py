@@ -1,6 +1,7 @@
 """CUDA engine features against the oracle (GPU): device set-up of kernels
 and ion potential, spline forces, large FFT plans, the product set-up path on
-a synthetic workload cell, mixed precision, batch invariance, serving."""
+a synthetic workload cell, mixed precision, batch invariance (one precision,
+and both precisions in concurrent graph branches), serving."""
 import numpy as np
 import pytest
 
@@ -138,6 +139,35 @@ def test_batch_invariance_on_gpu(gpu_engine):
             rb, eb, stb = gpu_engine.result(s)
             assert np.array_equal(eb, a[1]) and np.array_equal(rb, a[0])
             assert stb["num_evals"] == a[2]["num_evals"]
+    finally:
+        for s in slots:
+            gpu_engine.slot_destroy(s)
+
+
+def test_two_precisions_in_one_graph_match_alone(gpu_engine):
+    """FP64 and FP32 slots running together take two concurrent branches of
+    the engine's graphs; each solve must give bit for bit what it gives with
+    its precision running alone (one branch).  One FP32 cell is WGC (split y/z
+    path), the others WT (fused y-z pass)."""
+    cells = [wl.fcc_al((1, 1, 1), sigma_ang=0.05, grid=(24, 24, 24), seed=i) for i in range(3)]
+    cells.append(wl.fcc_al((1, 1, 2), sigma_ang=0.05, grid=(24, 24, 48), seed=7, kinetic=5))
+    cells[-1].alpha, cells[-1].beta = (5 + 5 ** 0.5) / 6, (5 - 5 ** 0.5) / 6
+    precs = [native.FP64, native.FP32, native.FP64, native.FP32]
+    o64 = native.ntn_options(conv_check=native.CONV_POT, pot_tol=1e-6, max_iter=300)
+    o32 = native.ntn_options(conv_check=native.CONV_POT, pot_tol=3e-5, max_iter=300, stall_line=6)
+    opts = [o64 if p == native.FP64 else o32 for p in precs]
+    slots = [pcell.setup_slot(gpu_engine, c, p) for c, p in zip(cells, precs)]
+    try:
+        rho = [wl.initial_density(c, seed=i) for i, c in enumerate(cells)]
+        alone = [gpu_engine.proj_norm_rho_minimization(s, r, o) for s, r, o in zip(slots, rho, opts)]
+        for s, r, o in zip(slots, rho, opts):
+            gpu_engine.start_solve(s, r, o)
+        while gpu_engine.run(8):
+            pass
+        for s, a in zip(slots, alone):
+            rb, eb, stb = gpu_engine.result(s)
+            assert np.array_equal(eb, a[1]) and np.array_equal(rb, a[0])
+            assert stb["num_evals"] == a[2]["num_evals"] and stb["outcome"] == a[2]["outcome"]
     finally:
         for s in slots:
             gpu_engine.slot_destroy(s)

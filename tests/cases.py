@@ -83,7 +83,6 @@ def random_density(n, ne, vol, seed=0, amp=0.3):
 
 def engine_slot(eng, f, cell, precision=0):
     """Create a slot for oracle functional ``f`` and upload its tables."""
-    from profess_b200 import native
     s = eng.slot_create(f.n, cell.lattice, kinetic=f.kinetic, lam=f.lam, mu=f.mu, alpha=f.alpha, beta=f.beta,
                         rho0=0.0, rho_s=f.rho_s, ion_ion=f.ion_ion, precision=precision)
     eng.set_kernel(s, f.kernel)

@@ -8,7 +8,7 @@ import pytest
 import cases
 from oracle import cellopt, ntn
 from oracle.consts import BOHR, HARTREE_TO_EV
-from profess_b200 import native, recpot, relax, workloads as wl
+from profess_b200 import recpot, relax, workloads as wl
 
 
 def test_oracle_cell_relax_follows_the_reference():

@@ -5,7 +5,6 @@ gathered on rank 0."""
 import os
 import socket
 
-import pytest
 import torch.multiprocessing as mp
 
 

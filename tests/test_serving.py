@@ -4,7 +4,7 @@ request's result is the same alone and in the mix."""
 import numpy as np
 import pytest
 
-from profess_b200 import native, serving, workloads as wl
+from profess_b200 import serving, workloads as wl
 
 
 def small_cell(seed, kinetic=4):

@@ -20,8 +20,12 @@ TOLS = 5.0e-7         # CellOptimizers.f90: tols (Ha/bohr^3)
 
 
 def steepest_descent(cell, n, opts: ntn.NtnOptions, max_steps=MAX_CELL_STEP, tols=TOLS, axis=0,
-                     alpha_=5.0 / 6.0, beta_=5.0 / 6.0):
-    """Returns (final lattice, [(energy (Ha), stress, lattice) per cell step])."""
+                     alpha_=5.0 / 6.0, beta_=5.0 / 6.0, kinetic=None, gamma=2.7):
+    """Returns (final lattice, [(energy (Ha), stress, lattice) per cell step]).
+    kinetic = KEDF_WGC relaxes with the second-order WGC functional (its
+    kernel rebuilt at the new N/V after each move, and WGCStress)."""
+    from . import functional as fn
+    kinetic = fn.KEDF_WT if kinetic is None else kinetic
     from . import cellsetup as cs
     cell = dataclasses.replace(cell, frac=np.array(cell.frac, dtype=float),
                                lattice=np.array(cell.lattice, dtype=float))
@@ -34,11 +38,11 @@ def steepest_descent(cell, n, opts: ntn.NtnOptions, max_steps=MAX_CELL_STEP, tol
         i += 1
         if i > max_steps:
             break
-        f = functional_for(cell, n, alpha_, beta_)  # RefreshCellSetup: kernel (rho0 = N/V), ions, Ewald
+        f = functional_for(cell, n, alpha_, beta_, kinetic, gamma)  # RefreshCellSetup: kernel (rho0 = N/V), ions, Ewald
         r = ntn.NtnSolver(f, opts).solve(rho)
         rho = r.rho
         energy = float(r.energy[0])
-        stress = ost.stress(cell, f, rho)
+        stress = ost.stress(cell, f, rho, gamma=gamma)
         trace.append((energy, stress.copy(), cell.lattice.copy()))
         if axis in (1, 2, 3):
             keep = stress[axis - 1, axis - 1]

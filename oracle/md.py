@@ -36,17 +36,29 @@ def atomic_mass(symbol: str) -> float:
     return _WEIGHT[symbol] / (_MOL * _EMASS)
 
 
-def functional_for(cell: cs.Cell, n, alpha: float, beta: float) -> fn.Functional:
-    """The WT functional of ``cell`` on grid n with the B-spline ion potential
-    and the Ewald energy of its current positions (RefreshIonTerms,
-    Source/RefreshIons.f90:125-238)."""
+_WGC_TABS = {}
+
+
+def functional_for(cell: cs.Cell, n, alpha: float, beta: float, kinetic: int = fn.KEDF_WT,
+                   gamma: float = 2.7) -> fn.Functional:
+    """The WT (or second-order WGC) functional of ``cell`` on grid n, its
+    kernel built at rho0 = rho* = N/V, with the B-spline ion potential and the
+    Ewald energy of its current positions (RefreshIonTerms,
+    Source/RefreshIons.f90:125-238).  The WGC radial tables depend only on
+    (alpha, beta, gamma) and are integrated once."""
     n = tuple(int(x) for x in n)
     qt = cs.q_table(cell.recip, *n)
     rho_avg = cell.num_electrons / cell.vol
-    kern = kk.wt_kernel(qt, rho_avg, alpha, beta, 1.0, 1.0)[None]
+    if kinetic == fn.KEDF_WT:
+        kern = kk.wt_kernel(qt, rho_avg, alpha, beta, 1.0, 1.0)[None]
+    else:
+        key = (float(alpha), float(beta), float(gamma))
+        if key not in _WGC_TABS:
+            _WGC_TABS[key] = kk.wgc_radial_tables(alpha, beta, gamma)
+        kern = kk.wgc_kernels(qt, rho_avg, gamma, _WGC_TABS[key])
     vion = cs.ion_potential_real(cell, *n)
     e_ii, _ = ew.ewald(cell.lattice, cell.frac, cell.charges())
-    return fn.Functional(kinetic=fn.KEDF_WT, n=n, dv=cell.vol / float(np.prod(n)), qtab=qt, kernel=kern,
+    return fn.Functional(kinetic=kinetic, n=n, dv=cell.vol / float(np.prod(n)), qtab=qt, kernel=kern,
                          ion_pot=vion, ion_ion=e_ii, lam=1.0, mu=1.0, alpha=alpha, beta=beta, rho_s=rho_avg)
 
 
@@ -163,12 +175,13 @@ def run_nvt(cell: cs.Cell, n, vel0: np.ndarray, dt: float, nsteps: int, opts: nt
 
 def run_npt(cell: cs.Cell, n, vel0: np.ndarray, dt: float, nsteps: int, opts: ntn.NtnOptions, q_mass: float,
             b_mass: float, temperature_ha: float, ext_pres: float, n_resn: int = 3, n_yosh: int = 3,
-            alpha: float = 5.0 / 6.0, beta: float = 5.0 / 6.0):
+            alpha: float = 5.0 / 6.0, beta: float = 5.0 / 6.0, kinetic: int = fn.KEDF_WT, gamma: float = 2.7):
     """Full-cell NPT, NPTFullCell / MVV / NPTFullCell_Integrator / NPTFullCell_Conserved
     (Source/MolecularDynamicsNPT.f90:76-274, 275-411, 413-640, 691-790), no box
     constraint and no frozen ions.  Velocities are held (3, numIon) as in the
-    reference.  Returns the list of (lattice, frac, energy, conserved, volume)
-    after the first solve and after each step."""
+    reference.  kinetic = KEDF_WGC runs the second-order WGC functional.
+    Returns the list of (lattice, frac, energy, conserved, volume) after the
+    first solve and after each step."""
     from . import stress as ost
     cell = dataclasses.replace(cell, frac=np.array(cell.frac, dtype=float), lattice=np.array(cell.lattice, float))
     mass = np.array([atomic_mass(cell.species[s].name) for s in cell.species_of_ion])
@@ -186,10 +199,10 @@ def run_npt(cell: cs.Cell, n, vel0: np.ndarray, dt: float, nsteps: int, opts: nt
     vbox = np.zeros((3, 3))
 
     def refresh_and_solve(rho):
-        f = functional_for(cell, n, alpha, beta)
+        f = functional_for(cell, n, alpha, beta, kinetic, gamma)
         r = ntn.NtnSolver(f, opts).solve(rho)
         forces, _, _ = ofo.total_forces(cell, r.rho)
-        return r.rho, float(r.energy[0]), forces, ost.stress(cell, f, r.rho)
+        return r.rho, float(r.energy[0]), forces, ost.stress(cell, f, r.rho, gamma=gamma)
 
     rho, energy, forces, stress = refresh_and_solve(cs.uniform_density(cell, *n))
 

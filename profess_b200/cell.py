@@ -29,6 +29,17 @@ def wgc_tables(lib, alpha: float, beta: float, gamma: float):
     return _WGC_TABLES[key]
 
 
+def build_kernel(eng: native.Engine, slot: int, cell: Cell) -> None:
+    """Build the slot's kinetic kernel on the device at its current rho0 and
+    rho* (WT: the LindG kernel; second-order WGC: the kernel planes from the
+    radial tables of (alpha, beta, gamma)), as RefreshCellSetup does after a
+    lattice change."""
+    if cell.kinetic == native.KEDF_WT:
+        eng.build_wt_kernel(slot)
+    else:
+        eng.build_wgc_kernel(slot, wgc_tables(eng.lib, cell.alpha, cell.beta, cell.gamma))
+
+
 def _create(eng: native.Engine, cell: Cell, precision, ion_ion) -> int:
     rho_avg = cell.num_electrons / cell.vol
     return eng.slot_create(cell.grid, cell.lattice, kinetic=cell.kinetic, alpha=cell.alpha, beta=cell.beta,
@@ -53,10 +64,7 @@ def setup_slot(eng: native.Engine, cell: Cell, precision=native.FP64, ion_ion=No
     device; the Ewald energy is summed on the device unless ``ion_ion`` gives it."""
     s = _create(eng, cell, precision, 0.0 if ion_ion is None else ion_ion)
     try:
-        if cell.kinetic == native.KEDF_WT:
-            eng.build_wt_kernel(s)
-        else:
-            eng.build_wgc_kernel(s, wgc_tables(eng.lib, cell.alpha, cell.beta, cell.gamma))
+        build_kernel(eng, s, cell)
         eng.build_ion_potential(s, cell.frac, cell.species_of_ion, cell.species)
         if ion_ion is None:
             eng.ewald(s, cell.nion, want_forces=False)

@@ -288,11 +288,11 @@ class NPT(NVE):
     (``q_mass``) and a barostat (``b_mass``) at external pressure ``ext_pres``
     (Ha/bohr^3).  Each step: NPTFullCell_Integrator over a half step, MVV
     (a half kick, the positions and the lattice propagated by the barostat
-    velocity, RefreshCellSetup on the device: new lattice, WT kernel, ion
+    velocity, RefreshCellSetup on the device: new lattice, kinetic kernel, ion
     potential and Ewald sum; RescaleDensity of the held density; the density
     solves of all replicas together; forces, stress and a half kick), and the
     integrator again.  The stress is the device stress of each new density.
-    WT functional only."""
+    WT or second-order WGC cells."""
 
     def __init__(self, eng, cells, dt: float, q_mass: float, b_mass: float, temperature_k: float,
                  ext_pres: float, velocities=None, seed: int = 0, opts=None, rho0=None, n_resn: int = 3,
@@ -390,7 +390,7 @@ class NPT(NVE):
             rho_avg = c.num_electrons / c.vol
             self.eng.set_lattice(r.slot, lat, rho_avg, rho_avg)
             self.eng.rescale_input(r.slot, c.num_electrons)
-            self.eng.build_wt_kernel(r.slot)
+            pcell.build_kernel(self.eng, r.slot, c)
             self.eng.build_ion_potential(r.slot, c.frac, c.species_of_ion, c.species)
             self._refresh_ewald(r)
             self.eng.start_solve(r.slot, None, self.opts)

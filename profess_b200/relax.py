@@ -818,9 +818,10 @@ class CellRelax:
     energy and /4 after a higher one; it stops when max |sigma| < tols
     (5e-7 Ha/bohr^3) or after max_steps.  axis 1-3 relaxes one diagonal
     component only.  A lattice move runs RefreshCellSetup and RescaleDensity
-    on the device (ofdft_slot_set_lattice, the WT kernel, ion potential and
+    on the device (ofdft_slot_set_lattice, the kinetic kernel, ion potential and
     Ewald rebuilt, ofdft_slot_rescale_input), and the next solve starts from
-    the held density.  All cells' solves run together.  WT functional."""
+    the held density.  All cells' solves run together.  WT or second-order
+    WGC cells (the kernel rebuilt at the new N/V; WTStress or WGCStress)."""
 
     def __init__(self, eng: native.Engine, cells, max_steps: int = CELL_MAX_STEPS, tols: float = CELL_TOLS,
                  axis: int = 0, opts=None):
@@ -877,7 +878,7 @@ class CellRelax:
         rho_avg = c.num_electrons / c.vol
         self.eng.set_lattice(st.slot, new, rho_avg, rho_avg)
         self.eng.rescale_input(st.slot, c.num_electrons)
-        self.eng.build_wt_kernel(st.slot)
+        pcell.build_kernel(self.eng, st.slot, c)
         self.eng.build_ion_potential(st.slot, c.frac, c.species_of_ion, c.species)
         self.eng.ewald(st.slot, c.nion, want_forces=False)
         self.eng.start_solve(st.slot, None, self.opts)

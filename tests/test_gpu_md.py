@@ -17,3 +17,8 @@ def test_nvt_matches_oracle_on_gpu(gpu_engine):
 def test_npt_matches_oracle_on_gpu(gpu_engine):
     from test_md import check_npt_matches_oracle
     check_npt_matches_oracle(gpu_engine)
+
+
+def test_npt_wgc_matches_oracle_on_gpu(gpu_engine):
+    from test_md import check_npt_matches_oracle
+    check_npt_matches_oracle(gpu_engine, nsteps=2, wgc=True)

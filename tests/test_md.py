@@ -4,6 +4,7 @@ build (CPU); test_gpu_md.py repeats them on the CUDA build."""
 import numpy as np
 
 from oracle import cellsetup as cs
+from oracle import functional as fn
 from oracle import md as omd
 from oracle import ntn
 from profess_b200 import md, native, workloads as wl
@@ -116,11 +117,17 @@ def test_yoshida_weights_sum_to_one():
 NPT_Q, NPT_B, NPT_P = 2.0e3, 2.0e5, 1.0e-5
 
 
-def check_npt_matches_oracle(eng, nsteps=3):
+def check_npt_matches_oracle(eng, nsteps=3, wgc=False):
     """Full-cell NPT (NPTFullCell) on the engine, with the device stress and
     the device lattice refresh, against the oracle's restatement: the same
-    lattice, positions, energy and conserved quantity after every step."""
+    lattice, positions, energy and conserved quantity after every step.  With
+    wgc, the cell runs the second-order WGC functional (its kernel rebuilt
+    on the device after every lattice move, WGCStress)."""
     c, ocell = _cells()
+    extra = {}
+    if wgc:
+        c.kinetic, c.alpha, c.beta = native.KEDF_WGC, (5 + 5 ** 0.5) / 6, (5 - 5 ** 0.5) / 6
+        extra = dict(alpha=c.alpha, beta=c.beta, kinetic=fn.KEDF_WGC, gamma=c.gamma)
     v0 = md.initial_velocities(c, 600.0, seed=4)
     opts = native.ntn_options(conv_check=native.CONV_POT, pot_tol=1.0e-6)
     run = md.NPT(eng, [c], DT, NPT_Q, NPT_B, 600.0, NPT_P, velocities=[v0], opts=opts)
@@ -128,7 +135,7 @@ def check_npt_matches_oracle(eng, nsteps=3):
         run.run(nsteps)
         rep = run.reps[0]
         ref = omd.run_npt(ocell, c.grid, v0, DT, nsteps, ntn.NtnOptions(conv_check="POT", pot_tol=1.0e-6),
-                          NPT_Q, NPT_B, 600.0 * md.BOLTZMANN, NPT_P)
+                          NPT_Q, NPT_B, 600.0 * md.BOLTZMANN, NPT_P, **extra)
         lat, frac, energy, cons, vol = ref[-1]
         assert np.abs(rep.cell.lattice - lat).max() < 1e-11
         assert np.abs(_wrap(rep.cell.frac - frac)).max() < 1e-10
@@ -142,6 +149,10 @@ def check_npt_matches_oracle(eng, nsteps=3):
 
 def test_npt_matches_oracle(emu_engine):
     check_npt_matches_oracle(emu_engine)
+
+
+def test_npt_wgc_matches_oracle(emu_engine):
+    check_npt_matches_oracle(emu_engine, nsteps=2, wgc=True)
 
 
 def test_box_constraint():

@@ -123,6 +123,11 @@ static void launch_shape(SlotDev& s, size_t csz, int nfx, int* rp1, int* ty, int
 // Shared memory of the fused y-z pass of one plane (rows of odd pitch), and
 // the largest plane it takes; bigger planes run the split y/z path.
 static size_t yz_smem(const SlotDev& s, size_t csz) { return (size_t)s.n3 * (s.n2 | 1) * csz; }
+// A WGC slot's fused pass holds the three planes of a WGC group at once
+// (interleaved along y, odd pitch of 3*n2).
+static size_t yz_smem_slot(const SlotDev& s, size_t csz) {
+  return s.kinetic == KIN_WGC ? (size_t)s.n3 * ((3 * s.n2) | 1) * csz : yz_smem(s, csz);
+}
 constexpr size_t YZ_SMEM_MAX = 200 * 1024;
 // Planes up to this size run 256-thread blocks (three per SM), larger ones 512.
 constexpr size_t YZ_SMEM_SMALL = 75 * 1024;
@@ -212,10 +217,12 @@ struct PlanTable {
 // Launch lists of one tick.  Passes 1, 3 and 5 have one list for the WT slots
 // (P_X1, P_Z3, P_X5) and one for the WGC slots (P_X1G, P_Z3G, P_X5G), each
 // launched with the kernel instantiated for that functional.  A slot takes
-// either the fused y-z pass (P_YZ, or P_YZB for planes above YZ_SMEM_SMALL)
+// either the fused y-z pass (P_YZ, or P_YZB for planes above YZ_SMEM_SMALL;
+// P_YZG / P_YZBG for WGC slots, whose three-field groups share one task)
 // or the split path (P_Y2, P_Z3/P_Z3G, P_Y4).
 enum Pass : int { P_VEC = 0, P_X1 = 1, P_Y2 = 2, P_Z3 = 3, P_Y4 = 4, P_X5 = 5, P_CTL = 6,
-                  P_X1G = 7, P_Z3G = 8, P_X5G = 9, P_YZ = 10, P_YZB = 11, NPASS = 12 };
+                  P_X1G = 7, P_Z3G = 8, P_X5G = 9, P_YZ = 10, P_YZB = 11, P_YZG = 12, P_YZBG = 13,
+                  NPASS = 14 };
 constexpr int VEC_PER_TICK = 2;
 constexpr int VCHUNK = 4096;
 
@@ -259,9 +266,10 @@ template <typename T, int KS> __global__ void __launch_bounds__(256, PassMinBloc
 }
 // Fused y-z pass: 256-thread blocks, three per SM, for planes up to
 // YZ_SMEM_SMALL; 512-thread blocks, one per SM, for larger planes.
-template <typename T, int NT> __global__ void __launch_bounds__(NT, NT == 256 ? 3 : 1) k_yzpass(Args<T> a) {
+template <typename T, int NT, int KS>
+__global__ void __launch_bounds__(NT, NT == 256 ? 3 : 1) k_yzpass(Args<T> a) {
   extern __shared__ __align__(16) char sm[];
-  yzpass_block<T>(a, blockIdx.x, threadIdx.x, blockDim.x, sm);
+  yzpass_block<T, KS>(a, blockIdx.x, threadIdx.x, blockDim.x, sm);
 }
 template <typename T, int KS> __global__ void __launch_bounds__(256, XinvMinBlocks<T>::value) k_xinv(Args<T> a) {
   extern __shared__ __align__(16) char sm[];
@@ -1792,7 +1800,7 @@ struct Engine {
     v[0] = h.xcap ? h.xcap : kCaps[pi][0];
     v[1] = h.rp1;
     v[2] = h.sd.rp;
-    v[3] = uses_yz(h) ? (h.yzt ? h.yzt : (yz_smem(h.sd, csz) <= YZ_SMEM_SMALL ? 256 : 512)) : 0;
+    v[3] = uses_yz(h) ? (h.yzt ? h.yzt : (yz_smem_slot(h.sd, csz) <= YZ_SMEM_SMALL ? 256 : 512)) : 0;
     return OFDFT_OK;
   }
 
@@ -1849,7 +1857,7 @@ struct Engine {
   // Whether a running slot takes the fused y-z pass: WT slots whose (y, z)
   // plane fits shared memory, outside the set-up passes.
   bool uses_yz(const HostSlot& h) const {
-    return h.sd.kinetic == KIN_WT && !h.setup_pass && yz_smem(h.sd, 2 * elem_size(h.prec)) <= YZ_SMEM_MAX;
+    return !h.setup_pass && yz_smem_slot(h.sd, 2 * elem_size(h.prec)) <= YZ_SMEM_MAX;
   }
 
   int build_lists() {
@@ -1874,11 +1882,12 @@ struct Engine {
       L[px1].nthr = 256;
       L[px1].smem = std::max(L[px1].smem, xfwd_smem(s.n1, std::max(s.nf, s.ion.nspec), h.rp1, cs / 2));
       if (uses_yz(h)) {  // fused y-z pass: one task per (field, kx)
-        const size_t sm = yz_smem(s, cs);
-        const int pyz = h.yzt == 256 ? P_YZ : h.yzt == 512 ? P_YZB : sm <= YZ_SMEM_SMALL ? P_YZ : P_YZB;
+        const size_t sm = yz_smem_slot(s, cs);
+        const bool big = h.yzt == 256 ? false : h.yzt == 512 ? true : sm > YZ_SMEM_SMALL;
+        const int pyz = wgc ? (big ? P_YZBG : P_YZG) : (big ? P_YZB : P_YZ);
         for (int g = 0; g < s.ngroups; ++g)
           for (int kx = 0; kx < s.k1; ++kx) L[pyz].h.push_back({i, g, kx, 0});
-        L[pyz].nthr = pyz == P_YZ ? 256 : 512;
+        L[pyz].nthr = big ? 512 : 256;
         L[pyz].smem = std::max(L[pyz].smem, sm);
       } else {  // split path: y forward, z with the operator, y inverse
         for (int pass : {P_Y2, P_Y4}) {
@@ -1972,8 +1981,10 @@ struct Engine {
     run(P_Z3, [](Args<T>& a, int b, char* sm) { zpass_block<T, KS_WT>(a, b, 0, 1, sm); });
     run(P_Z3G, [](Args<T>& a, int b, char* sm) { zpass_block<T, KS_WGC>(a, b, 0, 1, sm); });
     run(P_Y4, [](Args<T>& a, int b, char* sm) { ypass_block<T>(a, b, 0, 1, sm, 1); });
-    run(P_YZ, [](Args<T>& a, int b, char* sm) { yzpass_block<T>(a, b, 0, 1, sm); });
-    run(P_YZB, [](Args<T>& a, int b, char* sm) { yzpass_block<T>(a, b, 0, 1, sm); });
+    run(P_YZ, [](Args<T>& a, int b, char* sm) { yzpass_block<T, KS_WT>(a, b, 0, 1, sm); });
+    run(P_YZB, [](Args<T>& a, int b, char* sm) { yzpass_block<T, KS_WT>(a, b, 0, 1, sm); });
+    run(P_YZG, [](Args<T>& a, int b, char* sm) { yzpass_block<T, KS_WGC>(a, b, 0, 1, sm); });
+    run(P_YZBG, [](Args<T>& a, int b, char* sm) { yzpass_block<T, KS_WGC>(a, b, 0, 1, sm); });
     run(P_X5, [](Args<T>& a, int b, char* sm) { xinv_block<T, KS_WT>(a, b, 0, 1, sm); });
     run(P_X5G, [](Args<T>& a, int b, char* sm) { xinv_block<T, KS_WGC>(a, b, 0, 1, sm); });
     run(P_CTL, [](Args<T>& a, int b, char*) { ctl_block(a.slots, a.ctl, a.tasks, K_X5, b, 0, 1, (char*)ctl_sm); });
@@ -1996,8 +2007,10 @@ struct Engine {
     }
     if ((rc = launch_one<T>(prec, P_X1, k_xfwd<T, KS_WT>))) return rc;
     if ((rc = launch_one<T>(prec, P_X1G, k_xfwd<T, KS_WGC>))) return rc;
-    if ((rc = launch_one<T>(prec, P_YZ, k_yzpass<T, 256>))) return rc;
-    if ((rc = launch_one<T>(prec, P_YZB, k_yzpass<T, 512>))) return rc;
+    if ((rc = launch_one<T>(prec, P_YZ, k_yzpass<T, 256, KS_WT>))) return rc;
+    if ((rc = launch_one<T>(prec, P_YZB, k_yzpass<T, 512, KS_WT>))) return rc;
+    if ((rc = launch_one<T>(prec, P_YZG, k_yzpass<T, 256, KS_WGC>))) return rc;
+    if ((rc = launch_one<T>(prec, P_YZBG, k_yzpass<T, 512, KS_WGC>))) return rc;
     if ((rc = launch_one<T>(prec, P_Y2, k_ypass<T>, -1))) return rc;
     if ((rc = launch_one<T>(prec, P_Z3, k_zpass<T, KS_WT>))) return rc;
     if ((rc = launch_one<T>(prec, P_Z3G, k_zpass<T, KS_WGC>))) return rc;
@@ -2037,8 +2050,10 @@ struct Engine {
     load(k_ypass<T>);
     load(k_zpass<T, KS_WT>);
     load(k_zpass<T, KS_WGC>);
-    load(k_yzpass<T, 256>);
-    load(k_yzpass<T, 512>);
+    load(k_yzpass<T, 256, KS_WT>);
+    load(k_yzpass<T, 512, KS_WT>);
+    load(k_yzpass<T, 256, KS_WGC>);
+    load(k_yzpass<T, 512, KS_WGC>);
     load(k_xinv<T, KS_WT>);
     load(k_xinv<T, KS_WGC>);
     load(k_permute_kernel<T>);
@@ -2083,8 +2098,10 @@ struct Engine {
     if ((rc = attr(k_zpass<T, KS_WGC>, P_Z3G))) return rc;
     if ((rc = attr(k_xinv<T, KS_WGC>, P_X5G))) return rc;
     if ((rc = attr(k_ypass<T>, lists[prec][P_Y2].smem >= lists[prec][P_Y4].smem ? P_Y2 : P_Y4))) return rc;
-    if ((rc = attr(k_yzpass<T, 256>, P_YZ))) return rc;
-    if ((rc = attr(k_yzpass<T, 512>, P_YZB))) return rc;
+    if ((rc = attr(k_yzpass<T, 256, KS_WT>, P_YZ))) return rc;
+    if ((rc = attr(k_yzpass<T, 512, KS_WT>, P_YZB))) return rc;
+    if ((rc = attr(k_yzpass<T, 256, KS_WGC>, P_YZG))) return rc;
+    if ((rc = attr(k_yzpass<T, 512, KS_WGC>, P_YZBG))) return rc;
     if ((rc = attr(k_zpass<T, KS_WT>, P_Z3))) return rc;
     return attr(k_xinv<T, KS_WT>, P_X5);
   }
@@ -2827,7 +2844,7 @@ extern "C" int ofdft_calculate_potential_plus_noalloc(const ofdft_cell_desc* d, 
   };
   if ((rc = attr(k_xfwd<double, KS_WT>, sm1)) || (rc = attr(k_xinv<double, KS_WT>, sm5)))
     return rc;
-  if (fused && (rc = yzthr == 256 ? attr(k_yzpass<double, 256>, yzsm) : attr(k_yzpass<double, 512>, yzsm)))
+  if (fused && (rc = yzthr == 256 ? attr(k_yzpass<double, 256, KS_WT>, yzsm) : attr(k_yzpass<double, 512, KS_WT>, yzsm)))
     return rc;
   if (!fused && ((rc = attr(k_ypass<double>, sm2)) || (rc = attr(k_zpass<double, KS_WT>, sm3))))
     return rc;
@@ -2836,8 +2853,8 @@ extern "C" int ofdft_calculate_potential_plus_noalloc(const ofdft_cell_desc* d, 
   k_xfwd<double, KS_WT><<<nt[0], 256, sm1, st>>>(a);
   a.tasks = tb + nt[0];
   if (fused) {
-    if (yzthr == 256) k_yzpass<double, 256><<<nt[1], 256, yzsm, st>>>(a);
-    else k_yzpass<double, 512><<<nt[1], 512, yzsm, st>>>(a);
+    if (yzthr == 256) k_yzpass<double, 256, KS_WT><<<nt[1], 256, yzsm, st>>>(a);
+    else k_yzpass<double, 512, KS_WT><<<nt[1], 512, yzsm, st>>>(a);
   } else {
     k_ypass<double><<<nt[1], 256, sm2, st>>>(a, -1);
     a.tasks = tb + nt[0] + nt[1];

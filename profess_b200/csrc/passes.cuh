@@ -800,6 +800,136 @@ struct GOp {
   }
 };
 
+// The (y, z) planes at kx of the three fields of a WGC group in the spectra
+// (field p at base + p*Nc), seen as 3*n2 columns c = p*n2 + y of n3
+// positions z.
+template <typename T>
+struct Planes3IO {
+  cx<T>* base;
+  long long Nc;
+  int n2;
+  unsigned mn2;
+  HD size_t at(int c, int z) const {
+    const int p = magic_div32(c, mn2), y = c - p * n2;
+    return (size_t)p * (size_t)Nc + (size_t)z * n2 + y;
+  }
+  HD cx<T> ld(int c, int z) const { return base[at(c, z)]; }
+  HD void st(int c, int z, cx<T> v) const { base[at(c, z)] = v; }
+};
+
+// The last forward y stage (radix R, stride 1) of the three planes of a WGC
+// group, the second-order WGC operator (the same sums as the split z pass:
+// G_WGC3 in zpass_operator, KEDF_WGC.f90:219-236) and the first inverse y
+// stage, in registers.  Plane p of column z starts at buf + z*cs + p*n2; the
+// kernel planes K1..K4 of this kx are kern + j*Nc, indexed z*n2 + y.
+template <typename T, int R>
+HD void ip_stage_wgc3_r(cx<T>* __restrict__ buf, int n3, unsigned mn3, int cs, int n2,
+                        const T* __restrict__ kern, long long Nc, T sc, int tid, int nthr) {
+  const int total = (n2 / R) * n3;
+  for (int w = tid; w < total; w += nthr) {
+    const int blk = magic_div32(w, mn3), z = w - blk * n3;
+    cx<T>* p0 = buf + z * cs + blk * R;
+    cx<T> v0[R], v1[R], v2[R];
+#pragma unroll
+    for (int r = 0; r < R; ++r) {
+      v0[r] = p0[r];
+      v1[r] = p0[n2 + r];
+      v2[r] = p0[2 * n2 + r];
+    }
+    Dft<T, R, -1>::run(v0);
+    Dft<T, R, -1>::run(v1);
+    Dft<T, R, -1>::run(v2);
+#pragma unroll
+    for (int r = 0; r < R; ++r) {
+      const int kidx = z * n2 + blk * R + r;
+      const T K1 = kern[kidx], K2 = kern[Nc + kidx], K3 = kern[2 * Nc + kidx], K4 = kern[3 * Nc + kidx];
+      const cx<T> F0 = v0[r], F1 = v1[r], F2 = v2[r];
+      v0[r] = (F0 * K1 + F1 * K2 + F2 * K3) * sc;
+      v1[r] = (F0 * K2 + F1 * K4) * sc;
+      v2[r] = F0 * (K3 * sc);
+    }
+    Dft<T, R, 1>::run(v0);
+    Dft<T, R, 1>::run(v1);
+    Dft<T, R, 1>::run(v2);
+#pragma unroll
+    for (int r = 0; r < R; ++r) {
+      p0[r] = v0[r];
+      p0[n2 + r] = v1[r];
+      p0[2 * n2 + r] = v2[r];
+    }
+  }
+}
+
+template <typename T>
+HD void ip_stage_wgc3(cx<T>* buf, int n3, unsigned mn3, int cs, const FftPlan& py, const T* kern, long long Nc,
+                      T sc, int tid, int nthr) {
+  constexpr int RM = FftMaxRadix<T>::value;
+  const int n2 = py.n;
+#define OFDFT_W3_CASE(r)                                                                              \
+  case r:                                                                                             \
+    if constexpr (r <= RM) ip_stage_wgc3_r<T, r>(buf, n3, mn3, cs, n2, kern, Nc, sc, tid, nthr);     \
+    break;
+  switch (py.R[py.nst - 1]) {
+    OFDFT_W3_CASE(2)
+    OFDFT_W3_CASE(3)
+    OFDFT_W3_CASE(4)
+    OFDFT_W3_CASE(5)
+    OFDFT_W3_CASE(6)
+    OFDFT_W3_CASE(7)
+    OFDFT_W3_CASE(8)
+    OFDFT_W3_CASE(9)
+    OFDFT_W3_CASE(10)
+    OFDFT_W3_CASE(12)
+    OFDFT_W3_CASE(14)
+    OFDFT_W3_CASE(15)
+    OFDFT_W3_CASE(16)
+    default: break;
+  }
+#undef OFDFT_W3_CASE
+}
+
+// Task (WGC group g, kx): the three fields' (y, z) planes at kx together in
+// shared memory, interleaved along y (field p, y, z at z*P3 + p*n2 + y, P3 =
+// odd pitch of 3*n2), since the WGC operator mixes the three at each
+// frequency.  The z transforms run over all 3*n2 columns at once, the y
+// transforms plane by plane, and the last forward y stage, the operator and
+// the first inverse y stage run in registers for the three planes together.
+// As the single-field task, one read and one write of each plane in HBM.
+template <typename T>
+HD void yz_wgc3_block(const Args<T>& a, const SlotDev& s, int g, int kx, cx<T>* buf, int tid, int nthr) {
+  const int n2 = s.n2, n3 = s.n3, nrows = n2 * n3, nc = 3 * n2, P3 = odd_pitch(nc);
+  const long long Nc = s.Nc;
+  const FftPlan& py = s.py;
+  const FftPlan& pz = s.pz;
+  const cx<T>* ry = a.tw + py.root;
+  const cx<T>* rz = a.tw + pz.root;
+  const unsigned mnc = magic32(nc), mn3 = magic32(n3);
+  const Planes3IO<T> glob{(cx<T>*)s.spec + (size_t)s.group_f0[g] * (size_t)Nc + (size_t)kx * nrows, Nc, n2,
+                          magic32(n2)};
+  const PlaneIO<T> rows{buf, P3};
+  ip_stage_acc<T, -1>(glob, rows, nc, mnc, pz, 0, rz, tid, nthr);
+  BLOCK_SYNC();
+  for (int st = 1; st < pz.nst; ++st) {
+    ip_stage<T, -1>(buf, nc, mnc, 1, P3, pz, st, rz, tid, nthr);
+    BLOCK_SYNC();
+  }
+  for (int st = 0; st < py.nst - 1; ++st) {
+    for (int p = 0; p < 3; ++p) ip_stage<T, -1>(buf + p * n2, n3, mn3, P3, 1, py, st, ry, tid, nthr);
+    BLOCK_SYNC();
+  }
+  ip_stage_wgc3<T>(buf, n3, mn3, P3, py, (const T*)s.kern + (size_t)kx * nrows, Nc, (T)s.inv_n, tid, nthr);
+  BLOCK_SYNC();
+  for (int st = py.nst - 2; st >= 0; --st) {
+    for (int p = 0; p < 3; ++p) ip_stage<T, 1>(buf + p * n2, n3, mn3, P3, 1, py, st, ry, tid, nthr);
+    BLOCK_SYNC();
+  }
+  for (int st = pz.nst - 1; st >= 1; --st) {
+    ip_stage<T, 1>(buf, nc, mnc, 1, P3, pz, st, rz, tid, nthr);
+    BLOCK_SYNC();
+  }
+  ip_stage_acc<T, 1>(rows, glob, nc, mnc, pz, 0, rz, tid, nthr);
+}
+
 // Task (group g, kx) of a single-field group: the whole (y, z) plane of the
 // field at kx (n2*n3 contiguous values) in shared memory, rows of odd pitch
 // P.  The forward FFT along z loads its first stage straight from the
@@ -807,7 +937,9 @@ struct GOp {
 // its last stage, the operator and the first inverse stage run in registers
 // in one pass; then the inverse along y and z, whose last stage stores
 // straight to the spectra.  One read and one write of the plane in HBM.
-template <typename T>
+// KS = KS_WGC also takes the three-field WGC groups (yz_wgc3_block); the WT
+// instantiation carries none of their code.
+template <typename T, int KS>
 HD void yzpass_block(const Args<T>& a, int bid, int tid, int nthr, char* smem) {
   const Task t = a.tasks[bid];
   const SlotDev& s = a.slots[t.slot];
@@ -815,6 +947,12 @@ HD void yzpass_block(const Args<T>& a, int bid, int tid, int nthr, char* smem) {
   const int ev = c.ev;
   if (c.status != ST_RUNNING || ev == EV_NONE || ev == EV_ION || ev == EV_FORCE || ev == EV_STRESS) return;
   const int g = t.a, kx = t.b;
+  if constexpr (KS == KS_WGC) {
+    if (s.group_kind[g] == G_WGC3) {
+      yz_wgc3_block<T>(a, s, g, kx, (cx<T>*)smem, tid, nthr);
+      return;
+    }
+  }
   const int n2 = s.n2, n3 = s.n3, nrows = n2 * n3, P = odd_pitch(n2);
   const int kind = s.group_kind[g];
   cx<T>* plane = (cx<T>*)s.spec + (size_t)s.group_f0[g] * (size_t)s.Nc + (size_t)kx * nrows;

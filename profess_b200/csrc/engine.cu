@@ -129,8 +129,11 @@ static size_t yz_smem_slot(const SlotDev& s, size_t csz) {
   return s.kinetic == KIN_WGC ? (size_t)s.n3 * ((3 * s.n2) | 1) * csz : yz_smem(s, csz);
 }
 constexpr size_t YZ_SMEM_MAX = 200 * 1024;
-// Planes up to this size run 256-thread blocks (three per SM), larger ones 512.
-constexpr size_t YZ_SMEM_SMALL = 75 * 1024;
+// Planes up to this size run 256-thread blocks (three per SM up to 75 KB, two
+// up to 112 KB), larger ones one 512-thread block per SM.  Two 256-thread
+// blocks beat one 512-thread block on 84-99 KB plane sets (WT 72^3 FP64,
+// 108^3 FP32, WGC 64^3 FP32: 9-11 % faster evaluations).
+constexpr size_t YZ_SMEM_SMALL = 112 * 1024;
 
 // ------------------------------------------------------------ FFT plans
 static bool seven_smooth(int n) {
@@ -264,7 +267,7 @@ template <typename T, int KS> __global__ void __launch_bounds__(256, PassMinBloc
   extern __shared__ __align__(16) char sm[];
   zpass_block<T, KS>(a, blockIdx.x, threadIdx.x, blockDim.x, sm);
 }
-// Fused y-z pass: 256-thread blocks, three per SM, for planes up to
+// Fused y-z pass: 256-thread blocks, up to three per SM, for planes up to
 // YZ_SMEM_SMALL; 512-thread blocks, one per SM, for larger planes.
 template <typename T, int NT, int KS>
 __global__ void __launch_bounds__(NT, NT == 256 ? 3 : 1) k_yzpass(Args<T> a) {

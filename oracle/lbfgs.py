@@ -271,9 +271,12 @@ class LbfgsRC:
 
 
 def bfgs(cell, n, opts: ntn.NtnOptions, force_cutoff=FORCE_CUTOFF, max_calls=NMAX, alpha_=5.0 / 6.0,
-         beta_=5.0 / 6.0, rho0=None):
+         beta_=5.0 / 6.0, rho0=None, kinetic=None, gamma=2.7):
     """IonLBFGS on the oracle: returns (final fractional coordinates, the total
-    energy (Ha) of every density solve in order, final forces)."""
+    energy (Ha) of every density solve in order, final forces).  kinetic =
+    KEDF_WGC relaxes with the second-order WGC functional."""
+    from . import functional as fn
+    kinetic = fn.KEDF_WT if kinetic is None else kinetic
     from . import cellsetup as cs
     cell = dataclasses.replace(cell, frac=np.array(cell.frac, dtype=float))
     L = cell.lattice
@@ -281,7 +284,7 @@ def bfgs(cell, n, opts: ntn.NtnOptions, force_cutoff=FORCE_CUTOFF, max_calls=NMA
     rho = cs.uniform_density(cell, *n) if rho0 is None else rho0
 
     def solve(rho):
-        r = ntn.NtnSolver(functional_for(cell, n, alpha_, beta_), opts).solve(rho)
+        r = ntn.NtnSolver(functional_for(cell, n, alpha_, beta_, kinetic, gamma), opts).solve(rho)
         f, _, _ = ofo.total_forces(cell, r.rho)
         return r.rho, float(r.energy[0]), f
 

@@ -23,3 +23,8 @@ def test_bfgs_matches_oracle_on_gpu(gpu_engine):
 def test_gradient_cg_matches_oracle_on_gpu(gpu_engine):
     from test_relax import check_gradient_cg_matches_oracle
     check_gradient_cg_matches_oracle(gpu_engine)
+
+
+def test_bfgs_wgc_matches_oracle_on_gpu(gpu_engine):
+    from test_relax import check_bfgs_wgc_matches_oracle
+    check_bfgs_wgc_matches_oracle(gpu_engine)

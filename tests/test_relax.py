@@ -183,6 +183,41 @@ def test_bfgs_matches_oracle(emu_engine):
     check_bfgs_matches_oracle(emu_engine)
 
 
+def check_bfgs_wgc_matches_oracle(eng):
+    """IonLBFGS of a second-order WGC Al4 cell with displaced ions (the WGC
+    kernel stays, the ion potential and Ewald sum follow the ions) against
+    the oracle with the same functional."""
+    import cases
+    from oracle import functional as fn
+    from oracle import lbfgs as olb
+    from profess_b200 import recpot
+    import dataclasses
+    cell0, f, _, c = cases.golden_case("wgc_al4_fcc")
+    shift = np.array([[0.012, -0.008, 0.005], [-0.006, 0.01, 0.0], [0.0, -0.004, -0.009], [0.007, 0.0, 0.006]])
+    cell = dataclasses.replace(cell0, frac=np.mod(cell0.frac + shift, 1.0))
+    z = np.load(cases.GOLDEN + "/al_hc_recpot.npz")
+    sp = recpot.species_from_table(float(z["max_g"]), z["values"], "Al")
+    wc = wl.Cell(name="al4_wgc", lattice=cell.lattice, frac=cell.frac, species_of_ion=cell.species_of_ion,
+                 species=[sp], grid=tuple(f.n), kinetic=native.KEDF_WGC, alpha=c["alpha"], beta=c["beta"],
+                 gamma=c["gamma"])
+    run = relax.BFGS(eng, [wc])
+    try:
+        run.run()
+        frac, trace, _ = olb.bfgs(cell, f.n, ntn.NtnOptions(), alpha_=c["alpha"], beta_=c["beta"],
+                                  kinetic=fn.KEDF_WGC, gamma=c["gamma"])
+        assert len(run.traces[0]) == len(trace) > 2
+        assert np.abs(np.array(run.traces[0]) - trace).max() < 1e-9
+        assert trace[-1] < trace[0] - 1e-4
+        assert relax._max_force(run.states[0].forces) < relax.FORCE_CUTOFF
+        assert np.abs(run.states[0].cell.frac - frac).max() < 2e-7
+    finally:
+        run.close()
+
+
+def test_bfgs_wgc_matches_oracle(emu_engine):
+    check_bfgs_wgc_matches_oracle(emu_engine)
+
+
 def test_library_line_search_matches_oracle(emu_engine):
     """ofdft_dcsrch (the solver's Dcsrch) takes the same trial steps and ends
     with the same task as the oracle's Dcsrch on 1D functions."""

@@ -63,6 +63,28 @@ def test_eval_two_step_lengths_fp32(emu_engine, n):
     _eval_parity(emu_engine, f, cell, seed=6, prec=native.FP32, tol_pot=1e-3, tol_e=5e-5)
 
 
+WGC_AB = (1.2060113295832982827, 0.46065533708336838393)
+
+
+@pytest.mark.parametrize("n", [(8, 9, 10), (6, 14, 9), (5, 25, 8), (4, 49, 6), (6, 16, 15), (5, 18, 12),
+                               (4, 10, 14), (4, 12, 7)])
+def test_eval_wgc_fused_yz_radices(emu_engine, n):
+    """WGC groups in the fused y-z pass (three planes a task): y lengths whose
+    last stage, where the WGC operator sits, has radix 9, 2, 5, 7, 4, 3, 10 and
+    12, against the oracle in FP64."""
+    cell, _, _, _ = cases.golden_case("wgc_al4_fcc")
+    f = cases.functional_for(cell, n, fn.KEDF_WGC, *WGC_AB)
+    _eval_parity(emu_engine, f, cell, seed=7)
+
+
+@pytest.mark.parametrize("n", [(6, 16, 10), (5, 32, 9), (4, 15, 16)])
+def test_eval_wgc_fused_yz_fp32(emu_engine, n):
+    """The same in FP32 (radix 16, 4 and 15 in the operator stage)."""
+    cell, _, _, _ = cases.golden_case("wgc_al4_fcc")
+    f = cases.functional_for(cell, n, fn.KEDF_WGC, *WGC_AB)
+    _eval_parity(emu_engine, f, cell, seed=8, prec=native.FP32, tol_pot=1e-5, tol_e=2e-5)
+
+
 def test_eval_wt_alpha_ne_beta(emu_engine):
     cell, _, _, _ = cases.golden_case("wt_al4_displaced")
     f = cases.functional_for(cell, (16, 16, 18), fn.KEDF_WT, 1.0, 2.0 / 3.0)

@@ -269,3 +269,21 @@ def test_repeated_ion_builds_hold_device_memory(gpu_engine):
 def test_copy_tables_on_gpu(gpu_engine):
     from test_emu_engine import check_copy_tables
     check_copy_tables(gpu_engine)
+
+
+@pytest.mark.parametrize("n,prec", [((8, 9, 10), native.FP64), ((6, 14, 9), native.FP64), ((5, 25, 8), native.FP64),
+                                    ((4, 49, 6), native.FP64), ((6, 16, 15), native.FP64), ((5, 18, 12), native.FP64),
+                                    ((4, 10, 14), native.FP64), ((4, 12, 7), native.FP64), ((6, 16, 10), native.FP32),
+                                    ((5, 32, 9), native.FP32), ((4, 15, 16), native.FP32)])
+def test_wgc_fused_yz_radices_on_gpu(gpu_engine, n, prec):
+    """WGC groups in the fused y-z pass with the WGC operator in a last y
+    stage of radix 2 to 16, against the oracle (the grids of the emulated
+    test_eval_wgc_fused_yz_* cases)."""
+    from test_emu_engine import WGC_AB, _eval_parity
+    cell, _, _, _ = cases.golden_case("wgc_al4_fcc")
+    f = cases.functional_for(cell, n, fn.KEDF_WGC, *WGC_AB)
+    if prec == native.FP64:
+        _eval_parity(gpu_engine, f, cell, seed=7)
+    else:
+        _eval_parity(gpu_engine, f, cell, seed=8, prec=native.FP32, tol_pot=1e-5, tol_e=2e-5)
+
